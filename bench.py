@@ -1,0 +1,341 @@
+"""Benchmark: the plain FP32 fluid step at 128 x 192 x 128 cells (the operator-level configuration: seeded
+smoothed velocities, a masked smoke sphere, temperature 1 + 0.8 smoke; the smoke-puff step with 4 multigrid
+V-cycles of 2+2 sweeps, buoyancy, drag, vorticity confinement and a sphere emitter; dt = 1/96 s).
+
+One step = one substep of the whole grid (Stepper.step -> plume_step, about 70 kernels, no host sync).
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference] [--cells NX,NY,NZ]
+
+Multi-GPU: one process per GPU (torchrun); a single grid does not shard, so every rank steps its own
+replica (weak scaling, no collective on the data path); rank 0 prints one JSON line with the max time over
+ranks. `--impl reference` times the CPU restatement of the reference (the oracle, C++ with OpenMP on all host
+cores) on the same workload; the reference itself is Python driving NVIDIA Warp, which is not installed here.
+"""
+
+import argparse
+import json
+import math
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import time
+from pathlib import Path
+
+import numpy as np
+
+REPO = Path(__file__).resolve().parent
+sys.path.insert(0, str(REPO))
+
+METRIC = "Mcell-substeps/s"
+# Algorithmic bytes per cell-substep of each phase (FP32, compulsory traffic, intermediates not counted):
+# forces R s,T + R/W u,v,w = 32 (emission writes only the emitter's cells); velocity MacCormack R/W u,v,w = 24;
+# divergence R u,v,w + W div = 16; multigrid 74 per top cell per V-cycle; gradient R q + R/W u,v,w = 28;
+# scalar MacCormack + budget + dissipation R u,v,w,s,T + W s,T, then R/W s,T = 44.
+PHASE_BYTES = {"forces": 32.0, "velocity advection": 24.0, "divergence": 16.0, "pressure solve": None,
+               "gradient": 28.0, "scalar advection": 44.0}
+MG_BYTES_PER_CYCLE = 74.0
+
+
+def parse_args():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=96)
+    ap.add_argument("--warmup", type=int, default=5)
+    ap.add_argument("--impl", choices=("ours", "reference"), default="ours")
+    ap.add_argument("--cells", default="128,192,128")
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    return ap.parse_args()
+
+
+def peaks() -> tuple[float, str]:
+    path = REPO / "MEASURED_PEAKS.json"
+    if path.exists():
+        return float(json.loads(path.read_text())["hbm_gbs"]), "measured"
+    return 6650.0, "fallback"
+
+
+class ClockSampler:
+    """nvidia-smi clock and throttle samples for one GPU while the timed region runs."""
+
+    QUERY = ("index,uuid,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+             "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+             "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, uuid: str | None):
+        self.uuid = uuid
+        self.file = tempfile.NamedTemporaryFile("w+", suffix=".csv", delete=False)
+        self.proc = None
+
+    def __enter__(self):
+        try:
+            cmd = ["nvidia-smi", f"--query-gpu={self.QUERY}", "--format=csv,noheader,nounits", "-lms", "200"]
+            if self.uuid:
+                cmd += ["-i", self.uuid]
+            self.proc = subprocess.Popen(cmd, stdout=self.file, stderr=subprocess.DEVNULL)
+        except OSError:
+            self.proc = None
+        return self
+
+    def __exit__(self, *exc):
+        if self.proc is not None:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except subprocess.TimeoutExpired:
+                self.proc.kill()
+
+    def summary(self) -> dict:
+        self.file.flush()
+        rows = [line.split(",") for line in Path(self.file.name).read_text().splitlines() if line.strip()]
+        rows = [[c.strip() for c in r] for r in rows if len(r) >= 10]
+        if not rows:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unsampled"]}
+        sm = [float(r[2]) for r in rows if r[2].replace(".", "").isdigit()]
+        max_sm = [float(r[3]) for r in rows if r[3].replace(".", "").isdigit()]
+        names = ("hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap")
+        reasons = sorted({name for r in rows for name, flag in zip(names, r[6:10]) if flag.lower() == "active"})
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": max(max_sm) if max_sm else None,
+                "reasons": reasons, "samples": len(rows)}
+
+
+def dist_env():
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    return world, rank, local
+
+
+def seeded_state(cells, ambient_k):
+    from plume_b200.workloads import operator_fields
+
+    return operator_fields(cells, 20261203, ambient_k)
+
+
+def cpu_baseline(recipe, derived, fields, budget_s: float = 20.0) -> dict:
+    """The oracle (C++ restatement of the reference, OpenMP on all host cores) on a bounded sample of the same
+    workload: whole-grid substeps from the same seeded state, as many as fit in about `budget_s` seconds."""
+    from oracle import oracle as O
+
+    threads = O.set_threads(os.cpu_count() or 1)
+    d = recipe.domain
+    grid = O.make_grid(derived, d.cell_m, d.faces, d.ambient_k)
+    for name, values in fields.items():
+        getattr(grid, name).data[...] = values
+    stepper = O.Stepper(grid, recipe)
+    stepper.step(0.0, derived.dt_s)  # warm-up
+    steps, start = 0, time.perf_counter()
+    while True:
+        stepper.step((steps + 1) * derived.dt_s, derived.dt_s)
+        steps += 1
+        elapsed = time.perf_counter() - start
+        if elapsed > budget_s or steps >= 8:
+            break
+    cells = math.prod(derived.cells)
+    return {"value": cells * steps / elapsed / 1e6, "unit": METRIC, "cores": threads, "kind": "port",
+            "sample": f"{steps} whole-grid substeps of the {'x'.join(map(str, derived.cells))} plain step after 1 "
+                      f"warm-up, oracle C++ FP32 with OpenMP on {threads} threads ({elapsed:.1f} s)"}
+
+
+def run_reference(args, cells):
+    """--impl reference: the oracle port of the reference's CPU path on the host cores."""
+    world, rank, _ = dist_env()
+    if rank != 0:
+        return
+    from oracle import oracle as O
+    from plume_b200.recipe.derived import derive
+    from plume_b200.workloads import plain_step_recipe
+
+    recipe = plain_step_recipe(cells, cycles=4)
+    derived = derive(recipe)
+    threads = O.set_threads(os.cpu_count() or 1)
+    d = recipe.domain
+    grid = O.make_grid(derived, d.cell_m, d.faces, d.ambient_k)
+    for name, values in seeded_state(derived.cells, d.ambient_k).items():
+        getattr(grid, name).data[...] = values
+    stepper = O.Stepper(grid, recipe)
+    for n in range(args.warmup):
+        stepper.step(n * derived.dt_s, derived.dt_s)
+    budget_s, timed, start = 150.0, 0, time.perf_counter()
+    for n in range(args.steps):
+        stepper.step((args.warmup + n) * derived.dt_s, derived.dt_s)
+        timed += 1
+        if time.perf_counter() - start > budget_s:
+            break
+    elapsed = time.perf_counter() - start
+    value = math.prod(derived.cells) * timed / elapsed / 1e6
+    sample = (f"{timed} of {args.steps} whole-grid substeps (stopped at the {budget_s:.0f} s budget)" if timed < args.steps
+              else f"{timed} whole-grid substeps") + f" after {args.warmup} warm-up, {threads} threads"
+    line = {"metric": METRIC, "value": value, "unit": METRIC, "n_gpus": world, "steps": timed,
+            "warmup": args.warmup, "ms_per_step": elapsed * 1e3 / timed, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+            "impl": "reference",
+            "config": {"workload": f"plain FP32 fluid step {'x'.join(map(str, derived.cells))}, 4 multigrid V-cycles",
+                       "cells": list(derived.cells), "parallelism": "replicas"},
+            "cpu_baseline": {"value": value, "unit": METRIC, "cores": threads, "kind": "port", "sample": sample},
+            "e2e": {"value": value, "unit": METRIC, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+
+
+def main():
+    args = parse_args()
+    cells = tuple(int(x) for x in args.cells.split(","))
+    if args.impl == "reference":
+        run_reference(args, cells)
+        return
+    import torch
+    import torch.distributed as dist
+
+    from plume_b200 import _native as N
+    from plume_b200.recipe.derived import derive
+    from plume_b200.render.camera import sheet_domain_view
+    from plume_b200.render.frame_renderer import FrameRenderer
+    from plume_b200.sim.grid import make_grid
+    from plume_b200.sim.step_cap import StepCap
+    from plume_b200.sim.stepper import Stepper
+    from plume_b200.workloads import plain_step_recipe
+
+    world, rank, local = dist_env()
+    torch.cuda.set_device(local)
+    device = f"cuda:{local}"
+    if world > 1:
+        from datetime import timedelta
+
+        dist.init_process_group("nccl", timeout=timedelta(seconds=120), device_id=torch.device(device))
+    recipe = plain_step_recipe(cells, cycles=4)
+    derived = derive(recipe)
+    d = recipe.domain
+    fields = seeded_state(derived.cells, d.ambient_k)
+    grid = make_grid(derived, d.cell_m, d.faces, d.ambient_k, device)
+    for name, values in fields.items():
+        getattr(grid, name).data.copy_(torch.from_numpy(values))
+    stepper = Stepper(grid, recipe)
+    dt = derived.dt_s
+    stream = torch.cuda.current_stream()
+    for n in range(args.warmup):
+        stepper.step(n * dt, dt)
+    torch.cuda.synchronize()
+
+    # timed region: K substeps, phase events recorded inside plume_step on the same stream
+    phases = N.STEP_PHASES
+    events = [[torch.cuda.Event(enable_timing=True) for _ in range(len(phases) + 1)] for _ in range(args.steps)]
+    for row in events:  # torch creates an event on its first record; make every handle valid first
+        for e in row:
+            e.record(stream)
+    torch.cuda.synchronize()
+    handles = [(N.ctypes.c_void_p * (len(phases) + 1))(*[e.cuda_event for e in row]) for row in events]
+    base_params = stepper._params
+    uuid = None
+    try:
+        uuid = "GPU-" + str(torch.cuda.get_device_properties(local).uuid)
+    except Exception:
+        uuid = None
+    if world > 1:
+        dist.barrier()
+    torch.cuda.synchronize()
+    launches_before = N.launch_count()
+    start, end = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    with ClockSampler(uuid) as clocks:
+        start.record(stream)
+        for n in range(args.steps):
+            step = args.warmup + n
+            params = base_params(step * dt, dt)
+            params.phase_events = N.ctypes.cast(handles[n], N.ctypes.POINTER(N.ctypes.c_void_p))
+            N.call("plume_step", stepper._state(), params, N.stream())
+            for field in (*grid.velocity_fields(), grid.smoke, grid.temperature):
+                field.swap()
+        end.record(stream)
+        torch.cuda.synchronize()
+    launches = N.launch_count() - launches_before
+    elapsed_ms = start.elapsed_time(end)
+    timing = torch.tensor([elapsed_ms], dtype=torch.float64, device=device)
+    if world > 1:
+        dist.all_reduce(timing, op=dist.ReduceOp.MAX)
+    max_ms = float(timing.item())
+    phase_ms = {name: sum(row[i].elapsed_time(row[i + 1]) for row in events) / args.steps
+                for i, name in enumerate(phases)}
+
+    # e2e: the public API frame loop (StepCap.plan readback, Stepper.step x substeps, FrameRenderer.render
+    # copying the raw frame to the host) from a state uploaded from pinned host memory inside the timed region
+    pinned = {name: torch.from_numpy(values).pin_memory() for name, values in fields.items()}
+    view = sheet_domain_view(recipe, derived)
+    renderer = FrameRenderer(view, recipe.render, derived.cells, recipe.output.channels, device)
+    cap = StepCap(recipe)
+    substeps = derived.steps_per_frame
+    frames = max(1, args.steps // substeps)
+    grid2 = make_grid(derived, d.cell_m, d.faces, d.ambient_k, device)
+    stepper2 = Stepper(grid2, recipe)
+    renderer.render(grid2)  # warm the renderer
+    torch.cuda.synchronize()
+    if world > 1:
+        dist.barrier()
+    e2e_start, e2e_end = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e2e_start.record(stream)
+    for name, tensor in pinned.items():
+        getattr(grid2, name).data.copy_(tensor, non_blocking=True)
+    steps_run = 0
+    for frame in range(frames):  # run_block of plume_b200.sim.run, one frame per block
+        start_s, length_s = frame * substeps * dt, substeps * dt
+        steps = cap.plan(grid2, start_s, length_s, substeps, f"frame {frame}").steps
+        for index in range(steps):
+            if steps == substeps:
+                stepper2.step((frame * substeps + index) * dt, dt)
+            else:
+                stepper2.step(start_s + index * length_s / steps, length_s / steps)
+        steps_run += steps
+        renderer.render(grid2)
+    e2e_end.record(stream)
+    torch.cuda.synchronize()
+    e2e_ms = torch.tensor([e2e_start.elapsed_time(e2e_end)], dtype=torch.float64, device=device)
+    if world > 1:
+        dist.all_reduce(e2e_ms, op=dist.ReduceOp.MAX)
+    e2e_ms = float(e2e_ms.item())
+
+    ncells = math.prod(derived.cells)
+    value = world * ncells * args.steps / (max_ms / 1e3) / 1e6
+    e2e_value = world * ncells * steps_run / (e2e_ms / 1e3) / 1e6
+    h2d = sum(t.numel() * 4 for t in pinned.values()) / steps_run
+    d2h = (renderer.image.numel() * 4 + 4) * frames / steps_run
+
+    peak, peak_kind = peaks()
+    cycles = recipe.solver.multigrid_cycles
+    phase_bytes = dict(PHASE_BYTES)
+    phase_bytes["pressure solve"] = MG_BYTES_PER_CYCLE * cycles
+    phase_gbs = {name: (phase_bytes[name] * ncells / (ms / 1e3) / 1e9 if ms > 0 else None)
+                 for name, ms in phase_ms.items()}
+    dominant = max(phase_ms, key=phase_ms.get)
+    achieved = phase_gbs[dominant]
+    step_bytes = sum(phase_bytes.values())
+    line = {
+        "metric": METRIC, "value": value, "unit": METRIC, "n_gpus": world, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": max_ms / args.steps, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+        "config": {"workload": f"plain FP32 fluid step {'x'.join(map(str, derived.cells))} (seeded smoothed "
+                               f"velocities, masked smoke sphere), {cycles} multigrid V-cycles x 2+2 sweeps, "
+                               f"confinement + drag + emitter, dt 1/96 s",
+                   "cells": list(derived.cells), "parallelism": f"replicas x{world}",
+                   "l2": "inputs larger than L2 (state about 0.3 GB per grid)"},
+        "roofline": {"bound": "hbm", "kernel": f"{dominant} phase of plume_step", "achieved": achieved, "peak": peak,
+                     "unit": "GB/s", "frac": achieved / peak if achieved else None, "traffic": None,
+                     "peak_kind": peak_kind},
+        "step_roofline": {"bytes_per_cell_substep": step_bytes,
+                          "achieved": step_bytes * ncells * args.steps / (max_ms / 1e3) / 1e9,
+                          "frac": step_bytes * ncells * args.steps / (max_ms / 1e3) / 1e9 / peak},
+        "phases_ms": phase_ms, "phases_gbs": phase_gbs,
+        "e2e": {"value": e2e_value, "unit": METRIC, "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,
+                "steps": steps_run, "frames": frames},
+        "gpu_launches": launches,
+        "clocks": clocks.summary(),
+    }
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        line["cpu_baseline"] = cpu_baseline(recipe, derived, fields)
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+    if world > 1:
+        dist.barrier()
+        dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

@@ -1,0 +1,242 @@
+/* plume_b200.h -- C ABI of libplume_b200.so: the sm_100a fluid step and volume render of chadmv/plume.
+ *
+ * The drop-in boundary is the reference's Python API (src/plume/sim/*, src/plume/render/*); the Python
+ * package plume_b200 keeps those names and binds this ABI with ctypes. Each entry point below replaces the
+ * Warp kernel launch(es) cited beside it (paths relative to the reference project).
+ *
+ * Conventions
+ *   - Every array is a caller-owned, C-contiguous float32 device array, shape (n0, n1, n2), n2 contiguous.
+ *     Cell arrays are (nx, ny, nz); face arrays (nx+1, ny, nz), (nx, ny+1, nz), (nx, ny, nz+1).
+ *     The library never allocates or frees caller memory; scratch is passed in by the caller.
+ *   - `stream` is a cudaStream_t (0 = the legacy default stream). Calls only enqueue work unless noted.
+ *   - Every call returns PLUME_OK (0) or a negative status; plume_last_error() returns a thread-local message
+ *     for the last failure. Calls come from one host thread per stream.
+ */
+#ifndef PLUME_B200_H
+#define PLUME_B200_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define PLUME_OK 0
+#define PLUME_ERR_INVALID (-1) /* bad argument (null pointer, size, count) */
+#define PLUME_ERR_LAUNCH (-2)  /* a kernel launch or CUDA runtime call failed */
+#define PLUME_ERR_DEVICE (-3)  /* a device-side check failed (reported through a status word) */
+
+#define PLUME_MAX_EMITTERS 16 /* emitters applied per launch; longer lists are applied in order, in chunks */
+#define PLUME_STEP_PHASES 6   /* forces, velocity advection, divergence, pressure solve, gradient, scalars */
+
+/* GridInfo (sim/grid.py:21-33). fill_hi and ghost_gap describe multigrid coarse levels (multigrid.py:84-94);
+ * the simulation grid has fill_hi = (1,1,1), ghost_gap = 0.5. open_lo/open_hi: 1 = open face, 0 = wall. */
+typedef struct PlumeGridInfo {
+  int32_t dims[3];
+  float cell_m;
+  float origin_m[3];
+  int32_t open_lo[3];
+  int32_t open_hi[3];
+  float fill_hi[3];
+  float ghost_gap;
+} PlumeGridInfo;
+
+/* EmitterParams (sim/emitters.py:23-38). shape: 0 sphere, 1 box. */
+typedef struct PlumeEmitter {
+  int32_t shape;
+  float center_m[3];
+  float radius_m;
+  float half_size_m[3];
+  float edge_softness;
+  float start_s;
+  float end_s;
+  float smoke_per_s;
+  float temperature_k;
+  float velocity_mps[3];
+  int32_t outward;
+  float noise_scale_m;
+  float noise_strength;
+  int32_t stream;
+} PlumeEmitter;
+
+/* ViewParams and LookParams (render/raymarch.py:30-52). */
+typedef struct PlumeViewParams {
+  float right[3];
+  float up[3];
+  float toward[3];
+  float left_m;
+  float top_m;
+  float pixel_m;
+  int32_t perspective;
+  float eye[3];
+} PlumeViewParams;
+
+typedef struct PlumeLookParams {
+  float opacity_per_density;
+  float glow_start_k;
+  float smoke_hides_heat;
+  float normal_fade_thickness;
+  int32_t shade_layout;
+  float shade_fill;
+} PlumeLookParams;
+
+/* One advected quantity's buffers (AdvectedField, sim/grid.py:36-51). `back` is not needed: the MacCormack
+ * correction recomputes the backward pass on the fly. */
+typedef struct PlumeField {
+  float* data;
+  float* hat;
+  float* next;
+} PlumeField;
+
+/* One multigrid level (multigrid.py:71-77): its geometry and pressure, right-hand side, residual arrays. */
+typedef struct PlumeLevel {
+  PlumeGridInfo info;
+  float* q;
+  float* rhs;
+  float* residual;
+} PlumeLevel;
+
+/* Everything one substep reads and writes (Stepper.step, sim/stepper.py:28-44). */
+typedef struct PlumeStepState {
+  PlumeGridInfo info;
+  PlumeField u, v, w, smoke, temperature;
+  float* pressure;
+  float* divergence;
+  /* scratch: confinement curl and push, 3 arrays of nx*ny*nz floats each (x, y, z components) */
+  float* curl[3];
+  float* push[3];
+  /* scratch: the smoke budget's partial sums (plume_smoke_scratch_doubles() doubles) and its factor (1 float) */
+  double* sums;
+  float* factor;
+  /* multigrid levels: levels[0] must alias pressure/divergence; coarser levels are caller-allocated */
+  const PlumeLevel* levels;
+  int32_t level_count;
+} PlumeStepState;
+
+typedef struct PlumeStepParams {
+  float time_s;
+  float dt;
+  float dt_over_cell;       /* dt / info.cell_m, computed in double and rounded (advect.py:61) */
+  int32_t seed;
+  const PlumeEmitter* emitters; /* host array */
+  int32_t emitter_count;
+  float gravity, heat_buoyancy, smoke_weight, ambient_k;
+  float confinement;        /* 0: no confinement pass */
+  float turbulence_scale_m, turbulence_strength, turbulence_pattern_time;  /* strength 0: no pass */
+  int32_t apply_drag;       /* 0: no drag pass */
+  float wind[3];
+  float drag_keep;          /* exp(-drag_per_s * dt) in double, rounded */
+  int32_t solver;           /* 0 multigrid, 1 Gauss-Seidel */
+  int32_t solver_iterations;/* multigrid cycles or Gauss-Seidel sweeps */
+  int32_t multigrid_sweeps;
+  int32_t apply_dissipation;/* 0: no dissipation pass */
+  float smoke_keep, heat_keep;
+  void* const* phase_events;/* null, or PLUME_STEP_PHASES + 1 cudaEvent_t recorded at the phase boundaries */
+} PlumeStepParams;
+
+const char* plume_last_error(void);
+int plume_abi_version(void);
+/* Kernels this library has enqueued in this process (all streams); for launch accounting in benchmarks. */
+unsigned long long plume_launch_count(void);
+
+/* ---- per-operator entry points (used by the Python mirror of each reference function) ---------------- */
+
+/* advect.py:53-56,71-76 semi_lagrangian_kernel: dst = sample(src, trace(p, dt_over_cell)). */
+int plume_advect_semi_lagrangian(const PlumeGridInfo* info, const int32_t shape[3], const float* src, float* dst,
+                                 const float* u, const float* v, const float* w, float dt_over_cell,
+                                 const float offset[3], float outside, int32_t uses_outside, void* stream);
+
+/* advect.py:59-68 advect_maccormack (semi_lagrangian_kernel twice + maccormack_correct_kernel): writes the
+ * forward pass into `hat` and the clamped correction into `next`. */
+int plume_advect_maccormack(const PlumeGridInfo* info, const int32_t shape[3], const float* data, float* hat,
+                            float* next, const float* u, const float* v, const float* w, float dt_over_cell,
+                            const float offset[3], float outside, int32_t uses_outside, void* stream);
+
+/* emitters.py:147-153 emit (emit_scalars_kernel + 3 x emit_velocity_kernel); `emitters` is a host array. */
+int plume_emit(const PlumeGridInfo* info, float* smoke, float* temperature, float* u, float* v, float* w,
+               const PlumeEmitter* emitters, int32_t count, int32_t seed, float time_s, float dt, void* stream);
+
+/* forces.py:26-31 apply_buoyancy (buoyancy_kernel). */
+int plume_buoyancy(const PlumeGridInfo* info, float* v, const float* smoke, const float* temperature,
+                   float gravity, float heat_buoyancy, float smoke_weight, float ambient_k, float dt, void* stream);
+
+/* forces.py:40-48 apply_drag (drag_kernel x 3): f = wind + (f - wind) * keep. */
+int plume_drag(const PlumeGridInfo* info, float* u, float* v, float* w, const float wind[3], float keep,
+               void* stream);
+
+/* vorticity.py:95-111 VorticityConfinement.apply / measure_curl: writes curl[3] (and push[3] and adds
+ * push*dt to the faces when `apply` is 1). */
+int plume_confinement(const PlumeGridInfo* info, float* u, float* v, float* w, float* curl_xyz[3],
+                      float* push_xyz[3], float strength, float dt, int32_t apply, void* stream);
+
+/* turbulence.py:59-67 apply_turbulence (turbulence_kernel x 3). */
+int plume_turbulence(const PlumeGridInfo* info, float* u, float* v, float* w, int32_t seed, float scale_m,
+                     float strength, float pattern_time, float dt, void* stream);
+
+/* pressure.py:144-154 project: zero_closed_faces_kernel x 3 + divergence_kernel (this call), then the solve,
+ * then subtract_gradient_kernel x 3 (plume_subtract_gradient). */
+int plume_project_begin(const PlumeGridInfo* info, float* u, float* v, float* w, float* divergence,
+                        void* stream);
+int plume_divergence(const PlumeGridInfo* info, const float* u, const float* v, const float* w,
+                     float* divergence, void* stream);
+int plume_subtract_gradient(const PlumeGridInfo* info, float* u, float* v, float* w, const float* q,
+                            void* stream);
+
+/* pressure.py:124-141 GaussSeidel / red_black_sweeps (red_black_sweep_kernel, colour 0 then 1 per sweep). */
+int plume_red_black_sweeps(const PlumeGridInfo* info, float* q, const float* rhs, int32_t sweeps,
+                           float relaxation, void* stream);
+
+/* multigrid.py:124-147 Multigrid.__call__: `cycles` V-cycles over caller-allocated levels. */
+int plume_multigrid(const PlumeLevel* levels, int32_t level_count, int32_t cycles, int32_t sweeps, void* stream);
+
+/* multigrid.py:36-43 residual_kernel. */
+int plume_residual(const PlumeGridInfo* info, const float* q, const float* rhs, float* residual, void* stream);
+
+/* conserve.py:45-52 SmokeBudget.hold + reduce.py:28-38 TripleSum, on the device: totals of data, hat and next
+ * (each line summed along x in float, the lines added in double in a fixed order), the held factor
+ * max(sl, min(mc, before)) / mc (1 when mc <= 0) stored as float in *factor, and next *= factor.
+ * `sums` needs plume_smoke_scratch_doubles(info) doubles. If `totals_out` is not null the three totals are
+ * also copied to it (device memory, 3 doubles). */
+int plume_smoke_scratch_doubles(const PlumeGridInfo* info);
+int plume_smoke_budget(const PlumeGridInfo* info, const float* data, const float* hat, float* next,
+                       double* sums, float* factor, double* totals_out, void* stream);
+
+/* reduce.py:28-38 TripleSum: the three totals (device, 3 doubles) without scaling. */
+int plume_triple_sum(const int32_t shape[3], const float* a, const float* b, const float* c, double* sums,
+                     double* totals_out, void* stream);
+
+/* dissipate.py:18-24 dissipate (dissipate_kernel). */
+int plume_dissipate(const PlumeGridInfo* info, float* smoke, float* temperature, float smoke_keep,
+                    float heat_keep, float ambient_k, void* stream);
+
+/* step_cap.py:50-55 StepCap.grid_speed: largest |u|, |v|, |w| into *speed (device float). */
+int plume_grid_speed(const PlumeGridInfo* info, const float* u, const float* v, const float* w, float* speed,
+                     void* stream);
+
+/* stepper.py:28-44 Stepper.step: one whole substep. On return the caller swaps data/next of u, v, w, smoke and
+ * temperature, as the reference's AdvectedField.swap does. */
+int plume_step(const PlumeStepState* state, const PlumeStepParams* params, void* stream);
+
+/* ---- render ------------------------------------------------------------------------------------------ */
+
+/* light_volume.py:18-51 light_volume_kernel. */
+int plume_light_volume(const int32_t shape[3], const float* smoke, const float toward_light[3], float cell_m,
+                       float opacity_per_density, float* light, void* stream);
+
+/* normal_field.py:52-61 NormalField.compute (blur_axis_kernel x 3 + gradient_kernel); gradient is
+ * (n0, n1, n2, 3). */
+int plume_normal_field(const int32_t shape[3], const float* smoke, float* blurred, float* scratch, float* gradient,
+                       const float* weights_host, int32_t radius, void* stream);
+
+/* raymarch.py:86-140 raymarch_kernel; image is (height, width, 5). gradient/light are the unused pass's
+ * 1-cell stand-in when not read (frame_renderer.py:29-35). */
+int plume_raymarch(const PlumeGridInfo* info, const float* smoke, const float* temperature, const float* gradient,
+                   const int32_t gradient_shape[3], const float* light, const int32_t light_shape[3],
+                   const PlumeViewParams* view, const PlumeLookParams* look, float* image, int32_t height,
+                   int32_t width, void* stream);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* PLUME_B200_H */

@@ -451,7 +451,8 @@ class StepCap:
             speed = float(np.linalg.norm(vel)) if e.velocity_mode == "outward" else float(np.abs(vel).max())
             self.emitters.append((e.start_s, e.end_s, speed))
 
-    def grid_speed(self, grid: Grid) -> float:
+    @staticmethod
+    def grid_speed(grid: Grid) -> float:
         return max(grid.precision.fn("abs_max")(_shape(f.data), _ptr(f.data)) for f in grid.velocity_fields())
 
     def plan(self, grid: Grid, start_s: float, length_s: float, base_steps: int, label: str) -> int:
@@ -518,6 +519,16 @@ def domain_view_params(view) -> OView:
     params.perspective = 0
     params.eye = _d3((0.0, 0.0, 0.0))
     return params
+
+
+def light_volume(smoke: np.ndarray, toward_light_world, cell_m: float, opacity: float, precision="f32") -> np.ndarray:
+    """LightVolume.compute (light_volume.py:36-51) on a standalone smoke array."""
+    p = Precision(precision) if isinstance(precision, str) else precision
+    direction = np.asarray(toward_light_world, dtype=np.float64)
+    light = np.zeros(smoke.shape, dtype=p.dtype)
+    p.fn("light_volume")(_shape(smoke), _ptr(smoke), _d3(direction / np.linalg.norm(direction)),
+                         ctypes.c_double(cell_m), ctypes.c_double(opacity), _ptr(light))
+    return light
 
 
 def gaussian_weights(sigma: float, radius: int) -> np.ndarray:

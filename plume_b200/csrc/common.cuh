@@ -1,0 +1,178 @@
+// Device helpers shared by the sim and render kernels of libplume_b200.so (sm_100a).
+//
+// Arithmetic contract: every expression keeps the reference's order of IEEE float operations (the library is
+// compiled with -fmad=false, so no multiply-add is contracted), lerp(a, b, t) = a*(1-t) + b*t, float->int
+// conversions truncate, and min/max/clamp are plain comparisons. With that, every operator without exp/pow
+// gives the same floats as the FP32 restatement of chadmv/plume's Warp kernels. exp and pow are evaluated
+// in double and rounded once to float (within 1 ulp of the C library's expf/powf the reference calls).
+#pragma once
+
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include "../../include/plume_b200.h"
+
+namespace plume {
+
+// ---- status reporting (defined in sim.cu) -----------------------------------------------------------------
+int fail(int status, const char* fmt, ...);
+int launch_status(const char* what);                   // after a kernel launch: checks it and counts it
+int runtime_status(const char* what, cudaError_t err);  // after any other runtime call
+
+// ---- small vector type -----------------------------------------------------------------------------------
+struct F3 {
+  float c[3];
+  __host__ __device__ __forceinline__ float& operator[](int a) { return c[a]; }
+  __host__ __device__ __forceinline__ const float& operator[](int a) const { return c[a]; }
+};
+__host__ __device__ __forceinline__ F3 f3(float x, float y, float z) { return F3{{x, y, z}}; }
+__device__ __forceinline__ F3 add3(F3 a, F3 b) { return f3(a[0] + b[0], a[1] + b[1], a[2] + b[2]); }
+__device__ __forceinline__ F3 sub3(F3 a, F3 b) { return f3(a[0] - b[0], a[1] - b[1], a[2] - b[2]); }
+__device__ __forceinline__ F3 mul3(F3 a, float s) { return f3(a[0] * s, a[1] * s, a[2] * s); }
+__device__ __forceinline__ F3 div3(F3 a, float s) { return f3(a[0] / s, a[1] / s, a[2] / s); }
+__device__ __forceinline__ float dot3(F3 a, F3 b) { return a[0] * b[0] + a[1] * b[1] + a[2] * b[2]; }
+__device__ __forceinline__ float len3(F3 a) { return sqrtf(dot3(a, a)); }
+__device__ __forceinline__ F3 normalize3(F3 a) { return div3(a, len3(a)); }
+__device__ __forceinline__ F3 cross3(F3 a, F3 b) {
+  return f3(a[1] * b[2] - a[2] * b[1], a[2] * b[0] - a[0] * b[2], a[0] * b[1] - a[1] * b[0]);
+}
+__device__ __forceinline__ float fmin_(float a, float b) { return a < b ? a : b; }
+__device__ __forceinline__ float fmax_(float a, float b) { return a > b ? a : b; }
+__device__ __forceinline__ int imin_(int a, int b) { return a < b ? a : b; }
+__device__ __forceinline__ int imax_(int a, int b) { return a > b ? a : b; }
+__device__ __forceinline__ float clampf_(float x, float lo, float hi) { return x < lo ? lo : (x > hi ? hi : x); }
+__device__ __forceinline__ float lerpf_(float a, float b, float t) { return a * (1.0f - t) + b * t; }
+__device__ __forceinline__ F3 lerp3(F3 a, F3 b, float t) {
+  return f3(lerpf_(a[0], b[0], t), lerpf_(a[1], b[1], t), lerpf_(a[2], b[2], t));
+}
+__device__ __forceinline__ float exp_f(float x) { return (float)exp((double)x); }
+__device__ __forceinline__ float pow_f(float x, float y) { return (float)pow((double)x, (double)y); }
+
+// ---- arrays ------------------------------------------------------------------------------------------------
+struct Dims {
+  int n0, n1, n2;
+};
+__device__ __forceinline__ int at(const Dims& d, int i, int j, int k) { return (i * d.n1 + j) * d.n2 + k; }
+
+// Trilinear sample at continuous index g, clamped to the array (sim/sample.py:10-29).
+__device__ __forceinline__ float sample_index_space(const float* __restrict__ f, const Dims& d, F3 g) {
+  float x = clampf_(g[0], 0.0f, (float)(d.n0 - 1));
+  float y = clampf_(g[1], 0.0f, (float)(d.n1 - 1));
+  float z = clampf_(g[2], 0.0f, (float)(d.n2 - 1));
+  int i0 = (int)x, j0 = (int)y, k0 = (int)z;
+  int i1 = imin_(i0 + 1, d.n0 - 1), j1 = imin_(j0 + 1, d.n1 - 1), k1 = imin_(k0 + 1, d.n2 - 1);
+  float tx = x - (float)i0, ty = y - (float)j0, tz = z - (float)k0;
+  float c00 = lerpf_(__ldg(f + at(d, i0, j0, k0)), __ldg(f + at(d, i1, j0, k0)), tx);
+  float c10 = lerpf_(__ldg(f + at(d, i0, j1, k0)), __ldg(f + at(d, i1, j1, k0)), tx);
+  float c01 = lerpf_(__ldg(f + at(d, i0, j0, k1)), __ldg(f + at(d, i1, j0, k1)), tx);
+  float c11 = lerpf_(__ldg(f + at(d, i0, j1, k1)), __ldg(f + at(d, i1, j1, k1)), tx);
+  return lerpf_(lerpf_(c00, c10, ty), lerpf_(c01, c11, ty), tz);
+}
+
+// The value and the min/max of the eight values a trilinear sample blends (sample.py:10-50), from one set
+// of loads: MacCormack's forward pass and its clamp bounds read the same corners.
+__device__ __forceinline__ float sample_with_range(const float* __restrict__ f, const Dims& d, F3 g, float& lo,
+                                                   float& hi) {
+  float x = clampf_(g[0], 0.0f, (float)(d.n0 - 1));
+  float y = clampf_(g[1], 0.0f, (float)(d.n1 - 1));
+  float z = clampf_(g[2], 0.0f, (float)(d.n2 - 1));
+  int i0 = (int)x, j0 = (int)y, k0 = (int)z;
+  int i1 = imin_(i0 + 1, d.n0 - 1), j1 = imin_(j0 + 1, d.n1 - 1), k1 = imin_(k0 + 1, d.n2 - 1);
+  float tx = x - (float)i0, ty = y - (float)j0, tz = z - (float)k0;
+  float a000 = __ldg(f + at(d, i0, j0, k0)), a100 = __ldg(f + at(d, i1, j0, k0));
+  float a010 = __ldg(f + at(d, i0, j1, k0)), a110 = __ldg(f + at(d, i1, j1, k0));
+  float a001 = __ldg(f + at(d, i0, j0, k1)), a101 = __ldg(f + at(d, i1, j0, k1));
+  float a011 = __ldg(f + at(d, i0, j1, k1)), a111 = __ldg(f + at(d, i1, j1, k1));
+  lo = fmin_(fmin_(fmin_(fmin_(fmin_(fmin_(fmin_(a000, a000), a001), a010), a011), a100), a101), a110);
+  lo = fmin_(lo, a111);
+  hi = fmax_(fmax_(fmax_(fmax_(fmax_(fmax_(fmax_(a000, a000), a001), a010), a011), a100), a101), a110);
+  hi = fmax_(hi, a111);
+  float c00 = lerpf_(a000, a100, tx), c10 = lerpf_(a010, a110, tx);
+  float c01 = lerpf_(a001, a101, tx), c11 = lerpf_(a011, a111, tx);
+  return lerpf_(lerpf_(c00, c10, ty), lerpf_(c01, c11, ty), tz);
+}
+
+__device__ __forceinline__ bool is_outside_open_face(F3 p, const PlumeGridInfo& info) {  // sample.py:53-61
+#pragma unroll
+  for (int a = 0; a < 3; ++a) {
+    if (p[a] < 0.0f && info.open_lo[a] == 1) return true;
+    if (p[a] > (float)info.dims[a] && info.open_hi[a] == 1) return true;
+  }
+  return false;
+}
+
+struct Vel {
+  const float* __restrict__ u;
+  const float* __restrict__ v;
+  const float* __restrict__ w;
+  Dims du, dv, dw;
+};
+
+__host__ __device__ __forceinline__ Vel make_vel(const float* u, const float* v, const float* w, const int* dims) {
+  Vel r;
+  r.u = u;
+  r.v = v;
+  r.w = w;
+  r.du = Dims{dims[0] + 1, dims[1], dims[2]};
+  r.dv = Dims{dims[0], dims[1] + 1, dims[2]};
+  r.dw = Dims{dims[0], dims[1], dims[2] + 1};
+  return r;
+}
+
+__device__ __forceinline__ F3 velocity_at(const Vel& vel, F3 p) {  // sample.py:74-82
+  return f3(sample_index_space(vel.u, vel.du, sub3(p, f3(0.0f, 0.5f, 0.5f))),
+            sample_index_space(vel.v, vel.dv, sub3(p, f3(0.5f, 0.0f, 0.5f))),
+            sample_index_space(vel.w, vel.dw, sub3(p, f3(0.5f, 0.5f, 0.0f))));
+}
+
+// Midpoint backtrace (advect.py:16-21); a negative dt_over_cell traces forward.
+__device__ __forceinline__ F3 trace(const Vel& vel, F3 p, float dt_over_cell) {
+  F3 mid = sub3(p, mul3(velocity_at(vel, p), 0.5f * dt_over_cell));
+  return sub3(p, mul3(velocity_at(vel, mid), dt_over_cell));
+}
+
+// ---- value noise (sim/noise.py) ----------------------------------------------------------------------------
+constexpr uint32_t LATTICE_OFFSET = 1048576u;
+
+__device__ __forceinline__ uint32_t hash_u32(uint32_t x) {  // lowbias32 (noise.py:13-21)
+  x ^= x >> 16;
+  x *= 0x7FEB352Du;
+  x ^= x >> 15;
+  x *= 0x846CA68Bu;
+  x ^= x >> 16;
+  return x;
+}
+
+__device__ __forceinline__ float lattice_value(int seed, int stream, int i, int j, int k) {  // noise.py:24-32
+  uint32_t h = hash_u32((uint32_t)seed + LATTICE_OFFSET);
+  h = hash_u32(h ^ ((uint32_t)stream + LATTICE_OFFSET));
+  h = hash_u32(h ^ ((uint32_t)i + LATTICE_OFFSET));
+  h = hash_u32(h ^ ((uint32_t)j + LATTICE_OFFSET));
+  h = hash_u32(h ^ ((uint32_t)k + LATTICE_OFFSET));
+  const float scale = 2.0f / 16777215.0f;
+  return (float)(h >> 8) * scale - 1.0f;
+}
+
+__device__ __forceinline__ float fade(float t) { return t * t * (3.0f - 2.0f * t); }
+
+__device__ __forceinline__ float value_noise(int seed, int stream, F3 p) {  // noise.py:40-57
+  float fx = floorf(p[0]), fy = floorf(p[1]), fz = floorf(p[2]);
+  int i = (int)fx, j = (int)fy, k = (int)fz;
+  float tx = fade(p[0] - fx), ty = fade(p[1] - fy), tz = fade(p[2] - fz);
+  float c00 = lerpf_(lattice_value(seed, stream, i, j, k), lattice_value(seed, stream, i + 1, j, k), tx);
+  float c10 = lerpf_(lattice_value(seed, stream, i, j + 1, k), lattice_value(seed, stream, i + 1, j + 1, k), tx);
+  float c01 = lerpf_(lattice_value(seed, stream, i, j, k + 1), lattice_value(seed, stream, i + 1, j, k + 1), tx);
+  float c11 = lerpf_(lattice_value(seed, stream, i, j + 1, k + 1),
+                     lattice_value(seed, stream, i + 1, j + 1, k + 1), tx);
+  return lerpf_(lerpf_(c00, c10, ty), lerpf_(c01, c11, ty), tz);
+}
+
+// ---- launch geometry ---------------------------------------------------------------------------------------
+// Cell-parallel kernels use 256-thread blocks of 32 (z, the contiguous axis) x 8 (y), one x-slice per z-block.
+constexpr int TZ = 32, TY = 8;
+inline dim3 cell_grid(int n0, int n1, int n2) { return dim3((n2 + TZ - 1) / TZ, (n1 + TY - 1) / TY, n0); }
+inline dim3 cell_block() { return dim3(TZ, TY, 1); }
+
+inline cudaStream_t as_stream(void* s) { return reinterpret_cast<cudaStream_t>(s); }
+
+}  // namespace plume

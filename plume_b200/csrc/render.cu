@@ -1,0 +1,245 @@
+// Volume-render kernels of libplume_b200.so for sm_100a: the light volume (shadow march), the normal field
+// and the camera ray march of chadmv/plume (src/plume/render/*), with their C ABI.
+#include <algorithm>
+
+#include "common.cuh"
+
+namespace plume {
+
+__device__ __forceinline__ void slab_range(F3 origin, F3 dir, F3 bmin, F3 bmax, float& t0out, float& t1out) {
+  float t_enter = -1.0e30f, t_exit = 1.0e30f;  // raymarch.py:55-69
+#pragma unroll
+  for (int a = 0; a < 3; ++a) {
+    if (fabsf(dir[a]) < 1.0e-12f) {
+      if (origin[a] < bmin[a] || origin[a] > bmax[a]) {
+        t0out = 1.0f;
+        t1out = 0.0f;
+        return;
+      }
+    } else {
+      float t0 = (bmin[a] - origin[a]) / dir[a];
+      float t1 = (bmax[a] - origin[a]) / dir[a];
+      t_enter = fmax_(t_enter, fmin_(t0, t1));
+      t_exit = fmin_(t_exit, fmax_(t0, t1));
+    }
+  }
+  t0out = t_enter;
+  t1out = t_exit;
+}
+
+// light_volume_kernel (light_volume.py:18-33): one thread per cell marches toward the light in at most
+// half-cell steps to the box edge and writes exp(-opacity * column * cell_m).
+__global__ void k_light_volume(Dims d, const float* __restrict__ smoke, F3 toward, float cell_m, float opacity,
+                               float* __restrict__ light) {
+  const int i = blockIdx.z, j = blockIdx.y * blockDim.y + threadIdx.y, k = blockIdx.x * blockDim.x + threadIdx.x;
+  if (j >= d.n1 || k >= d.n2) return;
+  const F3 half = f3(0.5f, 0.5f, 0.5f);
+  F3 start = add3(f3((float)i, (float)j, (float)k), half);
+  F3 box_max = f3((float)d.n0, (float)d.n1, (float)d.n2);
+  float t0, length;
+  slab_range(start, toward, f3(0.0f, 0.0f, 0.0f), box_max, t0, length);
+  int steps = (int)ceilf(length / 0.5f);
+  float column = 0.0f;
+  if (steps > 0) {
+    float step = length / (float)steps;
+    for (int s = 0; s < steps; ++s) {
+      F3 position = add3(start, mul3(toward, ((float)s + 0.5f) * step));
+      column = column + fmax_(sample_index_space(smoke, d, sub3(position, half)), 0.0f) * step;
+    }
+  }
+  light[at(d, i, j, k)] = exp_f(-opacity * column * cell_m);
+}
+
+// blur_axis_kernel (normal_field.py:12-22); weights in constant memory.
+constexpr int MAX_BLUR_TAPS = 129;
+__constant__ float c_weights[MAX_BLUR_TAPS];
+
+__global__ void k_blur_axis(Dims d, const float* __restrict__ src, float* __restrict__ dst, int radius, int axis) {
+  const int i = blockIdx.z, j = blockIdx.y * blockDim.y + threadIdx.y, k = blockIdx.x * blockDim.x + threadIdx.x;
+  if (j >= d.n1 || k >= d.n2) return;
+  const int cell[3] = {i, j, k};
+  const int n[3] = {d.n0, d.n1, d.n2};
+  float total = 0.0f;
+  for (int o = -radius; o <= radius; ++o) {
+    int c[3] = {i, j, k};
+    c[axis] = imin_(imax_(cell[axis] + o, 0), n[axis] - 1);
+    total = total + c_weights[o + radius] * __ldg(src + at(d, c[0], c[1], c[2]));
+  }
+  dst[at(d, i, j, k)] = total;
+}
+
+// gradient_kernel (normal_field.py:25-38): per-cell central differences, one-sided at the edges; AoS output.
+__global__ void k_gradient(Dims d, const float* __restrict__ src, float* __restrict__ gradient) {
+  const int i = blockIdx.z, j = blockIdx.y * blockDim.y + threadIdx.y, k = blockIdx.x * blockDim.x + threadIdx.x;
+  if (j >= d.n1 || k >= d.n2) return;
+  const int cell[3] = {i, j, k};
+  const int n[3] = {d.n0, d.n1, d.n2};
+  float r[3] = {0.0f, 0.0f, 0.0f};
+#pragma unroll
+  for (int a = 0; a < 3; ++a) {
+    int lo[3] = {i, j, k}, hi[3] = {i, j, k};
+    lo[a] = imax_(cell[a] - 1, 0);
+    hi[a] = imin_(cell[a] + 1, n[a] - 1);
+    float span = (float)(hi[a] - lo[a]);
+    if (span > 0.0f) r[a] = (__ldg(src + at(d, hi[0], hi[1], hi[2])) - __ldg(src + at(d, lo[0], lo[1], lo[2]))) / span;
+  }
+  float* out = gradient + (size_t)at(d, i, j, k) * 3;
+  out[0] = r[0];
+  out[1] = r[1];
+  out[2] = r[2];
+}
+
+__device__ __forceinline__ F3 sample_vec(const float* __restrict__ f, const Dims& d, F3 g) {
+  float x = clampf_(g[0], 0.0f, (float)(d.n0 - 1));
+  float y = clampf_(g[1], 0.0f, (float)(d.n1 - 1));
+  float z = clampf_(g[2], 0.0f, (float)(d.n2 - 1));
+  int i0 = (int)x, j0 = (int)y, k0 = (int)z;
+  int i1 = imin_(i0 + 1, d.n0 - 1), j1 = imin_(j0 + 1, d.n1 - 1), k1 = imin_(k0 + 1, d.n2 - 1);
+  float tx = x - (float)i0, ty = y - (float)j0, tz = z - (float)k0;
+  auto ld = [&](int i, int j, int k) {
+    const float* q = f + (size_t)at(d, i, j, k) * 3;
+    return f3(__ldg(q), __ldg(q + 1), __ldg(q + 2));
+  };
+  F3 c00 = lerp3(ld(i0, j0, k0), ld(i1, j0, k0), tx);
+  F3 c10 = lerp3(ld(i0, j1, k0), ld(i1, j1, k0), tx);
+  F3 c01 = lerp3(ld(i0, j0, k1), ld(i1, j0, k1), tx);
+  F3 c11 = lerp3(ld(i0, j1, k1), ld(i1, j1, k1), tx);
+  return lerp3(lerp3(c00, c10, ty), lerp3(c01, c11, ty), tz);
+}
+
+struct MarchArgs {
+  PlumeGridInfo info;
+  PlumeViewParams view;
+  PlumeLookParams look;
+  Dims d, dg, dl;
+};
+
+// raymarch_kernel (raymarch.py:86-140): one thread per pixel.
+__global__ void k_raymarch(MarchArgs a, const float* __restrict__ smoke, const float* __restrict__ temperature,
+                           const float* __restrict__ gradient, const float* __restrict__ light, float* __restrict__ image,
+                           int height, int width) {
+  const int px = blockIdx.x * blockDim.x + threadIdx.x, py = blockIdx.y * blockDim.y + threadIdx.y;
+  if (px >= width || py >= height) return;
+  const PlumeViewParams& view = a.view;
+  const PlumeLookParams& look = a.look;
+  const PlumeGridInfo& info = a.info;
+  F3 right = f3(view.right[0], view.right[1], view.right[2]);
+  F3 up = f3(view.up[0], view.up[1], view.up[2]);
+  F3 toward = f3(view.toward[0], view.toward[1], view.toward[2]);
+  float plane_x = view.left_m + ((float)px + 0.5f) * view.pixel_m;  // pixel_ray (raymarch.py:72-83)
+  float plane_y = view.top_m - ((float)py + 0.5f) * view.pixel_m;
+  F3 origin = add3(add3(mul3(right, plane_x), mul3(up, plane_y)), mul3(toward, 1.0e4f));
+  F3 direction = f3(-toward[0], -toward[1], -toward[2]);
+  if (view.perspective == 1) {
+    origin = f3(view.eye[0], view.eye[1], view.eye[2]);
+    direction = normalize3(sub3(add3(mul3(right, plane_x), mul3(up, plane_y)), toward));
+  }
+  F3 box_origin = f3(info.origin_m[0], info.origin_m[1], info.origin_m[2]);
+  F3 box_max = add3(box_origin, mul3(f3((float)info.dims[0], (float)info.dims[1], (float)info.dims[2]), info.cell_m));
+  float s0, s1;
+  slab_range(origin, direction, box_origin, box_max, s0, s1);
+  if (view.perspective == 1) s0 = fmax_(s0, 0.0f);
+  float tr = 1.0f, heat = 0.0f, shade_sum = 0.0f;
+  F3 normal_sum = f3(0.0f, 0.0f, 0.0f);
+  if (s1 > s0) {
+    float length = s1 - s0;
+    int steps = (int)ceilf(length / (0.5f * info.cell_m));
+    float step_m = length / (float)steps;
+    for (int s = 0; s < steps; ++s) {
+      F3 position = add3(origin, mul3(direction, s0 + ((float)s + 0.5f) * step_m));
+      F3 g = sub3(div3(sub3(position, box_origin), info.cell_m), f3(0.5f, 0.5f, 0.5f));
+      float density = fmax_(sample_index_space(smoke, a.d, g), 0.0f);
+      float alpha = 1.0f - exp_f(-look.opacity_per_density * density * step_m);
+      float glow = fmax_(sample_index_space(temperature, a.d, g) - look.glow_start_k, 0.0f);
+      heat = heat + glow * step_m * pow_f(tr, look.smoke_hides_heat);
+      if (look.shade_layout == 1) {
+        float lit = look.shade_fill + (1.0f - look.shade_fill) * sample_index_space(light, a.dl, g);
+        shade_sum = shade_sum + tr * alpha * lit;
+      } else {
+        F3 slope = sample_vec(gradient, a.dg, g);
+        if (alpha > 0.0f && len3(slope) > 1.0e-9f) normal_sum = sub3(normal_sum, mul3(normalize3(slope), tr * alpha));
+      }
+      tr = tr * (1.0f - alpha);
+    }
+  }
+  float thickness = 1.0f - tr;
+  float* out = image + ((size_t)py * width + px) * 5;
+  out[0] = heat;
+  out[1] = thickness;
+  if (look.shade_layout == 1) {
+    out[2] = shade_sum;
+    out[3] = 0.0f;
+    out[4] = 0.0f;
+    return;
+  }
+  F3 facing = f3(0.0f, 0.0f, 1.0f);
+  F3 normal = facing;
+  F3 cam = f3(dot3(normal_sum, right), dot3(normal_sum, up), dot3(normal_sum, toward));
+  if (len3(cam) > 1.0e-9f) {
+    normal = normalize3(cam);
+    normal = f3(normal[0], normal[1], fabsf(normal[2]));
+    float weight = clampf_(thickness / look.normal_fade_thickness, 0.0f, 1.0f);
+    normal = normalize3(lerp3(facing, normal, weight));
+  }
+  out[2] = normal[0];
+  out[3] = normal[1];
+  out[4] = normal[2];
+}
+
+static bool valid_shape(const int32_t* s) {
+  return s && s[0] >= 1 && s[1] >= 1 && s[2] >= 1 && (long long)s[0] * s[1] * s[2] * 3 < (1LL << 31);
+}
+
+}  // namespace plume
+
+using namespace plume;
+
+extern "C" int plume_light_volume(const int32_t shape[3], const float* smoke, const float toward_light[3], float cell_m,
+                                  float opacity_per_density, float* light, void* stream) {
+  if (!valid_shape(shape) || !smoke || !toward_light || !light) return fail(PLUME_ERR_INVALID, "light_volume: bad argument");
+  Dims d{shape[0], shape[1], shape[2]};
+  k_light_volume<<<cell_grid(d.n0, d.n1, d.n2), cell_block(), 0, as_stream(stream)>>>(
+      d, smoke, f3(toward_light[0], toward_light[1], toward_light[2]), cell_m, opacity_per_density, light);
+  return launch_status("light volume");
+}
+
+extern "C" int plume_normal_field(const int32_t shape[3], const float* smoke, float* blurred, float* scratch,
+                                  float* gradient, const float* weights_host, int32_t radius, void* stream) {
+  if (!valid_shape(shape) || !smoke || !blurred || !scratch || !gradient || !weights_host || radius < 0 ||
+      2 * radius + 1 > MAX_BLUR_TAPS)
+    return fail(PLUME_ERR_INVALID, "normal_field: bad argument");
+  cudaStream_t st = as_stream(stream);
+  int weights = runtime_status("blur weights", cudaMemcpyToSymbolAsync(c_weights, weights_host, sizeof(float) * (2 * radius + 1),
+                                                                      0, cudaMemcpyHostToDevice, st));
+  if (weights != PLUME_OK) return weights;
+  Dims d{shape[0], shape[1], shape[2]};
+  const float* source = smoke;
+  float* targets[3] = {blurred, scratch, blurred};
+  for (int axis = 0; axis < 3; ++axis) {
+    k_blur_axis<<<cell_grid(d.n0, d.n1, d.n2), cell_block(), 0, st>>>(d, source, targets[axis], radius, axis);
+    int status = launch_status("blur");
+    if (status != PLUME_OK) return status;
+    source = targets[axis];
+  }
+  k_gradient<<<cell_grid(d.n0, d.n1, d.n2), cell_block(), 0, st>>>(d, source, gradient);
+  return launch_status("gradient");
+}
+
+extern "C" int plume_raymarch(const PlumeGridInfo* info, const float* smoke, const float* temperature,
+                              const float* gradient, const int32_t gradient_shape[3], const float* light,
+                              const int32_t light_shape[3], const PlumeViewParams* view, const PlumeLookParams* look,
+                              float* image, int32_t height, int32_t width, void* stream) {
+  if (!info || !smoke || !temperature || !gradient || !light || !view || !look || !image || height < 1 || width < 1 ||
+      !valid_shape(info->dims) || !valid_shape(gradient_shape) || !valid_shape(light_shape))
+    return fail(PLUME_ERR_INVALID, "raymarch: bad argument");
+  MarchArgs a;
+  a.info = *info;
+  a.view = *view;
+  a.look = *look;
+  a.d = Dims{info->dims[0], info->dims[1], info->dims[2]};
+  a.dg = Dims{gradient_shape[0], gradient_shape[1], gradient_shape[2]};
+  a.dl = Dims{light_shape[0], light_shape[1], light_shape[2]};
+  dim3 block(16, 16), grid((width + 15) / 16, (height + 15) / 16);
+  k_raymarch<<<grid, block, 0, as_stream(stream)>>>(a, smoke, temperature, gradient, light, image, height, width);
+  return launch_status("raymarch");
+}

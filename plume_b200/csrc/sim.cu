@@ -1,0 +1,1059 @@
+// Fluid-step kernels of libplume_b200.so for sm_100a, and their C ABI (include/plume_b200.h).
+//
+// Each kernel cites the Warp kernel(s) of chadmv/plume whose result it produces (paths relative to that
+// project). Kernels are gathers with one thread per output element, so results never depend on scheduling;
+// the only reduction (the smoke budget) adds in a fixed order.
+#include <cstdarg>
+#include <cstdio>
+#include <cstring>
+#include <string>
+#include <vector>
+
+#include "common.cuh"
+
+namespace plume {
+
+static thread_local char g_error[512] = "";
+
+int fail(int status, const char* fmt, ...) {
+  va_list args;
+  va_start(args, fmt);
+  vsnprintf(g_error, sizeof(g_error), fmt, args);
+  va_end(args);
+  return status;
+}
+
+static unsigned long long g_launches = 0;  // kernels enqueued by this library (host-side count)
+
+int launch_status(const char* what) {
+  cudaError_t err = cudaGetLastError();
+  if (err != cudaSuccess) return fail(PLUME_ERR_LAUNCH, "%s: %s", what, cudaGetErrorString(err));
+  __atomic_add_fetch(&g_launches, 1ULL, __ATOMIC_RELAXED);
+  return PLUME_OK;
+}
+
+int runtime_status(const char* what, cudaError_t err) {
+  if (err != cudaSuccess) return fail(PLUME_ERR_LAUNCH, "%s: %s", what, cudaGetErrorString(err));
+  return PLUME_OK;
+}
+
+static bool valid_dims(const int* d) {
+  if (d[0] < 1 || d[1] < 1 || d[2] < 1) return false;
+  long long n = (long long)(d[0] + 1) * (d[1] + 1) * (d[2] + 1);
+  return n < (1LL << 31);
+}
+
+#define CHECK_ARG(cond, ...) \
+  do {                       \
+    if (!(cond)) return fail(PLUME_ERR_INVALID, __VA_ARGS__); \
+  } while (0)
+
+#define CHECK_LAUNCH(what)                  \
+  do {                                      \
+    int _s = launch_status(what);           \
+    if (_s != PLUME_OK) return _s;          \
+  } while (0)
+
+// ---- emitters: sim/emitters.py -----------------------------------------------------------------------------
+
+struct EmitterSet {
+  int count;
+  PlumeEmitter e[PLUME_MAX_EMITTERS];
+};
+
+__device__ __forceinline__ F3 v3(const float* a) { return f3(a[0], a[1], a[2]); }
+
+__device__ __forceinline__ float soft_edge(float distance, float extent, float softness) {  // emitters.py:41-50
+  float inner = extent * (1.0f - softness);
+  if (distance <= inner) return 1.0f;
+  if (distance >= extent) return 0.0f;
+  float t = (distance - inner) / (extent - inner);
+  return 1.0f - t * t * (3.0f - 2.0f * t);
+}
+
+__device__ __forceinline__ float coverage(const PlumeEmitter& e, F3 x, int seed) {  // emitters.py:53-67
+  F3 offset = sub3(x, v3(e.center_m));
+  float amount = 0.0f;
+  if (e.shape == 0) {
+    amount = soft_edge(len3(offset), e.radius_m, e.edge_softness);
+  } else {
+    amount = soft_edge(fabsf(offset[0]), e.half_size_m[0], e.edge_softness) *
+             soft_edge(fabsf(offset[1]), e.half_size_m[1], e.edge_softness) *
+             soft_edge(fabsf(offset[2]), e.half_size_m[2], e.edge_softness);
+  }
+  if (amount > 0.0f && e.noise_strength > 0.0f) {
+    float breakup = 1.0f + e.noise_strength * value_noise(seed, e.stream, div3(x, e.noise_scale_m));
+    amount = amount * fmax_(breakup, 0.0f);
+  }
+  return fmin_(amount, 1.0f);
+}
+
+__device__ __forceinline__ float blend_factor(float amount, float dt) {  // emitters.py:70-77
+  const float reference = 1.0f / 80.0f;
+  return 1.0f - pow_f(1.0f - amount, dt / reference);
+}
+
+__device__ __forceinline__ F3 world_position(const PlumeGridInfo& info, F3 index) {
+  return add3(v3(info.origin_m), mul3(index, info.cell_m));
+}
+
+// emit_scalars_kernel (emitters.py:90-102) over the cells, then emit_velocity_kernel (:105-121) over the
+// three face arrays, selected by blockIdx.z segments: [0, nx) cells, then nx+1, nx, nx face slices.
+__global__ void k_emit(PlumeGridInfo info, float* __restrict__ smoke, float* __restrict__ temperature,
+                       float* __restrict__ u, float* __restrict__ v, float* __restrict__ w, EmitterSet set, int seed,
+                       float time_s, float dt) {
+  const int nx = info.dims[0], ny = info.dims[1], nz = info.dims[2];
+  int slab = blockIdx.z;
+  int part = 0;
+  if (slab >= nx) { slab -= nx; part = 1; }
+  if (part == 1 && slab >= nx + 1) { slab -= nx + 1; part = 2; }
+  if (part == 2 && slab >= nx) { slab -= nx; part = 3; }
+  const int i = slab;
+  const int j = blockIdx.y * blockDim.y + threadIdx.y;
+  const int k = blockIdx.x * blockDim.x + threadIdx.x;
+  if (part == 0) {
+    if (j >= ny || k >= nz) return;
+    F3 x = world_position(info, add3(f3((float)i, (float)j, (float)k), f3(0.5f, 0.5f, 0.5f)));
+    const int c = (i * ny + j) * nz + k;
+    for (int n = 0; n < set.count; ++n) {
+      const PlumeEmitter& e = set.e[n];
+      if (!(time_s >= e.start_s && time_s < e.end_s)) continue;
+      float amount = coverage(e, x, seed);
+      if (amount > 0.0f) {
+        smoke[c] = smoke[c] + e.smoke_per_s * amount * dt;
+        temperature[c] = lerpf_(temperature[c], e.temperature_k, blend_factor(amount, dt));
+      }
+    }
+    return;
+  }
+  const int axis = part - 1;
+  float* comp = axis == 0 ? u : (axis == 1 ? v : w);
+  const int n1 = ny + (axis == 1), n2 = nz + (axis == 2);
+  if (j >= n1 || k >= n2) return;
+  F3 offset = axis == 0 ? f3(0.0f, 0.5f, 0.5f) : (axis == 1 ? f3(0.5f, 0.0f, 0.5f) : f3(0.5f, 0.5f, 0.0f));
+  F3 x = world_position(info, add3(f3((float)i, (float)j, (float)k), offset));
+  const int c = (i * n1 + j) * n2 + k;
+  for (int n = 0; n < set.count; ++n) {
+    const PlumeEmitter& e = set.e[n];
+    if (!(time_s >= e.start_s && time_s < e.end_s)) continue;
+    float amount = coverage(e, x, seed);
+    if (amount > 0.0f) {
+      F3 target = v3(e.velocity_mps);
+      if (e.outward == 1) {
+        F3 away = sub3(x, v3(e.center_m));
+        if (len3(away) > 0.0f) target = mul3(normalize3(away), len3(v3(e.velocity_mps)));
+      }
+      comp[c] = lerpf_(comp[c], target[axis], blend_factor(amount, dt));
+    }
+  }
+}
+
+static int launch_emit(const PlumeGridInfo& info, float* smoke, float* temperature, float* u, float* v, float* w,
+                       const PlumeEmitter* emitters, int count, int seed, float time_s, float dt, cudaStream_t st) {
+  // Emitters inactive at time_s change nothing; skip them on the host (the kernel re-checks).
+  std::vector<PlumeEmitter> active;
+  for (int n = 0; n < count; ++n)
+    if (time_s >= emitters[n].start_s && time_s < emitters[n].end_s) active.push_back(emitters[n]);
+  const int nx = info.dims[0], ny = info.dims[1], nz = info.dims[2];
+  for (size_t first = 0; first < active.size(); first += PLUME_MAX_EMITTERS) {
+    EmitterSet set;
+    set.count = (int)std::min<size_t>(PLUME_MAX_EMITTERS, active.size() - first);
+    for (int n = 0; n < set.count; ++n) set.e[n] = active[first + n];
+    dim3 grid((nz + 1 + TZ - 1) / TZ, (ny + 1 + TY - 1) / TY, nx + (nx + 1) + nx + nx);
+    k_emit<<<grid, cell_block(), 0, st>>>(info, smoke, temperature, u, v, w, set, seed, time_s, dt);
+    CHECK_LAUNCH("emit");
+  }
+  return PLUME_OK;
+}
+
+// ---- buoyancy: forces.py:13-23 -----------------------------------------------------------------------------
+__global__ void k_buoyancy(PlumeGridInfo info, float* __restrict__ v, const float* __restrict__ smoke,
+                           const float* __restrict__ temperature, float gravity, float heat_buoyancy,
+                           float smoke_weight, float ambient, float dt) {
+  const int ny = info.dims[1], nz = info.dims[2];
+  const int i = blockIdx.z, j = blockIdx.y * blockDim.y + threadIdx.y, k = blockIdx.x * blockDim.x + threadIdx.x;
+  if (j > ny || k >= nz) return;
+  const int below = imax_(j - 1, 0), above = imin_(j, ny - 1);
+  const int cb = (i * ny + below) * nz + k, ca = (i * ny + above) * nz + k;
+  float heat = 0.5f * (temperature[cb] + temperature[ca]);
+  float density = 0.5f * (smoke[cb] + smoke[ca]);
+  float lift = heat_buoyancy * (heat - ambient) / ambient - smoke_weight * density;
+  const int c = (i * (ny + 1) + j) * nz + k;
+  v[c] = v[c] + gravity * lift * dt;
+}
+
+// ---- vorticity confinement: vorticity.py:17-84 -------------------------------------------------------------
+__device__ __forceinline__ F3 center_velocity(const Vel& vel, int i, int j, int k) {  // vorticity.py:17-22
+  return f3(0.5f * (__ldg(vel.u + at(vel.du, i, j, k)) + __ldg(vel.u + at(vel.du, i + 1, j, k))),
+            0.5f * (__ldg(vel.v + at(vel.dv, i, j, k)) + __ldg(vel.v + at(vel.dv, i, j + 1, k))),
+            0.5f * (__ldg(vel.w + at(vel.dw, i, j, k)) + __ldg(vel.w + at(vel.dw, i, j, k + 1))));
+}
+
+// curl_kernel (vorticity.py:38-45) with the centre velocities of center_velocity_kernel computed in place.
+__global__ void k_curl(PlumeGridInfo info, Vel vel, float* __restrict__ cx, float* __restrict__ cy,
+                       float* __restrict__ cz) {
+  const int nx = info.dims[0], ny = info.dims[1], nz = info.dims[2];
+  const int i = blockIdx.z, j = blockIdx.y * blockDim.y + threadIdx.y, k = blockIdx.x * blockDim.x + threadIdx.x;
+  if (j >= ny || k >= nz) return;
+  const int cell[3] = {i, j, k};
+  const int n[3] = {nx, ny, nz};
+  F3 d[3];
+#pragma unroll
+  for (int axis = 0; axis < 3; ++axis) {  // central_difference (vorticity.py:25-35)
+    int lo[3] = {i, j, k}, hi[3] = {i, j, k};
+    lo[axis] = imax_(cell[axis] - 1, 0);
+    hi[axis] = imin_(cell[axis] + 1, n[axis] - 1);
+    float span = (float)(hi[axis] - lo[axis]);
+    if (span == 0.0f) {
+      d[axis] = f3(0.0f, 0.0f, 0.0f);
+    } else {
+      d[axis] = div3(sub3(center_velocity(vel, hi[0], hi[1], hi[2]), center_velocity(vel, lo[0], lo[1], lo[2])),
+                     span * info.cell_m);
+    }
+  }
+  const int c = (i * ny + j) * nz + k;
+  cx[c] = d[1][2] - d[2][1];
+  cy[c] = d[2][0] - d[0][2];
+  cz[c] = d[0][1] - d[1][0];
+}
+
+__device__ __forceinline__ F3 load3(const float* __restrict__ x, const float* __restrict__ y,
+                                    const float* __restrict__ z, int c) {
+  return f3(__ldg(x + c), __ldg(y + c), __ldg(z + c));
+}
+
+// confinement_push_kernel (vorticity.py:53-71).
+__global__ void k_push(PlumeGridInfo info, const float* __restrict__ cx, const float* __restrict__ cy,
+                       const float* __restrict__ cz, float* __restrict__ px, float* __restrict__ py,
+                       float* __restrict__ pz, float strength) {
+  const int nx = info.dims[0], ny = info.dims[1], nz = info.dims[2];
+  const int i = blockIdx.z, j = blockIdx.y * blockDim.y + threadIdx.y, k = blockIdx.x * blockDim.x + threadIdx.x;
+  if (j >= ny || k >= nz) return;
+  const Dims d{nx, ny, nz};
+  const int cell[3] = {i, j, k};
+  const int n[3] = {nx, ny, nz};
+  F3 toward = f3(0.0f, 0.0f, 0.0f);
+#pragma unroll
+  for (int axis = 0; axis < 3; ++axis) {
+    int lo[3] = {i, j, k}, hi[3] = {i, j, k};
+    lo[axis] = imax_(cell[axis] - 1, 0);
+    hi[axis] = imin_(cell[axis] + 1, n[axis] - 1);
+    float span = (float)(hi[axis] - lo[axis]);
+    if (span > 0.0f) {
+      float spin_hi = len3(load3(cx, cy, cz, at(d, hi[0], hi[1], hi[2])));
+      float spin_lo = len3(load3(cx, cy, cz, at(d, lo[0], lo[1], lo[2])));
+      toward[axis] = (spin_hi - spin_lo) / (span * info.cell_m);
+    }
+  }
+  const int c = at(d, i, j, k);
+  float length = len3(toward);
+  if (length < 1.0e-12f) {
+    px[c] = 0.0f;
+    py[c] = 0.0f;
+    pz[c] = 0.0f;
+    return;
+  }
+  F3 push = mul3(cross3(div3(toward, length), load3(cx, cy, cz, c)), strength * info.cell_m);
+  px[c] = push[0];
+  py[c] = push[1];
+  pz[c] = push[2];
+}
+
+// ---- turbulence: turbulence.py:26-53 -----------------------------------------------------------------------
+constexpr int TURBULENCE_STREAM = 1 << 24;
+
+__device__ __forceinline__ float potential(int seed, int component, F3 p, float pattern_time) {
+  float slice_lo = floorf(pattern_time);
+  float blend = fade(pattern_time - slice_lo);
+  int first = TURBULENCE_STREAM + 3 * (int)slice_lo + component;
+  return lerpf_(value_noise(seed, first, p), value_noise(seed, first + 3, p), blend);
+}
+
+struct FaceForces {
+  int confinement;  // add the averaged push (add_face_push_kernel, vorticity.py:74-84)
+  const float* push[3];
+  int turbulence;   // turbulence_kernel (turbulence.py:35-53)
+  int seed;
+  float scale_m, strength, pattern_time;
+  int drag;         // drag_kernel (forces.py:34-37)
+  float wind[3];
+  float keep;
+  float dt;
+};
+
+// One pass over the three face arrays applying, per face and in the reference's order, the confinement push,
+// the turbulence push and drag. blockIdx.z segments: nx+1 u slices, nx v slices, nx w slices.
+__global__ void k_face_forces(PlumeGridInfo info, float* __restrict__ u, float* __restrict__ v,
+                              float* __restrict__ w, FaceForces ff) {
+  const int nx = info.dims[0], ny = info.dims[1], nz = info.dims[2];
+  int slab = blockIdx.z, axis = 0;
+  if (slab >= nx + 1) { slab -= nx + 1; axis = 1; }
+  if (axis == 1 && slab >= nx) { slab -= nx; axis = 2; }
+  const int i = slab, j = blockIdx.y * blockDim.y + threadIdx.y, k = blockIdx.x * blockDim.x + threadIdx.x;
+  const int n1 = ny + (axis == 1), n2 = nz + (axis == 2);
+  if (j >= n1 || k >= n2) return;
+  float* f = axis == 0 ? u : (axis == 1 ? v : w);
+  const int c = (i * n1 + j) * n2 + k;
+  float value = f[c];
+  if (ff.confinement) {
+    int below[3] = {i, j, k}, above[3] = {i, j, k};
+    below[axis] = imax_(below[axis] - 1, 0);
+    above[axis] = imin_(above[axis], info.dims[axis] - 1);
+    const Dims d{nx, ny, nz};
+    const float* p = ff.push[axis];
+    float average = 0.5f * (__ldg(p + at(d, below[0], below[1], below[2])) + __ldg(p + at(d, above[0], above[1], above[2])));
+    value = value + average * ff.dt;
+  }
+  if (ff.turbulence) {
+    F3 offset = axis == 0 ? f3(0.0f, 0.5f, 0.5f) : (axis == 1 ? f3(0.5f, 0.0f, 0.5f) : f3(0.5f, 0.5f, 0.0f));
+    F3 face = add3(f3((float)i, (float)j, (float)k), offset);
+    const int b = (axis + 1) % 3, cc = (axis + 2) % 3;
+    F3 half_b = f3(0.0f, 0.0f, 0.0f), half_c = f3(0.0f, 0.0f, 0.0f);
+    half_b[b] = 0.5f;
+    half_c[cc] = 0.5f;
+    float to_lattice = info.cell_m / ff.scale_m;
+    float c_plus = potential(ff.seed, cc, mul3(add3(face, half_b), to_lattice), ff.pattern_time);
+    float c_minus = potential(ff.seed, cc, mul3(sub3(face, half_b), to_lattice), ff.pattern_time);
+    float b_plus = potential(ff.seed, b, mul3(add3(face, half_c), to_lattice), ff.pattern_time);
+    float b_minus = potential(ff.seed, b, mul3(sub3(face, half_c), to_lattice), ff.pattern_time);
+    float curl = ((c_plus - c_minus) - (b_plus - b_minus)) / to_lattice;
+    value = value + ff.strength * curl * ff.dt;
+  }
+  if (ff.drag) value = ff.wind[axis] + (value - ff.wind[axis]) * ff.keep;
+  f[c] = value;
+}
+
+static dim3 face_grid(const PlumeGridInfo& info) {
+  const int nx = info.dims[0], ny = info.dims[1], nz = info.dims[2];
+  return dim3((nz + 1 + TZ - 1) / TZ, (ny + 1 + TY - 1) / TY, (nx + 1) + nx + nx);
+}
+
+static int launch_confinement_push(const PlumeGridInfo& info, const float* u, const float* v, const float* w,
+                                   float* const curl[3], float* const push[3], float strength, int apply,
+                                   cudaStream_t st) {
+  const int nx = info.dims[0], ny = info.dims[1], nz = info.dims[2];
+  Vel vel = make_vel(u, v, w, info.dims);
+  k_curl<<<cell_grid(nx, ny, nz), cell_block(), 0, st>>>(info, vel, curl[0], curl[1], curl[2]);
+  CHECK_LAUNCH("curl");
+  if (!apply) return PLUME_OK;
+  k_push<<<cell_grid(nx, ny, nz), cell_block(), 0, st>>>(info, curl[0], curl[1], curl[2], push[0], push[1], push[2],
+                                                         strength);
+  CHECK_LAUNCH("confinement push");
+  return PLUME_OK;
+}
+
+// ---- advection: advect.py -----------------------------------------------------------------------------------
+
+struct FieldDesc {
+  const float* data;
+  float* hat;
+  float* next;
+  Dims d;
+  F3 offset;
+  float outside;
+  int uses_outside;
+};
+
+// semi_lagrangian_kernel (advect.py:24-31) for up to three fields in one launch (blockIdx.z segments).
+struct FieldSet {
+  FieldDesc f[3];
+  int count;
+};
+
+__device__ __forceinline__ int pick_field(const FieldSet& set, int& slab) {
+  int which = 0;
+  while (which + 1 < set.count && slab >= set.f[which].d.n0) {
+    slab -= set.f[which].d.n0;
+    ++which;
+  }
+  return which;
+}
+
+__global__ void k_semi_lagrangian(PlumeGridInfo info, Vel vel, FieldSet set, float dt_over_cell, int write_next) {
+  int slab = blockIdx.z;
+  const FieldDesc& fd = set.f[pick_field(set, slab)];
+  const int i = slab, j = blockIdx.y * blockDim.y + threadIdx.y, k = blockIdx.x * blockDim.x + threadIdx.x;
+  if (j >= fd.d.n1 || k >= fd.d.n2) return;
+  F3 p = add3(f3((float)i, (float)j, (float)k), fd.offset);
+  F3 src = trace(vel, p, dt_over_cell);
+  float value;
+  if (fd.uses_outside == 1 && is_outside_open_face(src, info)) value = fd.outside;
+  else value = sample_index_space(fd.data, fd.d, sub3(src, fd.offset));
+  (write_next ? fd.next : fd.hat)[at(fd.d, i, j, k)] = value;
+}
+
+// maccormack_correct_kernel (advect.py:34-50) with the backward pass (advect.py:64) evaluated in place:
+// back = sample(hat, trace(p, -dt)) at this element, then the clamp to the range at the forward trace.
+__global__ void k_maccormack(PlumeGridInfo info, Vel vel, FieldSet set, float dt_over_cell) {
+  int slab = blockIdx.z;
+  const FieldDesc& fd = set.f[pick_field(set, slab)];
+  const int i = slab, j = blockIdx.y * blockDim.y + threadIdx.y, k = blockIdx.x * blockDim.x + threadIdx.x;
+  if (j >= fd.d.n1 || k >= fd.d.n2) return;
+  const int c = at(fd.d, i, j, k);
+  F3 p = add3(f3((float)i, (float)j, (float)k), fd.offset);
+  F3 back_src = trace(vel, p, -dt_over_cell);
+  float back;
+  if (fd.uses_outside == 1 && is_outside_open_face(back_src, info)) back = fd.outside;
+  else back = sample_index_space(fd.hat, fd.d, sub3(back_src, fd.offset));
+  float corrected = __ldg(fd.hat + c) + 0.5f * (__ldg(fd.data + c) - back);
+  F3 source = trace(vel, p, dt_over_cell);
+  float lo = fd.outside, hi = fd.outside;
+  if (fd.uses_outside == 0 || !is_outside_open_face(source, info)) {
+    sample_with_range(fd.data, fd.d, sub3(source, fd.offset), lo, hi);
+  }
+  fd.next[c] = clampf_(corrected, lo, hi);
+}
+
+static int launch_advect(const PlumeGridInfo& info, const Vel& vel, const FieldSet& set, float dt_over_cell,
+                         bool maccormack, cudaStream_t st) {
+  int slabs = 0, n1 = 0, n2 = 0;
+  for (int n = 0; n < set.count; ++n) {
+    slabs += set.f[n].d.n0;
+    n1 = std::max(n1, set.f[n].d.n1);
+    n2 = std::max(n2, set.f[n].d.n2);
+  }
+  dim3 grid((n2 + TZ - 1) / TZ, (n1 + TY - 1) / TY, slabs);
+  if (!maccormack) {
+    k_semi_lagrangian<<<grid, cell_block(), 0, st>>>(info, vel, set, dt_over_cell, 1);
+    CHECK_LAUNCH("semi-Lagrangian advection");
+    return PLUME_OK;
+  }
+  k_semi_lagrangian<<<grid, cell_block(), 0, st>>>(info, vel, set, dt_over_cell, 0);
+  CHECK_LAUNCH("MacCormack forward pass");
+  k_maccormack<<<grid, cell_block(), 0, st>>>(info, vel, set, dt_over_cell);
+  CHECK_LAUNCH("MacCormack correction");
+  return PLUME_OK;
+}
+
+// ---- pressure: pressure.py ----------------------------------------------------------------------------------
+
+// zero_closed_faces_kernel (pressure.py:21-28) on the two boundary planes of each face array.
+__global__ void k_zero_walls(PlumeGridInfo info, float* __restrict__ u, float* __restrict__ v, float* __restrict__ w) {
+  const int nx = info.dims[0], ny = info.dims[1], nz = info.dims[2];
+  const int axis = blockIdx.z / 2, side = blockIdx.z % 2;
+  const bool closed = side == 0 ? info.open_lo[axis] == 0 : info.open_hi[axis] == 0;
+  if (!closed) return;
+  const int a = blockIdx.y * blockDim.y + threadIdx.y, b = blockIdx.x * blockDim.x + threadIdx.x;
+  const int plane = side == 0 ? 0 : info.dims[axis];
+  if (axis == 0) {
+    if (a < ny && b < nz) u[(plane * ny + a) * nz + b] = 0.0f;
+  } else if (axis == 1) {
+    if (a < nx && b < nz) v[(a * (ny + 1) + plane) * nz + b] = 0.0f;
+  } else {
+    if (a < nx && b < ny) w[(a * ny + b) * (nz + 1) + plane] = 0.0f;
+  }
+}
+
+__global__ void k_divergence(PlumeGridInfo info, const float* __restrict__ u, const float* __restrict__ v,
+                             const float* __restrict__ w, float* __restrict__ div) {  // pressure.py:31-36
+  const int ny = info.dims[1], nz = info.dims[2];
+  const int i = blockIdx.z, j = blockIdx.y * blockDim.y + threadIdx.y, k = blockIdx.x * blockDim.x + threadIdx.x;
+  if (j >= ny || k >= nz) return;
+  float flux = (__ldg(u + ((i + 1) * ny + j) * nz + k) - __ldg(u + (i * ny + j) * nz + k)) +
+               (__ldg(v + (i * (ny + 1) + j + 1) * nz + k) - __ldg(v + (i * (ny + 1) + j) * nz + k)) +
+               (__ldg(w + (i * ny + j) * (nz + 1) + k + 1) - __ldg(w + (i * ny + j) * (nz + 1) + k));
+  div[(i * ny + j) * nz + k] = flux / info.cell_m;
+}
+
+// subtract_gradient_kernel (pressure.py:95-116) over the three face arrays (blockIdx.z segments).
+__global__ void k_subtract_gradient(PlumeGridInfo info, float* __restrict__ u, float* __restrict__ v,
+                                    float* __restrict__ w, const float* __restrict__ q) {
+  const int nx = info.dims[0], ny = info.dims[1], nz = info.dims[2];
+  int slab = blockIdx.z, axis = 0;
+  if (slab >= nx + 1) { slab -= nx + 1; axis = 1; }
+  if (axis == 1 && slab >= nx) { slab -= nx; axis = 2; }
+  const int i = slab, j = blockIdx.y * blockDim.y + threadIdx.y, k = blockIdx.x * blockDim.x + threadIdx.x;
+  const int n1 = ny + (axis == 1), n2 = nz + (axis == 2);
+  if (j >= n1 || k >= n2) return;
+  float* f = axis == 0 ? u : (axis == 1 ? v : w);
+  const int face[3] = {i, j, k};
+  const int index = face[axis];
+  int below[3] = {i, j, k};
+  below[axis] = index - 1;
+  const Dims d{nx, ny, nz};
+  float q_above = 0.0f, q_below = 0.0f;
+  if (index == 0) {
+    if (info.open_lo[axis] == 0) return;
+    q_above = __ldg(q + at(d, i, j, k));
+  } else if (index == info.dims[axis]) {
+    if (info.open_hi[axis] == 0) return;
+    q_below = __ldg(q + at(d, below[0], below[1], below[2]));
+  } else {
+    q_above = __ldg(q + at(d, i, j, k));
+    q_below = __ldg(q + at(d, below[0], below[1], below[2]));
+  }
+  const int c = (i * n1 + j) * n2 + k;
+  f[c] = f[c] - (q_above - q_below) / info.cell_m;
+}
+
+// ---- the variable-coefficient Poisson stencil (pressure.py:39-77) -------------------------------------------
+
+__device__ __forceinline__ float cell_fill(const PlumeGridInfo& info, int axis, int index) {
+  return index == info.dims[axis] - 1 ? info.fill_hi[axis] : 1.0f;
+}
+
+// q is read with ordinary loads: the red-black kernel writes other cells of the same array.
+__device__ __forceinline__ void neighbor_sum(const float* q, const PlumeGridInfo& info, const int c[3],
+                                             float& sq, float& sc) {
+  sq = 0.0f;
+  sc = 0.0f;
+  const Dims d{info.dims[0], info.dims[1], info.dims[2]};
+#pragma unroll
+  for (int axis = 0; axis < 3; ++axis) {
+    float area = 1.0f;
+#pragma unroll
+    for (int other = 0; other < 3; ++other)
+      if (other != axis) area = area * cell_fill(info, other, c[other]);
+    const float own = cell_fill(info, axis, c[axis]);
+    float tq[2], tc[2];
+#pragma unroll
+    for (int side = 0; side < 2; ++side) {
+      const int step = side == 0 ? -1 : 1;
+      int n[3] = {c[0], c[1], c[2]};
+      n[axis] = n[axis] + step;
+      if (n[axis] >= 0 && n[axis] < info.dims[axis]) {
+        float coupling = area / (0.5f * (own + cell_fill(info, axis, n[axis])));
+        tq[side] = coupling * q[at(d, n[0], n[1], n[2])];
+        tc[side] = coupling;
+      } else if ((step < 0 && info.open_lo[axis] == 1) || (step > 0 && info.open_hi[axis] == 1)) {
+        tq[side] = 0.0f;
+        tc[side] = area / (0.5f * own + info.ghost_gap);
+      } else {
+        tq[side] = 0.0f;
+        tc[side] = 0.0f;
+      }
+    }
+    sq = (sq + tq[0]) + tq[1];
+    sc = (sc + tc[0]) + tc[1];
+  }
+}
+
+__device__ __forceinline__ float cell_volume(const PlumeGridInfo& info, const int c[3]) {
+  return cell_fill(info, 0, c[0]) * cell_fill(info, 1, c[1]) * cell_fill(info, 2, c[2]);
+}
+
+// red_black_sweep_kernel (pressure.py:80-92): one colour; each thread owns one cell of that colour.
+__global__ void k_red_black(PlumeGridInfo info, float* q, const float* __restrict__ rhs, int color, float relaxation) {
+  const int ny = info.dims[1], nz = info.dims[2];
+  const int i = blockIdx.z, j = blockIdx.y * blockDim.y + threadIdx.y;
+  const int kk = blockIdx.x * blockDim.x + threadIdx.x;
+  const int k = 2 * kk + ((i + j + color) & 1);
+  if (j >= ny || k >= nz) return;
+  const int c[3] = {i, j, k};
+  float sq, sc;
+  neighbor_sum(q, info, c, sq, sc);
+  if (sc == 0.0f) return;
+  const int idx = (i * ny + j) * nz + k;
+  float source = cell_volume(info, c) * info.cell_m * info.cell_m * __ldg(rhs + idx);
+  float target = (sq - source) / sc;
+  q[idx] = q[idx] + relaxation * (target - q[idx]);
+}
+
+__global__ void k_residual(PlumeGridInfo info, const float* __restrict__ q, const float* __restrict__ rhs,
+                           float* __restrict__ res) {  // multigrid.py:36-43
+  const int ny = info.dims[1], nz = info.dims[2];
+  const int i = blockIdx.z, j = blockIdx.y * blockDim.y + threadIdx.y, k = blockIdx.x * blockDim.x + threadIdx.x;
+  if (j >= ny || k >= nz) return;
+  const int c[3] = {i, j, k};
+  float sq, sc;
+  neighbor_sum(q, info, c, sq, sc);
+  float scale = cell_volume(info, c) * info.cell_m * info.cell_m;
+  const int idx = (i * ny + j) * nz + k;
+  res[idx] = __ldg(rhs + idx) - (sq - sc * __ldg(q + idx)) / scale;
+}
+
+__global__ void k_restrict(Dims fine, Dims coarse, const float* __restrict__ f, float* __restrict__ out) {
+  const int i = blockIdx.z, j = blockIdx.y * blockDim.y + threadIdx.y, k = blockIdx.x * blockDim.x + threadIdx.x;
+  if (j >= coarse.n1 || k >= coarse.n2) return;  // multigrid.py:46-60
+  float total = 0.0f, count = 0.0f;
+#pragma unroll
+  for (int di = 0; di < 2; ++di)
+#pragma unroll
+    for (int dj = 0; dj < 2; ++dj)
+#pragma unroll
+      for (int dk = 0; dk < 2; ++dk) {
+        const int fi = 2 * i + di, fj = 2 * j + dj, fk = 2 * k + dk;
+        if (fi < fine.n0 && fj < fine.n1 && fk < fine.n2) {
+          total = total + __ldg(f + at(fine, fi, fj, fk));
+          count = count + 1.0f;
+        }
+      }
+  out[at(coarse, i, j, k)] = total / count;
+}
+
+__global__ void k_prolong_add(Dims coarse, Dims fine, const float* __restrict__ cq, float* __restrict__ q) {
+  const int i = blockIdx.z, j = blockIdx.y * blockDim.y + threadIdx.y, k = blockIdx.x * blockDim.x + threadIdx.x;
+  if (j >= fine.n1 || k >= fine.n2) return;  // multigrid.py:63-68
+  F3 g = sub3(mul3(f3((float)i, (float)j, (float)k), 0.5f), f3(0.25f, 0.25f, 0.25f));
+  const int idx = at(fine, i, j, k);
+  q[idx] = q[idx] + sample_index_space(cq, coarse, g);
+}
+
+static int red_black_sweeps(const PlumeGridInfo& info, float* q, const float* rhs, int sweeps, float relaxation,
+                            cudaStream_t st) {
+  const int nx = info.dims[0], ny = info.dims[1], nz = info.dims[2];
+  dim3 grid(((nz + 1) / 2 + TZ - 1) / TZ, (ny + TY - 1) / TY, nx);
+  for (int s = 0; s < sweeps; ++s)
+    for (int color = 0; color < 2; ++color) {
+      k_red_black<<<grid, cell_block(), 0, st>>>(info, q, rhs, color, relaxation);
+      CHECK_LAUNCH("red-black sweep");
+    }
+  return PLUME_OK;
+}
+
+constexpr int COARSEST_SWEEPS = 20;  // multigrid.py:24-33
+constexpr int COARSEST_SWEEPS_PER_CELL = 4;
+
+static Dims dims_of(const PlumeGridInfo& info) { return Dims{info.dims[0], info.dims[1], info.dims[2]}; }
+
+static int v_cycle(const PlumeLevel* levels, int count, int index, int sweeps, cudaStream_t st) {  // multigrid.py:130-147
+  const PlumeLevel& lv = levels[index];
+  int status;
+  if (index == count - 1) {
+    int longest = std::max(lv.info.dims[0], std::max(lv.info.dims[1], lv.info.dims[2]));
+    return red_black_sweeps(lv.info, lv.q, lv.rhs, std::max(COARSEST_SWEEPS, COARSEST_SWEEPS_PER_CELL * longest),
+                            1.5f, st);
+  }
+  if ((status = red_black_sweeps(lv.info, lv.q, lv.rhs, sweeps, 1.0f, st)) != PLUME_OK) return status;
+  const Dims fd = dims_of(lv.info);
+  k_residual<<<cell_grid(fd.n0, fd.n1, fd.n2), cell_block(), 0, st>>>(lv.info, lv.q, lv.rhs, lv.residual);
+  CHECK_LAUNCH("residual");
+  const PlumeLevel& coarse = levels[index + 1];
+  const Dims cd = dims_of(coarse.info);
+  k_restrict<<<cell_grid(cd.n0, cd.n1, cd.n2), cell_block(), 0, st>>>(fd, cd, lv.residual, coarse.rhs);
+  CHECK_LAUNCH("restrict");
+  if ((status = runtime_status("zero coarse pressure",
+                               cudaMemsetAsync(coarse.q, 0, sizeof(float) * (size_t)cd.n0 * cd.n1 * cd.n2, st))) !=
+      PLUME_OK)
+    return status;
+  if ((status = v_cycle(levels, count, index + 1, sweeps, st)) != PLUME_OK) return status;
+  k_prolong_add<<<cell_grid(fd.n0, fd.n1, fd.n2), cell_block(), 0, st>>>(cd, fd, coarse.q, lv.q);
+  CHECK_LAUNCH("prolong");
+  return red_black_sweeps(lv.info, lv.q, lv.rhs, sweeps, 1.0f, st);
+}
+
+// ---- smoke budget: conserve.py:33-52 + reduce.py:12-38 ------------------------------------------------------
+// Line totals along x in float (reduce.py:12-25); lines added in double in blocks of 256 by a halving tree,
+// then the block partials in order on one thread. The CPU oracle adds in the same order.
+constexpr int SUM_BLOCK = 256;
+
+__global__ void k_line_partials(Dims d, const float* __restrict__ a, const float* __restrict__ b,
+                                const float* __restrict__ c, double* __restrict__ partial, int blocks) {
+  __shared__ double slot[SUM_BLOCK];
+  const float* src = blockIdx.y == 0 ? a : (blockIdx.y == 1 ? b : c);
+  const long line = (long)blockIdx.x * SUM_BLOCK + threadIdx.x;
+  const long lines = (long)d.n1 * d.n2;
+  double value = 0.0;
+  if (line < lines) {
+    float total = 0.0f;
+    for (int i = 0; i < d.n0; ++i) total = total + __ldg(src + (long)i * lines + line);
+    value = (double)total;
+  }
+  slot[threadIdx.x] = value;
+  __syncthreads();
+  for (int h = SUM_BLOCK / 2; h >= 1; h >>= 1) {
+    if ((int)threadIdx.x < h) slot[threadIdx.x] = slot[threadIdx.x] + slot[threadIdx.x + h];
+    __syncthreads();
+  }
+  if (threadIdx.x == 0) partial[blockIdx.y * blocks + blockIdx.x] = slot[0];
+}
+
+// totals[0..2] = before, semi-Lagrangian, MacCormack; factor = held / MacCormack (1 when MacCormack <= 0).
+__global__ void k_budget_factor(const double* __restrict__ partial, int blocks, float* factor, double* totals_out,
+                                int want_factor) {
+  if (threadIdx.x != 0 || blockIdx.x != 0) return;
+  double t[3];
+  for (int which = 0; which < 3; ++which) {
+    double total = 0.0;
+    for (int b = 0; b < blocks; ++b) total = total + partial[which * blocks + b];
+    t[which] = total;
+  }
+  if (totals_out) {
+    totals_out[0] = t[0];
+    totals_out[1] = t[1];
+    totals_out[2] = t[2];
+  }
+  if (!want_factor) return;
+  const double before = t[0], sl = t[1], mc = t[2];
+  const double held = sl > (mc < before ? mc : before) ? sl : (mc < before ? mc : before);
+  *factor = mc > 0.0 ? (float)(held / mc) : 1.0f;
+}
+
+__global__ void k_scale(float* __restrict__ f, long n, const float* __restrict__ factor) {  // conserve.py:27-30
+  const float s = *factor;
+  for (long idx = (long)blockIdx.x * blockDim.x + threadIdx.x; idx < n; idx += (long)gridDim.x * blockDim.x)
+    f[idx] = f[idx] * s;
+}
+
+static int sum_blocks(const Dims& d) { return (int)(((long)d.n1 * d.n2 + SUM_BLOCK - 1) / SUM_BLOCK); }
+
+static int launch_triple_sum(const Dims& d, const float* a, const float* b, const float* c, double* sums,
+                             float* factor, double* totals_out, cudaStream_t st) {
+  const int blocks = sum_blocks(d);
+  k_line_partials<<<dim3(blocks, 3), SUM_BLOCK, 0, st>>>(d, a, b, c, sums, blocks);
+  CHECK_LAUNCH("line sums");
+  k_budget_factor<<<1, 32, 0, st>>>(sums, blocks, factor, totals_out, factor != nullptr);
+  CHECK_LAUNCH("budget factor");
+  return PLUME_OK;
+}
+
+static int grid_stride_blocks(long n) {
+  long b = (n + 255) / 256;
+  return (int)std::min<long>(b, 148L * 16);
+}
+
+// ---- the scalar epilogue: conserve scale + dissipation (conserve.py:50-52, dissipate.py:10-15) -------------
+__global__ void k_scalar_finish(float* __restrict__ smoke, float* __restrict__ temperature, long n,
+                                const float* __restrict__ factor, int dissipate, float smoke_keep, float heat_keep,
+                                float ambient) {
+  const float s = *factor;
+  for (long idx = (long)blockIdx.x * blockDim.x + threadIdx.x; idx < n; idx += (long)gridDim.x * blockDim.x) {
+    float value = smoke[idx] * s;
+    if (dissipate) {
+      value = value * smoke_keep;
+      temperature[idx] = ambient + (temperature[idx] - ambient) * heat_keep;
+    }
+    smoke[idx] = value;
+  }
+}
+
+__global__ void k_dissipate(float* __restrict__ smoke, float* __restrict__ temperature, long n, float smoke_keep,
+                            float heat_keep, float ambient) {  // dissipate.py:10-15
+  for (long idx = (long)blockIdx.x * blockDim.x + threadIdx.x; idx < n; idx += (long)gridDim.x * blockDim.x) {
+    smoke[idx] = smoke[idx] * smoke_keep;
+    temperature[idx] = ambient + (temperature[idx] - ambient) * heat_keep;
+  }
+}
+
+// ---- grid speed: step_cap.py:50-55 (max is exact in any order) ----------------------------------------------
+__global__ void k_abs_max(const float* __restrict__ a, long na, const float* __restrict__ b, long nb,
+                          const float* __restrict__ c, long nc, unsigned int* __restrict__ out) {
+  float best = 0.0f;
+  const long total = na + nb + nc;
+  for (long idx = (long)blockIdx.x * blockDim.x + threadIdx.x; idx < total; idx += (long)gridDim.x * blockDim.x) {
+    float value = idx < na ? __ldg(a + idx) : (idx < na + nb ? __ldg(b + idx - na) : __ldg(c + idx - na - nb));
+    best = fmax_(best, fabsf(value));
+  }
+  for (int off = 16; off >= 1; off >>= 1) best = fmax_(best, __shfl_xor_sync(0xffffffffu, best, off));
+  if ((threadIdx.x & 31) == 0) atomicMax(out, __float_as_uint(best));  // non-negative floats order as ints
+}
+
+}  // namespace plume
+
+using namespace plume;
+
+// ---- C ABI -------------------------------------------------------------------------------------------------
+
+extern "C" const char* plume_last_error(void) { return g_error; }
+extern "C" int plume_abi_version(void) { return 1; }
+extern "C" unsigned long long plume_launch_count(void) { return __atomic_load_n(&g_launches, __ATOMIC_RELAXED); }
+
+extern "C" int plume_advect_semi_lagrangian(const PlumeGridInfo* info, const int32_t shape[3], const float* src,
+                                            float* dst, const float* u, const float* v, const float* w,
+                                            float dt_over_cell, const float offset[3], float outside,
+                                            int32_t uses_outside, void* stream) {
+  CHECK_ARG(info && shape && src && dst && u && v && w && offset, "semi_lagrangian: null argument");
+  CHECK_ARG(valid_dims(info->dims) && valid_dims(shape), "semi_lagrangian: bad dims");
+  FieldSet set{};
+  set.count = 1;
+  set.f[0] = FieldDesc{src, nullptr, dst, Dims{shape[0], shape[1], shape[2]}, f3(offset[0], offset[1], offset[2]),
+                       outside, uses_outside};
+  return launch_advect(*info, make_vel(u, v, w, info->dims), set, dt_over_cell, false, as_stream(stream));
+}
+
+extern "C" int plume_advect_maccormack(const PlumeGridInfo* info, const int32_t shape[3], const float* data,
+                                       float* hat, float* next, const float* u, const float* v, const float* w,
+                                       float dt_over_cell, const float offset[3], float outside, int32_t uses_outside,
+                                       void* stream) {
+  CHECK_ARG(info && shape && data && hat && next && u && v && w && offset, "maccormack: null argument");
+  CHECK_ARG(valid_dims(info->dims) && valid_dims(shape), "maccormack: bad dims");
+  FieldSet set{};
+  set.count = 1;
+  set.f[0] = FieldDesc{data, hat, next, Dims{shape[0], shape[1], shape[2]}, f3(offset[0], offset[1], offset[2]),
+                       outside, uses_outside};
+  return launch_advect(*info, make_vel(u, v, w, info->dims), set, dt_over_cell, true, as_stream(stream));
+}
+
+extern "C" int plume_emit(const PlumeGridInfo* info, float* smoke, float* temperature, float* u, float* v, float* w,
+                          const PlumeEmitter* emitters, int32_t count, int32_t seed, float time_s, float dt,
+                          void* stream) {
+  CHECK_ARG(info && smoke && temperature && u && v && w, "emit: null argument");
+  CHECK_ARG(count >= 0 && (count == 0 || emitters), "emit: bad emitter list");
+  CHECK_ARG(valid_dims(info->dims), "emit: bad dims");
+  return launch_emit(*info, smoke, temperature, u, v, w, emitters, count, seed, time_s, dt, as_stream(stream));
+}
+
+extern "C" int plume_buoyancy(const PlumeGridInfo* info, float* v, const float* smoke, const float* temperature,
+                              float gravity, float heat_buoyancy, float smoke_weight, float ambient_k, float dt,
+                              void* stream) {
+  CHECK_ARG(info && v && smoke && temperature, "buoyancy: null argument");
+  CHECK_ARG(valid_dims(info->dims), "buoyancy: bad dims");
+  const int nx = info->dims[0], ny = info->dims[1], nz = info->dims[2];
+  k_buoyancy<<<cell_grid(nx, ny + 1, nz), cell_block(), 0, as_stream(stream)>>>(
+      *info, v, smoke, temperature, gravity, heat_buoyancy, smoke_weight, ambient_k, dt);
+  return launch_status("buoyancy");
+}
+
+extern "C" int plume_drag(const PlumeGridInfo* info, float* u, float* v, float* w, const float wind[3], float keep,
+                          void* stream) {
+  CHECK_ARG(info && u && v && w && wind, "drag: null argument");
+  CHECK_ARG(valid_dims(info->dims), "drag: bad dims");
+  FaceForces ff{};
+  ff.drag = 1;
+  ff.wind[0] = wind[0];
+  ff.wind[1] = wind[1];
+  ff.wind[2] = wind[2];
+  ff.keep = keep;
+  k_face_forces<<<face_grid(*info), cell_block(), 0, as_stream(stream)>>>(*info, u, v, w, ff);
+  return launch_status("drag");
+}
+
+extern "C" int plume_confinement(const PlumeGridInfo* info, float* u, float* v, float* w, float* curl_xyz[3],
+                                 float* push_xyz[3], float strength, float dt, int32_t apply, void* stream) {
+  CHECK_ARG(info && u && v && w && curl_xyz && curl_xyz[0] && curl_xyz[1] && curl_xyz[2], "confinement: null argument");
+  CHECK_ARG(!apply || (push_xyz && push_xyz[0] && push_xyz[1] && push_xyz[2]), "confinement: null push");
+  CHECK_ARG(valid_dims(info->dims), "confinement: bad dims");
+  cudaStream_t st = as_stream(stream);
+  int status = launch_confinement_push(*info, u, v, w, curl_xyz, push_xyz, strength, apply, st);
+  if (status != PLUME_OK || !apply) return status;
+  FaceForces ff{};
+  ff.confinement = 1;
+  ff.push[0] = push_xyz[0];
+  ff.push[1] = push_xyz[1];
+  ff.push[2] = push_xyz[2];
+  ff.dt = dt;
+  k_face_forces<<<face_grid(*info), cell_block(), 0, st>>>(*info, u, v, w, ff);
+  return launch_status("add face push");
+}
+
+extern "C" int plume_turbulence(const PlumeGridInfo* info, float* u, float* v, float* w, int32_t seed, float scale_m,
+                                float strength, float pattern_time, float dt, void* stream) {
+  CHECK_ARG(info && u && v && w, "turbulence: null argument");
+  CHECK_ARG(valid_dims(info->dims), "turbulence: bad dims");
+  FaceForces ff{};
+  ff.turbulence = 1;
+  ff.seed = seed;
+  ff.scale_m = scale_m;
+  ff.strength = strength;
+  ff.pattern_time = pattern_time;
+  ff.dt = dt;
+  k_face_forces<<<face_grid(*info), cell_block(), 0, as_stream(stream)>>>(*info, u, v, w, ff);
+  return launch_status("turbulence");
+}
+
+extern "C" int plume_divergence(const PlumeGridInfo* info, const float* u, const float* v, const float* w,
+                                float* divergence, void* stream) {
+  CHECK_ARG(info && u && v && w && divergence, "divergence: null argument");
+  CHECK_ARG(valid_dims(info->dims), "divergence: bad dims");
+  const int nx = info->dims[0], ny = info->dims[1], nz = info->dims[2];
+  k_divergence<<<cell_grid(nx, ny, nz), cell_block(), 0, as_stream(stream)>>>(*info, u, v, w, divergence);
+  return launch_status("divergence");
+}
+
+extern "C" int plume_project_begin(const PlumeGridInfo* info, float* u, float* v, float* w, float* divergence,
+                                   void* stream) {
+  CHECK_ARG(info && u && v && w && divergence, "project: null argument");
+  CHECK_ARG(valid_dims(info->dims), "project: bad dims");
+  const int nx = info->dims[0], ny = info->dims[1], nz = info->dims[2];
+  const int m = std::max(nx, ny) + 1, n = std::max(ny, nz) + 1;
+  k_zero_walls<<<dim3((n + TZ - 1) / TZ, (m + TY - 1) / TY, 6), cell_block(), 0, as_stream(stream)>>>(*info, u, v, w);
+  CHECK_LAUNCH("zero closed faces");
+  return plume_divergence(info, u, v, w, divergence, stream);
+}
+
+extern "C" int plume_subtract_gradient(const PlumeGridInfo* info, float* u, float* v, float* w, const float* q,
+                                       void* stream) {
+  CHECK_ARG(info && u && v && w && q, "subtract_gradient: null argument");
+  CHECK_ARG(valid_dims(info->dims), "subtract_gradient: bad dims");
+  k_subtract_gradient<<<face_grid(*info), cell_block(), 0, as_stream(stream)>>>(*info, u, v, w, q);
+  return launch_status("subtract gradient");
+}
+
+extern "C" int plume_red_black_sweeps(const PlumeGridInfo* info, float* q, const float* rhs, int32_t sweeps,
+                                      float relaxation, void* stream) {
+  CHECK_ARG(info && q && rhs && sweeps >= 0, "red_black_sweeps: bad argument");
+  CHECK_ARG(valid_dims(info->dims), "red_black_sweeps: bad dims");
+  return red_black_sweeps(*info, q, rhs, sweeps, relaxation, as_stream(stream));
+}
+
+extern "C" int plume_multigrid(const PlumeLevel* levels, int32_t level_count, int32_t cycles, int32_t sweeps,
+                               void* stream) {
+  CHECK_ARG(levels && level_count >= 1 && cycles >= 0 && sweeps >= 0, "multigrid: bad argument");
+  for (int l = 0; l < level_count; ++l)
+    CHECK_ARG(levels[l].q && levels[l].rhs && (l == level_count - 1 || levels[l].residual) && valid_dims(levels[l].info.dims),
+              "multigrid: bad level %d", l);
+  for (int c = 0; c < cycles; ++c) {
+    int status = v_cycle(levels, level_count, 0, sweeps, as_stream(stream));
+    if (status != PLUME_OK) return status;
+  }
+  return PLUME_OK;
+}
+
+extern "C" int plume_residual(const PlumeGridInfo* info, const float* q, const float* rhs, float* residual,
+                              void* stream) {
+  CHECK_ARG(info && q && rhs && residual, "residual: null argument");
+  CHECK_ARG(valid_dims(info->dims), "residual: bad dims");
+  const int nx = info->dims[0], ny = info->dims[1], nz = info->dims[2];
+  k_residual<<<cell_grid(nx, ny, nz), cell_block(), 0, as_stream(stream)>>>(*info, q, rhs, residual);
+  return launch_status("residual");
+}
+
+extern "C" int plume_smoke_scratch_doubles(const PlumeGridInfo* info) {
+  if (!info || !valid_dims(info->dims)) return fail(PLUME_ERR_INVALID, "smoke_scratch_doubles: bad dims");
+  return 3 * sum_blocks(dims_of(*info));
+}
+
+extern "C" int plume_triple_sum(const int32_t shape[3], const float* a, const float* b, const float* c, double* sums,
+                                double* totals_out, void* stream) {
+  CHECK_ARG(shape && a && b && c && sums && totals_out, "triple_sum: null argument");
+  CHECK_ARG(valid_dims(shape), "triple_sum: bad dims");
+  return launch_triple_sum(Dims{shape[0], shape[1], shape[2]}, a, b, c, sums, nullptr, totals_out, as_stream(stream));
+}
+
+extern "C" int plume_smoke_budget(const PlumeGridInfo* info, const float* data, const float* hat, float* next,
+                                  double* sums, float* factor, double* totals_out, void* stream) {
+  CHECK_ARG(info && data && hat && next && sums && factor, "smoke_budget: null argument");
+  CHECK_ARG(valid_dims(info->dims), "smoke_budget: bad dims");
+  cudaStream_t st = as_stream(stream);
+  const Dims d = dims_of(*info);
+  int status = launch_triple_sum(d, data, hat, next, sums, factor, totals_out, st);
+  if (status != PLUME_OK) return status;
+  const long n = (long)d.n0 * d.n1 * d.n2;
+  k_scale<<<grid_stride_blocks(n), 256, 0, st>>>(next, n, factor);
+  return launch_status("smoke budget scale");
+}
+
+extern "C" int plume_dissipate(const PlumeGridInfo* info, float* smoke, float* temperature, float smoke_keep,
+                               float heat_keep, float ambient_k, void* stream) {
+  CHECK_ARG(info && smoke && temperature, "dissipate: null argument");
+  CHECK_ARG(valid_dims(info->dims), "dissipate: bad dims");
+  const long n = (long)info->dims[0] * info->dims[1] * info->dims[2];
+  k_dissipate<<<grid_stride_blocks(n), 256, 0, as_stream(stream)>>>(smoke, temperature, n, smoke_keep, heat_keep,
+                                                                    ambient_k);
+  return launch_status("dissipate");
+}
+
+extern "C" int plume_grid_speed(const PlumeGridInfo* info, const float* u, const float* v, const float* w,
+                                float* speed, void* stream) {
+  CHECK_ARG(info && u && v && w && speed, "grid_speed: null argument");
+  CHECK_ARG(valid_dims(info->dims), "grid_speed: bad dims");
+  cudaStream_t st = as_stream(stream);
+  const long nx = info->dims[0], ny = info->dims[1], nz = info->dims[2];
+  const long na = (nx + 1) * ny * nz, nb = nx * (ny + 1) * nz, nc = nx * ny * (nz + 1);
+  int status = runtime_status("grid speed reset", cudaMemsetAsync(speed, 0, sizeof(float), st));
+  if (status != PLUME_OK) return status;
+  k_abs_max<<<grid_stride_blocks(na + nb + nc), 256, 0, st>>>(u, na, v, nb, w, nc, reinterpret_cast<unsigned int*>(speed));
+  return launch_status("grid speed");
+}
+
+extern "C" int plume_step(const PlumeStepState* s, const PlumeStepParams* p, void* stream) {
+  CHECK_ARG(s && p, "step: null argument");
+  CHECK_ARG(valid_dims(s->info.dims), "step: bad dims");
+  CHECK_ARG(s->u.data && s->u.hat && s->u.next && s->v.data && s->v.hat && s->v.next && s->w.data && s->w.hat &&
+                s->w.next && s->smoke.data && s->smoke.hat && s->smoke.next && s->temperature.data &&
+                s->temperature.hat && s->temperature.next && s->pressure && s->divergence && s->sums && s->factor,
+            "step: null buffer");
+  CHECK_ARG(p->solver != 0 || (s->levels && s->level_count >= 1 && s->levels[0].q == s->pressure &&
+                               s->levels[0].rhs == s->divergence),
+            "step: multigrid levels must start at the grid's pressure and divergence");
+  CHECK_ARG(p->confinement == 0.0f || (s->curl[0] && s->curl[1] && s->curl[2] && s->push[0] && s->push[1] && s->push[2]),
+            "step: confinement scratch missing");
+  cudaStream_t st = as_stream(stream);
+  const PlumeGridInfo& info = s->info;
+  const int nx = info.dims[0], ny = info.dims[1], nz = info.dims[2];
+  int status;
+  int phase = 0;
+  auto mark = [&]() -> int {  // phase boundary event, when the caller asked for them
+    if (!p->phase_events) return PLUME_OK;
+    return runtime_status("phase event", cudaEventRecord(reinterpret_cast<cudaEvent_t>(p->phase_events[phase++]), st));
+  };
+  if ((status = mark()) != PLUME_OK) return status;
+  // emit, buoyancy (stepper.py:32-34)
+  if ((status = launch_emit(info, s->smoke.data, s->temperature.data, s->u.data, s->v.data, s->w.data, p->emitters,
+                            p->emitter_count, p->seed, p->time_s, p->dt, st)) != PLUME_OK)
+    return status;
+  k_buoyancy<<<cell_grid(nx, ny + 1, nz), cell_block(), 0, st>>>(info, s->v.data, s->smoke.data, s->temperature.data,
+                                                                 p->gravity, p->heat_buoyancy, p->smoke_weight,
+                                                                 p->ambient_k, p->dt);
+  CHECK_LAUNCH("buoyancy");
+  // confinement, turbulence, drag (stepper.py:35-40): one face pass after the push is known
+  FaceForces ff{};
+  ff.dt = p->dt;
+  if (p->confinement != 0.0f) {
+    float* curl[3] = {s->curl[0], s->curl[1], s->curl[2]};
+    float* push[3] = {s->push[0], s->push[1], s->push[2]};
+    if ((status = launch_confinement_push(info, s->u.data, s->v.data, s->w.data, curl, push, p->confinement, 1, st)) !=
+        PLUME_OK)
+      return status;
+    ff.confinement = 1;
+    ff.push[0] = s->push[0];
+    ff.push[1] = s->push[1];
+    ff.push[2] = s->push[2];
+  }
+  if (p->turbulence_strength != 0.0f) {
+    ff.turbulence = 1;
+    ff.seed = p->seed;
+    ff.scale_m = p->turbulence_scale_m;
+    ff.strength = p->turbulence_strength;
+    ff.pattern_time = p->turbulence_pattern_time;
+  }
+  if (p->apply_drag) {
+    ff.drag = 1;
+    ff.wind[0] = p->wind[0];
+    ff.wind[1] = p->wind[1];
+    ff.wind[2] = p->wind[2];
+    ff.keep = p->drag_keep;
+  }
+  if (ff.confinement || ff.turbulence || ff.drag) {
+    k_face_forces<<<face_grid(info), cell_block(), 0, st>>>(info, s->u.data, s->v.data, s->w.data, ff);
+    CHECK_LAUNCH("face forces");
+  }
+  if ((status = mark()) != PLUME_OK) return status;
+  // advect velocity (stepper.py:46-52)
+  {
+    FieldSet set{};
+    set.count = 3;
+    set.f[0] = FieldDesc{s->u.data, s->u.hat, s->u.next, Dims{nx + 1, ny, nz}, f3(0.0f, 0.5f, 0.5f), 0.0f, 0};
+    set.f[1] = FieldDesc{s->v.data, s->v.hat, s->v.next, Dims{nx, ny + 1, nz}, f3(0.5f, 0.0f, 0.5f), 0.0f, 0};
+    set.f[2] = FieldDesc{s->w.data, s->w.hat, s->w.next, Dims{nx, ny, nz + 1}, f3(0.5f, 0.5f, 0.0f), 0.0f, 0};
+    if ((status = launch_advect(info, make_vel(s->u.data, s->v.data, s->w.data, info.dims), set, p->dt_over_cell, true,
+                                st)) != PLUME_OK)
+      return status;
+  }
+  if ((status = mark()) != PLUME_OK) return status;
+  float* u = s->u.next;  // after the swap
+  float* v = s->v.next;
+  float* w = s->w.next;
+  // project (stepper.py:42, pressure.py:144-154)
+  if ((status = plume_project_begin(&info, u, v, w, s->divergence, stream)) != PLUME_OK) return status;
+  if ((status = mark()) != PLUME_OK) return status;
+  if (p->solver == 0) {
+    for (int c = 0; c < p->solver_iterations; ++c)
+      if ((status = v_cycle(s->levels, s->level_count, 0, p->multigrid_sweeps, st)) != PLUME_OK) return status;
+  } else if ((status = red_black_sweeps(info, s->pressure, s->divergence, p->solver_iterations, 1.5f, st)) != PLUME_OK) {
+    return status;
+  }
+  if ((status = mark()) != PLUME_OK) return status;
+  k_subtract_gradient<<<face_grid(info), cell_block(), 0, st>>>(info, u, v, w, s->pressure);
+  CHECK_LAUNCH("subtract gradient");
+  if ((status = mark()) != PLUME_OK) return status;
+  // advect smoke and temperature (stepper.py:54-60): the smoke budget holds smoke.next before its swap
+  {
+    Vel vel = make_vel(u, v, w, info.dims);
+    FieldSet set{};
+    set.count = 2;
+    set.f[0] = FieldDesc{s->smoke.data, s->smoke.hat, s->smoke.next, Dims{nx, ny, nz}, f3(0.5f, 0.5f, 0.5f), 0.0f, 1};
+    set.f[1] = FieldDesc{s->temperature.data, s->temperature.hat, s->temperature.next, Dims{nx, ny, nz},
+                         f3(0.5f, 0.5f, 0.5f), p->ambient_k, 1};
+    if ((status = launch_advect(info, vel, set, p->dt_over_cell, true, st)) != PLUME_OK) return status;
+  }
+  if ((status = launch_triple_sum(dims_of(info), s->smoke.data, s->smoke.hat, s->smoke.next, s->sums, s->factor,
+                                  nullptr, st)) != PLUME_OK)
+    return status;
+  // scale + dissipate (stepper.py:44) on the advected buffers
+  const long n = (long)nx * ny * nz;
+  k_scalar_finish<<<grid_stride_blocks(n), 256, 0, st>>>(s->smoke.next, s->temperature.next, n, s->factor,
+                                                         p->apply_dissipation, p->smoke_keep, p->heat_keep, p->ambient_k);
+  CHECK_LAUNCH("scale and dissipate");
+  return mark();
+}

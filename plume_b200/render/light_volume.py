@@ -1,0 +1,21 @@
+"""The light volume (mirrors chadmv/plume src/plume/render/light_volume.py:36-51): the share of the key light
+reaching each cell through the smoke toward the light, exp(-opacity_per_density * column density)."""
+
+import numpy as np
+import torch
+
+from plume_b200 import _native as N
+
+
+class LightVolume:
+    def __init__(self, cells, toward_light_world, opacity_per_density: float, device: str):
+        self.device = device
+        direction = np.asarray(toward_light_world, dtype=np.float64)
+        self.toward_light = tuple(float(x) for x in direction / np.linalg.norm(direction))
+        self.opacity_per_density = opacity_per_density
+        self.light = torch.zeros(tuple(cells), dtype=torch.float32, device=device)
+
+    def compute(self, smoke: torch.Tensor, cell_m: float) -> torch.Tensor:
+        N.call("plume_light_volume", N.shape3(smoke), N.ptr(smoke), N.f3(self.toward_light), cell_m,
+               self.opacity_per_density, N.ptr(self.light), N.stream())
+        return self.light

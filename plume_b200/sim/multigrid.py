@@ -1,0 +1,87 @@
+"""Geometric multigrid for the pressure solve (mirrors chadmv/plume src/plume/sim/multigrid.py:24-147).
+
+Cell-centred V-cycles with averaging restriction and trilinear prolongation. Levels halve each axis
+(rounding up) until the shortest axis is at most 2 cells or there are 8 levels; a coarse level's overhanging
+last cell is weighted by the share inside the domain (`fill_hi`). The whole V-cycle runs in one library call.
+"""
+
+from dataclasses import dataclass
+
+import torch
+
+from plume_b200 import _native as N
+from plume_b200.sim.grid import GridInfo, make_info
+
+MIN_LEVEL_CELLS = 2
+MAX_LEVELS = 8
+COARSEST_SWEEPS = 20
+COARSEST_SWEEPS_PER_CELL = 4
+COARSEST_RELAXATION = 1.5
+SMOOTHING_RELAXATION = 1.0
+
+
+@dataclass
+class Level:
+    info: GridInfo
+    cells: tuple
+    q: torch.Tensor
+    rhs: torch.Tensor
+    residual: torch.Tensor
+
+
+def coarse_cells(cells):
+    return tuple((n + 1) // 2 for n in cells)
+
+
+def coarse_geometry(top_cells, cells, level: int):
+    """(fill_hi, ghost_gap) of a level `level` steps down: the share of its last cell inside the domain on each
+    axis, and the distance in its cells to the pressure-0 ghost beyond an open face."""
+    scale = 2.0 ** level
+    return tuple(top / scale - (n - 1) for top, n in zip(top_cells, cells)), 0.5 / scale
+
+
+class Multigrid:
+    """`cycles` V-cycles per solve, with `sweeps` smoothing sweeps before and after each correction."""
+
+    def __init__(self, grid, cycles: int, sweeps: int):
+        self.cycles = cycles
+        self.sweeps = sweeps
+        self.device = grid.device
+        self.levels = self._build_levels(grid)
+        self._native_levels = None
+
+    def _build_levels(self, grid):
+        levels = [Level(grid.info, grid.cells, grid.pressure, grid.divergence,
+                        torch.zeros(grid.cells, dtype=torch.float32, device=grid.device))]
+        while min(levels[-1].cells) > MIN_LEVEL_CELLS and len(levels) < MAX_LEVELS:
+            above = levels[-1]
+            cells = coarse_cells(above.cells)
+            fill, gap = coarse_geometry(grid.cells, cells, len(levels))
+            info = make_info(cells, above.info.cell_m * 2.0, tuple(above.info.origin_m), tuple(above.info.open_lo),
+                             tuple(above.info.open_hi), fill, gap)
+            levels.append(Level(info, cells, *(torch.zeros(cells, dtype=torch.float32, device=self.device)
+                                               for _ in range(3))))
+        return levels
+
+    def native_levels(self, grid):
+        """The levels as the C structs the library reads (the top level aliases the grid's arrays)."""
+        self.levels[0].q = grid.pressure
+        self.levels[0].rhs = grid.divergence
+        array = (N.PlumeLevel * len(self.levels))()
+        for slot, level in zip(array, self.levels):
+            slot.info = level.info
+            slot.q = N.ptr(level.q).value
+            slot.rhs = N.ptr(level.rhs).value
+            slot.residual = N.ptr(level.residual).value
+        self._native_levels = array
+        return array
+
+    def __call__(self, grid) -> None:
+        levels = self.native_levels(grid)
+        N.call("plume_multigrid", levels, len(self.levels), self.cycles, self.sweeps, N.stream())
+
+    def residual(self, level_index: int = 0) -> torch.Tensor:
+        """Fills and returns one level's residual rhs - A q (multigrid.py:36-43)."""
+        level = self.levels[level_index]
+        N.call("plume_residual", level.info, N.ptr(level.q), N.ptr(level.rhs), N.ptr(level.residual), N.stream())
+        return level.residual

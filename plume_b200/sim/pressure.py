@@ -1,0 +1,48 @@
+"""Pressure projection (mirrors chadmv/plume src/plume/sim/pressure.py:17-162).
+
+Solves laplacian(q) = divergence(u) for a scaled pressure q, then subtracts gradient(q) from the face
+velocities. Closed faces are walls; open faces see q = 0 just outside. The solve is pluggable: GaussSeidel
+here, Multigrid in plume_b200.sim.multigrid.
+"""
+
+from typing import Protocol
+
+from plume_b200 import _native as N
+
+RELAXATION = 1.5
+
+
+class PressureSolve(Protocol):
+    def __call__(self, grid) -> None:
+        """Improves grid.pressure toward the solution of laplacian(q) = grid.divergence."""
+
+
+class GaussSeidel:
+    """A fixed number of red-black Gauss-Seidel sweeps with over-relaxation."""
+
+    def __init__(self, iterations: int):
+        self.iterations = iterations
+
+    def __call__(self, grid) -> None:
+        red_black_sweeps(grid.pressure, grid.divergence, grid.info, grid.cells, grid.device, self.iterations,
+                         RELAXATION)
+
+
+def red_black_sweeps(q, rhs, info, cells, device, sweeps: int, relaxation: float) -> None:
+    """`sweeps` red-black sweeps (colour 0 then 1) of laplacian(q) = rhs on the grid `info` describes."""
+    N.call("plume_red_black_sweeps", info, N.ptr(q), N.ptr(rhs), sweeps, relaxation, N.stream())
+
+
+def project(grid, solve) -> None:
+    """Makes the face velocities divergence-free (to the solver's accuracy) and walls impermeable."""
+    u, v, w = (f.data for f in grid.velocity_fields())
+    N.call("plume_project_begin", grid.info, N.ptr(u), N.ptr(v), N.ptr(w), N.ptr(grid.divergence), N.stream())
+    solve(grid)
+    N.call("plume_subtract_gradient", grid.info, N.ptr(u), N.ptr(v), N.ptr(w), N.ptr(grid.pressure), N.stream())
+
+
+def compute_divergence(grid):
+    """Fills and returns grid.divergence from the current face velocities."""
+    u, v, w = (f.data for f in grid.velocity_fields())
+    N.call("plume_divergence", grid.info, N.ptr(u), N.ptr(v), N.ptr(w), N.ptr(grid.divergence), N.stream())
+    return grid.divergence

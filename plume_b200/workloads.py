@@ -1,0 +1,91 @@
+"""Synthetic workloads: seeded fields and recipes with the shapes and value distributions of the benchmark
+configurations (no dataset is involved; everything is generated from a seed).
+
+- `operator_fields`: the operator-level case -- u, v, w ~ U(-1, 1) m/s smoothed by three 3x3x3 box-filter
+  passes with edge clamp; smoke ~ U(0, 1) masked to a sphere of radius 40/128 of the x extent at the grid
+  centre; temperature = ambient + 0.8 * smoke (ambient 1).
+- `plain_step_recipe`: the plain smoke-puff step at a given grid: dx = 1/64 m scaled to the grid, buoyancy
+  f_y = 1.0 T - 0.05 density with ambient 1, drag 0.2/s, vorticity confinement 0.3, closed floor and open
+  sides and ceiling, multigrid 4 V-cycles of 2+2 sweeps, a sphere emitter of radius 12/128 of the x extent
+  near the floor holding temperature 2 and adding smoke at 1/s, dt = 1/96 s.
+- `smoke_puff_recipe`: the 64 x 96 x 64 puff run (24 fps x 48 frames, CFL 1, at most 4 substeps).
+"""
+
+import numpy as np
+
+from plume_b200.recipe.load import resolve_table
+
+DEFAULT_SEED = 20261203
+
+
+def box_filter(field: np.ndarray, passes: int = 3) -> np.ndarray:
+    """`passes` 3x3x3 box-filter passes with edge clamp, in float64."""
+    out = field.astype(np.float64)
+    for _ in range(passes):
+        padded = np.pad(out, 1, mode="edge")
+        total = np.zeros_like(out)
+        n0, n1, n2 = out.shape
+        for a in range(3):
+            for b in range(3):
+                for c in range(3):
+                    total += padded[a:a + n0, b:b + n1, c:c + n2]
+        out = total / 27.0
+    return out
+
+
+def operator_fields(cells, seed: int = DEFAULT_SEED, ambient_k: float = 1.0) -> dict:
+    nx, ny, nz = cells
+    rng = np.random.default_rng(seed)
+    fields = {
+        "u": box_filter(rng.uniform(-1.0, 1.0, (nx + 1, ny, nz))),
+        "v": box_filter(rng.uniform(-1.0, 1.0, (nx, ny + 1, nz))),
+        "w": box_filter(rng.uniform(-1.0, 1.0, (nx, ny, nz + 1))),
+    }
+    smoke = rng.uniform(0.0, 1.0, cells)
+    idx = np.indices(cells).astype(np.float64) + 0.5
+    radius = 40.0 * nx / 128.0
+    inside = sum((idx[a] - cells[a] / 2.0) ** 2 for a in range(3)) <= radius * radius
+    fields["smoke"] = np.where(inside, smoke, 0.0)
+    fields["temperature"] = ambient_k + 0.8 * fields["smoke"]
+    return {name: value.astype(np.float32) for name, value in fields.items()}
+
+
+def plain_step_recipe(cells=(128, 192, 128), cycles: int = 4, frames: int = 24, substeps: int = 4):
+    nx, ny, nz = cells
+    cell_m = (128.0 / nx) / 64.0
+    table = {
+        "seed": 7,
+        "domain": {"size_m": [nx * cell_m, ny * cell_m, nz * cell_m], "cell_m": cell_m, "ambient_k": 1.0},
+        "time": {"duration_s": frames / 24.0, "frames": frames, "substeps": substeps},
+        "emitter": [{"name": "source", "center_m": [0.0, 16.0 * (nx / 128.0) * cell_m, 0.0],
+                     "radius_m": 12.0 * (nx / 128.0) * cell_m, "edge_softness": 0.0, "end_s": 1.0e6,
+                     "smoke_per_s": 1.0, "temperature_k": 2.0}],
+        "forces": {"gravity_mps2": 1.0, "heat_buoyancy": 1.0, "smoke_weight": 0.05, "drag_per_s": 0.2,
+                   "vorticity_confinement": 0.3},
+        "solver": {"multigrid_cycles": cycles, "multigrid_sweeps": 2, "max_cells_per_step": 1.0,
+                   "max_substeps": 32},
+        "render": {"glow_start_k": 1.0, "light_dir": [0.5, 0.8, 0.3]},
+        "output": {"frame_px": 128},
+    }
+    return resolve_table(table, "plain_step")
+
+
+def smoke_puff_recipe(cells=(64, 96, 64), frames: int = 48):
+    """The 64 x 96 x 64 puff: dx = 1/32 m, sphere of radius 6 cells at cell (32, 8, 32) adding density 1/s and
+    holding temperature 2 (ambient 1) for the first 0.5 s, 24 fps, CFL 1 with at most 4 substeps."""
+    nx, ny, nz = cells
+    cell_m = 1.0 / 32.0 * (64.0 / nx)
+    table = {
+        "seed": 7,
+        "domain": {"size_m": [nx * cell_m, ny * cell_m, nz * cell_m], "cell_m": cell_m, "ambient_k": 1.0},
+        "time": {"duration_s": frames / 24.0, "frames": frames, "substeps": 1},
+        "emitter": [{"name": "puff", "center_m": [0.0, 8.0 * (nx / 64.0) * cell_m, 0.0],
+                     "radius_m": 6.0 * (nx / 64.0) * cell_m, "edge_softness": 0.0, "end_s": 0.5,
+                     "smoke_per_s": 1.0, "temperature_k": 2.0}],
+        "forces": {"gravity_mps2": 1.0, "heat_buoyancy": 1.0, "smoke_weight": 0.05, "drag_per_s": 0.2,
+                   "vorticity_confinement": 0.3},
+        "solver": {"multigrid_cycles": 4, "multigrid_sweeps": 2, "max_cells_per_step": 1.0, "max_substeps": 4},
+        "render": {"glow_start_k": 1.0, "light_dir": [0.5, 0.8, 0.3]},
+        "output": {"frame_px": 128},
+    }
+    return resolve_table(table, "smoke_puff_c1")

@@ -1,0 +1,64 @@
+"""CPU checks of the boundary: the C-ABI library loads without a GPU and exports every entry point the
+public header declares, the Python binding's struct layouts match the header's, and the package refuses to
+run anywhere but CUDA."""
+
+import ctypes
+import re
+from pathlib import Path
+
+import pytest
+
+from plume_b200 import _native as N
+
+HEADER = Path(__file__).resolve().parents[1] / "include" / "plume_b200.h"
+
+
+def declared_functions() -> list[str]:
+    text = re.sub(r"/\*.*?\*/", "", HEADER.read_text(), flags=re.S)
+    return sorted(set(re.findall(r"\b(plume_[a-z0-9_]+)\s*\(", text)))
+
+
+def test_the_library_exports_every_declared_entry_point():
+    lib = N.lib()
+    names = declared_functions()
+    assert len(names) >= 20
+    missing = [name for name in names if not hasattr(lib, name)]
+    assert missing == []
+    assert set(names) == set(N.EXPORTED)
+
+
+def test_every_binding_has_a_signature():
+    for name in declared_functions():
+        if name not in ("plume_last_error", "plume_launch_count"):
+            assert name in N.SIGNATURES, name
+
+
+def test_struct_layouts_match_the_header():
+    # sizes follow from the header's field lists (all 4-byte fields; pointers 8 bytes)
+    assert ctypes.sizeof(N.PlumeGridInfo) == 4 * (3 + 1 + 3 + 3 + 3 + 3 + 1)
+    assert ctypes.sizeof(N.PlumeEmitter) == 4 * (1 + 3 + 1 + 3 + 1 + 1 + 1 + 1 + 1 + 3 + 1 + 1 + 1 + 1)
+    assert ctypes.sizeof(N.PlumeViewParams) == 4 * (3 + 3 + 3 + 1 + 1 + 1 + 1 + 3)
+    assert ctypes.sizeof(N.PlumeLookParams) == 4 * 6
+    assert ctypes.sizeof(N.PlumeField) == 3 * 8
+
+
+def test_abi_version_and_error_message_need_no_gpu():
+    lib = N.lib()
+    assert lib.plume_abi_version() == 1
+    status = lib.plume_buoyancy(None, None, None, None, 0.0, 0.0, 0.0, 1.0, 0.0, None)
+    assert status == -1
+    assert b"null" in lib.plume_last_error()
+
+
+def test_the_cpu_device_is_refused():
+    from plume_b200.sim.device import DeviceError, init_device
+
+    with pytest.raises(DeviceError):
+        init_device("cpu")
+
+
+def test_kernels_refuse_host_tensors():
+    import torch
+
+    with pytest.raises(RuntimeError, match="CUDA"):
+        N.ptr(torch.zeros(4))

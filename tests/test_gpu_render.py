@@ -1,0 +1,96 @@
+"""Render parity: light volume, normal field and ray march (both layouts, orthographic and perspective)
+through the C ABI against the FP32 oracle. exp/pow are evaluated in double on the device and as expf/powf in
+the oracle, so values agree to about an ulp per call; the march accumulates them (tolerance below)."""
+
+import numpy as np
+import pytest
+
+from oracle import oracle as O
+from plume_b200.recipe.schema import NORMAL_LAYOUT, SHADE_LAYOUT, RenderSettings
+from plume_b200.render.camera import make_camera, make_domain_view
+from plume_b200.workloads import operator_fields
+from support import OPEN, assert_same, blob, cuda_grid, host, load_state, max_rel, oracle_grid
+
+pytestmark = pytest.mark.gpu
+
+LIGHT_RTOL = 1e-5
+MARCH_ATOL = 1e-5
+
+
+def render_pair(cells=(24, 32, 20), seed=4):
+    o = oracle_grid(cells, 0.05, OPEN, 293.0)
+    c = cuda_grid(cells, 0.05, OPEN, 293.0)
+    fields = operator_fields(cells, seed, 293.0)
+    fields["temperature"] = (293.0 + 900.0 * blob(cells, [n / 2 for n in cells], 3.0)).astype(np.float32)
+    fields["smoke"] = (3.0 * fields["smoke"]).astype(np.float32)
+    load_state(o, c, fields)
+    return o, c
+
+
+def test_light_volume_matches_the_oracle(cuda_device):
+    from plume_b200.render.light_volume import LightVolume
+
+    o, c = render_pair()
+    direction = np.array([0.5, 0.8, 0.3])
+    light = LightVolume(c.cells, direction, 4.0, "cuda:0").compute(c.smoke.data, c.info.cell_m)
+    expected = O.light_volume(o.smoke.data, direction, o.cell_m, 4.0)
+    assert max_rel(host(light), expected, floor=1e-6) < LIGHT_RTOL
+
+
+@pytest.mark.parametrize("channels", [SHADE_LAYOUT, NORMAL_LAYOUT])
+@pytest.mark.parametrize("elevation,azimuth", [(0.0, 0.0), (20.0, 30.0), (90.0, 0.0), (-35.0, 200.0)])
+def test_frame_matches_the_oracle(cuda_device, channels, elevation, azimuth):
+    from plume_b200.render.frame_renderer import FrameRenderer
+
+    o, c = render_pair()
+    cells = c.cells
+    size = tuple(n * 0.05 for n in cells)
+    view = make_domain_view(make_camera(elevation, azimuth), (-size[0] / 2, 0.0, -size[2] / 2), size, 0.05, 2.0)
+    settings = RenderSettings(glow_start_k=600.0, light_dir=(0.5, 0.8, 0.3))
+    image = FrameRenderer(view, settings, cells, channels, "cuda:0").render(c)
+    expected = O.FrameRenderer(view, settings, cells, channels).render(o)
+    assert image.shape == expected.shape == (view.height_px, view.width_px, 5)
+    heat_scale = max(float(np.abs(expected[..., 0]).max()), 1.0)
+    assert np.abs(image[..., 0] - expected[..., 0]).max() < MARCH_ATOL * heat_scale * 10
+    assert np.abs(image[..., 1:] - expected[..., 1:]).max() < MARCH_ATOL * 10
+
+
+def test_normal_field_matches_the_oracle(cuda_device):
+    from plume_b200.render.normal_field import NormalField
+
+    o, c = render_pair()
+    field = NormalField(c.cells, 1.5, "cuda:0")
+    gradient = field.compute(c.smoke.data)
+    renderer = O.FrameRenderer(make_domain_view(make_camera(0, 0), (0, 0, 0), (1, 1, 1), 0.05, 2.0),
+                               RenderSettings(), c.cells, NORMAL_LAYOUT)
+    renderer.prepare(o.smoke.data, o.cell_m)
+    assert_same(host(gradient), renderer.gradient, "gradient")
+
+
+def test_perspective_march_matches_the_oracle(cuda_device):
+    import torch
+
+    from plume_b200.render.frame_renderer import FrameRenderer, domain_view_params
+
+    o, c = render_pair()
+    cells = c.cells
+    size = tuple(n * 0.05 for n in cells)
+    view = make_domain_view(make_camera(25.0, 40.0), (-size[0] / 2, 0.0, -size[2] / 2), size, 0.05, 2.0)
+    settings = RenderSettings()
+    renderer = FrameRenderer(view, settings, cells, SHADE_LAYOUT, "cuda:0")
+    oracle = O.FrameRenderer(view, settings, cells, SHADE_LAYOUT)
+    params = domain_view_params(view)
+    params.perspective = 1
+    params.eye = type(params.eye)(0.1, 0.6, 0.2)  # inside the domain
+    params.left_m, params.top_m, params.pixel_m = -0.5, 0.5, 1.0 / 9.0
+    image = torch.zeros((9, 9, 5), dtype=torch.float32, device="cuda:0")
+    renderer.prepare(c.smoke.data, c.info.cell_m)
+    renderer.march(c.smoke.data, c.temperature.data, c.info, params, image)
+    oparams = O.domain_view_params(view)
+    oparams.perspective = 1
+    oparams.eye = O._d3((0.1, 0.6, 0.2))
+    oparams.left_m, oparams.top_m, oparams.pixel_m = -0.5, 0.5, 1.0 / 9.0
+    expected = np.zeros((9, 9, 5), dtype=np.float32)
+    oracle.prepare(o.smoke.data, o.cell_m)
+    oracle.march(o.smoke.data, o.temperature.data, o.info, oparams, expected)
+    assert np.abs(host(image)[..., 1:] - expected[..., 1:]).max() < MARCH_ATOL * 10
