@@ -201,6 +201,18 @@ int plume_smoke_scratch_doubles(const PlumeGridInfo* info);
 int plume_smoke_budget(const PlumeGridInfo* info, const float* data, const float* hat, float* next,
                        double* sums, float* factor, double* totals_out, void* stream);
 
+/* No counterpart in the reference. The smoke budget for callers that cannot allocate device memory: a host
+ * engine that passes in only the field arrays it owns while its allocator is locked or budgeted, or code that
+ * runs where a cudaMalloc would synchronise the device or is not allowed. Same result as plume_smoke_budget
+ * (next *= factor, optional device totals_out of 3 doubles), but the partial sums and the factor live in a
+ * fixed 96 KiB array inside the library, reserved on every device that loads it until the process exits; no
+ * memory is allocated or freed by the call. Limit: ny * nz <= 1048576 (1 << 20) lines, else PLUME_ERR_INVALID.
+ * The first call on a device looks up the array's device address on that device (make it before any stream
+ * capture). All calls share the one array: calls that overlap on the GPU (other streams, other threads) race
+ * and must be ordered by the caller. */
+int plume_smoke_budget_static(const PlumeGridInfo* info, const float* data, const float* hat, float* next,
+                              double* totals_out, void* stream);
+
 /* reduce.py:28-38 TripleSum: the three totals (device, 3 doubles) without scaling. */
 int plume_triple_sum(const int32_t shape[3], const float* a, const float* b, const float* c, double* sums,
                      double* totals_out, void* stream);

@@ -95,6 +95,7 @@ SIGNATURES = {
     "plume_smoke_scratch_doubles": [_INFO],
     "plume_smoke_budget": [_INFO, _P, _P, _P, _P, _P, _P, _P],
     "plume_triple_sum": [_SHAPE, _P, _P, _P, _P, _P, _P],
+    "plume_smoke_budget_static": [_INFO, _P, _P, _P, _P, _P],
     "plume_dissipate": [_INFO, _P, _P, _F, _F, _F, _P],
     "plume_grid_speed": [_INFO, _P, _P, _P, _P, _P],
     "plume_step": [ctypes.POINTER(PlumeStepState), ctypes.POINTER(PlumeStepParams), _P],

@@ -6,6 +6,7 @@
 #include <cstdarg>
 #include <cstdio>
 #include <cstring>
+#include <mutex>
 #include <string>
 #include <vector>
 
@@ -1056,4 +1057,65 @@ extern "C" int plume_step(const PlumeStepState* s, const PlumeStepParams* p, voi
                                                          p->apply_dissipation, p->smoke_keep, p->heat_keep, p->ambient_k);
   CHECK_LAUNCH("scale and dissipate");
   return mark();
+}
+
+// ---- the smoke budget without caller scratch --------------------------------------------------------------
+// Some callers cannot allocate device memory at the moment they run the budget: a host engine that hands
+// this library only the field arrays it owns, with its own allocator locked or budgeted, or code running
+// inside a region where any cudaMalloc would synchronise the device or is forbidden. For them,
+// plume_smoke_budget_static keeps its partial sums and its factor in one fixed array that lives in the
+// library's own device memory (allocated when the library's module loads on a device, held until the
+// process exits).
+namespace plume {
+
+constexpr long STATIC_BUDGET_MAX_LINES = 1L << 20;  // ny * nz: every (y, z) line summed along x
+constexpr long STATIC_BUDGET_BLOCKS = STATIC_BUDGET_MAX_LINES / SUM_BLOCK;
+// 3 totals' partials, then one slot whose first 4 bytes hold the float factor: 3 * 4096 + 1 doubles (96 KiB)
+static __device__ __align__(256) double g_budget_scratch[3 * STATIC_BUDGET_BLOCKS + 1];
+
+constexpr int MAX_DEVICES = 64;
+static std::mutex g_scratch_mutex;
+static double* g_scratch_address[MAX_DEVICES] = {};
+
+// The array's device address on the current device. The name g_budget_scratch, used in host code, is only a
+// host-side stand-in and must never be passed to a kernel; the real address is looked up once per device.
+static int static_budget_scratch(double** out) {
+  int device = 0;
+  int status = runtime_status("static smoke budget: current device", cudaGetDevice(&device));
+  if (status != PLUME_OK) return status;
+  if (device < 0 || device >= MAX_DEVICES) return fail(PLUME_ERR_INVALID, "static smoke budget: device %d", device);
+  std::lock_guard<std::mutex> lock(g_scratch_mutex);
+  if (g_scratch_address[device] == nullptr) {
+    void* address = nullptr;
+    status = runtime_status("static smoke budget: cudaGetSymbolAddress",
+                            cudaGetSymbolAddress(&address, g_budget_scratch));
+    if (status != PLUME_OK) return status;
+    g_scratch_address[device] = static_cast<double*>(address);
+  }
+  *out = g_scratch_address[device];
+  return PLUME_OK;
+}
+
+}  // namespace plume
+
+extern "C" int plume_smoke_budget_static(const PlumeGridInfo* info, const float* data, const float* hat, float* next,
+                                         double* totals_out, void* stream) {
+  CHECK_ARG(info && data && hat && next, "smoke_budget_static: null argument");
+  CHECK_ARG(valid_dims(info->dims), "smoke_budget_static: bad dims");
+  const Dims d = dims_of(*info);
+  const long lines = (long)d.n1 * d.n2;
+  CHECK_ARG(lines <= STATIC_BUDGET_MAX_LINES,
+            "smoke_budget_static: ny * nz = %ld lines exceeds the fixed scratch for %ld lines; use "
+            "plume_smoke_budget with caller scratch", lines, STATIC_BUDGET_MAX_LINES);
+  double* scratch = nullptr;
+  int status = static_budget_scratch(&scratch);
+  if (status != PLUME_OK) return status;
+  // Nothing in the array needs clearing: each call writes every partial it reads, and the factor, before use.
+  float* factor = reinterpret_cast<float*>(scratch + 3 * STATIC_BUDGET_BLOCKS);
+  cudaStream_t st = as_stream(stream);
+  status = launch_triple_sum(d, data, hat, next, scratch, factor, totals_out, st);
+  if (status != PLUME_OK) return status;
+  const long n = (long)d.n0 * d.n1 * d.n2;
+  k_scale<<<grid_stride_blocks(n), 256, 0, st>>>(next, n, factor);
+  return launch_status("static smoke budget scale");
 }
