@@ -108,7 +108,11 @@ typedef struct PlumeStepState {
   /* scratch: the smoke budget's partial sums (plume_smoke_scratch_doubles() doubles) and its factor (1 float) */
   double* sums;
   float* factor;
-  /* multigrid levels: levels[0] must alias pressure/divergence; coarser levels are caller-allocated */
+  /* scratch (optional, may be null): plume_advect_scratch_floats() floats; with it the MacCormack forward
+   * pass stores each element's clamp range and the correction does not trace forward a second time */
+  float* advect_scratch;
+  /* pressure-solve levels: levels[0] aliases pressure/divergence and its residual array is the sweeps' second
+   * pressure array (Gauss-Seidel uses levels[0] only); coarser multigrid levels are caller-allocated */
   const PlumeLevel* levels;
   int32_t level_count;
 } PlumeStepState;
@@ -182,12 +186,22 @@ int plume_divergence(const PlumeGridInfo* info, const float* u, const float* v, 
 int plume_subtract_gradient(const PlumeGridInfo* info, float* u, float* v, float* w, const float* q,
                             void* stream);
 
-/* pressure.py:124-141 GaussSeidel / red_black_sweeps (red_black_sweep_kernel, colour 0 then 1 per sweep). */
-int plume_red_black_sweeps(const PlumeGridInfo* info, float* q, const float* rhs, int32_t sweeps,
+/* pressure.py:124-141 GaussSeidel / red_black_sweeps (red_black_sweep_kernel, colour 0 then 1 per sweep).
+ * Each sweep is one launch that reads one pressure array and writes the other: `scratch` (same size as q,
+ * contents ignored) is the second array; the result is always left in q. */
+int plume_red_black_sweeps(const PlumeGridInfo* info, float* q, float* scratch, const float* rhs, int32_t sweeps,
                            float relaxation, void* stream);
 
-/* multigrid.py:124-147 Multigrid.__call__: `cycles` V-cycles over caller-allocated levels. */
+/* multigrid.py:124-147 Multigrid.__call__: `cycles` V-cycles over caller-allocated levels. Every level's
+ * `residual` array serves as its second pressure array (the residual is restricted without being stored). */
 int plume_multigrid(const PlumeLevel* levels, int32_t level_count, int32_t cycles, int32_t sweeps, void* stream);
+
+/* Pressure-solve strategy (no reference counterpart; results do not depend on it): levels with at least
+ * `tiled_min_cells` cells sweep in shared-memory tiles (one launch per sweep), smaller levels one colour per
+ * launch; the first level with at most `bottom_max_cells` cells and all coarser ones run in one launch:
+ * bottom_kind 1 an 8-CTA thread-block cluster (levels split in x-slabs over the CTAs' shared memory), 0 one
+ * 1024-thread block; at most 200 KiB of shared memory per CTA. Process-wide; defaults 2^40, 8192, 0. */
+int plume_tune_solver(long long tiled_min_cells, long long bottom_max_cells, int32_t bottom_kind);
 
 /* multigrid.py:36-43 residual_kernel. */
 int plume_residual(const PlumeGridInfo* info, const float* q, const float* rhs, float* residual, void* stream);
@@ -198,6 +212,7 @@ int plume_residual(const PlumeGridInfo* info, const float* q, const float* rhs, 
  * `sums` needs plume_smoke_scratch_doubles(info) doubles. If `totals_out` is not null the three totals are
  * also copied to it (device memory, 3 doubles). */
 int plume_smoke_scratch_doubles(const PlumeGridInfo* info);
+long long plume_advect_scratch_floats(const PlumeGridInfo* info);
 int plume_smoke_budget(const PlumeGridInfo* info, const float* data, const float* hat, float* next,
                        double* sums, float* factor, double* totals_out, void* stream);
 

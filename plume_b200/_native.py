@@ -54,7 +54,8 @@ class PlumeStepState(ctypes.Structure):
     _fields_ = [("info", PlumeGridInfo), ("u", PlumeField), ("v", PlumeField), ("w", PlumeField),
                 ("smoke", PlumeField), ("temperature", PlumeField), ("pressure", ctypes.c_void_p),
                 ("divergence", ctypes.c_void_p), ("curl", ctypes.c_void_p * 3), ("push", ctypes.c_void_p * 3),
-                ("sums", ctypes.c_void_p), ("factor", ctypes.c_void_p), ("levels", ctypes.POINTER(PlumeLevel)),
+                ("sums", ctypes.c_void_p), ("factor", ctypes.c_void_p), ("advect_scratch", ctypes.c_void_p),
+                ("levels", ctypes.POINTER(PlumeLevel)),
                 ("level_count", ctypes.c_int32)]
 
 
@@ -89,10 +90,12 @@ SIGNATURES = {
     "plume_project_begin": [_INFO, _P, _P, _P, _P, _P],
     "plume_divergence": [_INFO, _P, _P, _P, _P, _P],
     "plume_subtract_gradient": [_INFO, _P, _P, _P, _P, _P],
-    "plume_red_black_sweeps": [_INFO, _P, _P, _I, _F, _P],
+    "plume_red_black_sweeps": [_INFO, _P, _P, _P, _I, _F, _P],
     "plume_multigrid": [ctypes.POINTER(PlumeLevel), _I, _I, _I, _P],
     "plume_residual": [_INFO, _P, _P, _P, _P],
+    "plume_tune_solver": [ctypes.c_longlong, ctypes.c_longlong, _I],
     "plume_smoke_scratch_doubles": [_INFO],
+    "plume_advect_scratch_floats": [_INFO],
     "plume_smoke_budget": [_INFO, _P, _P, _P, _P, _P, _P, _P],
     "plume_triple_sum": [_SHAPE, _P, _P, _P, _P, _P, _P],
     "plume_smoke_budget_static": [_INFO, _P, _P, _P, _P, _P],
@@ -122,7 +125,7 @@ def lib() -> ctypes.CDLL:
         for name, argtypes in SIGNATURES.items():
             fn = getattr(loaded, name)
             fn.argtypes = argtypes
-            fn.restype = ctypes.c_int
+            fn.restype = ctypes.c_longlong if name == "plume_advect_scratch_floats" else ctypes.c_int
         _lib = loaded
     return _lib
 

@@ -53,6 +53,9 @@ struct Dims {
   int n0, n1, n2;
 };
 __device__ __forceinline__ int at(const Dims& d, int i, int j, int k) { return (i * d.n1 + j) * d.n2 + k; }
+__host__ __device__ __forceinline__ Dims dims_of(const PlumeGridInfo& info) {
+  return Dims{info.dims[0], info.dims[1], info.dims[2]};
+}
 
 // Trilinear sample at continuous index g, clamped to the array (sim/sample.py:10-29).
 __device__ __forceinline__ float sample_index_space(const float* __restrict__ f, const Dims& d, F3 g) {

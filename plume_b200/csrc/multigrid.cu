@@ -1,0 +1,783 @@
+// The pressure solve on the device (chadmv/plume src/plume/sim/pressure.py:124-141, multigrid.py:24-147):
+// red-black Gauss-Seidel sweeps and multigrid V-cycles, with the reference's update order and arithmetic.
+//
+// Launch structure of one V-cycle:
+//   - each full sweep (red then black) is one launch of k_rb_sweep: a tile of 8x8x32 cells and a 2-cell halo
+//     in shared memory; red is updated on the tile and a 1-cell shell, then black on the tile, so every value
+//     equals the one the two separate colour passes produce;
+//   - the residual, its restriction to the coarse level and the zeroing of the coarse pressure are one
+//     launch (k_residual_restrict);
+//   - prolongation is folded into the first post-smoothing sweep (the tile loads q + prolong(coarse));
+//   - every level from the first of at most 8192 cells down to the coarsest solve runs in one launch: one
+//     1024-thread block with all its arrays in shared memory (k_block_solve), or, selectable, one 8-CTA
+//     thread-block cluster with the larger levels split in x-slabs over distributed shared memory
+//     (k_cluster_solve).
+#include <cooperative_groups.h>
+
+#include <algorithm>
+#include <mutex>
+
+#include "poisson.cuh"
+
+namespace plume {
+
+constexpr int TILE_I = 8, TILE_J = 8, TILE_K = 32, HALO = 2;
+constexpr int QI = TILE_I + 2 * HALO, QJ = TILE_J + 2 * HALO, QK = TILE_K + 2 * HALO;  // pressure region
+constexpr int RI = TILE_I + 2, RJ = TILE_J + 2, RK = TILE_K + 2;                      // rhs region
+constexpr int SWEEP_THREADS = 256;
+constexpr int COARSEST_SWEEPS = 20;  // multigrid.py:24-33
+constexpr int COARSEST_SWEEPS_PER_CELL = 4;
+constexpr int BOTTOM_THREADS = 1024;
+constexpr int BOTTOM_MAX_LEVELS = 8;
+constexpr int BOTTOM_WARP_PAIRS = 128;  // levels with at most this many cell pairs per colour run on one warp
+// Per-level strategy (set by plume_tune_solver): levels of at least g_tiled_min_cells cells sweep in tiles,
+// smaller ones one colour per launch; the first level of at most g_bottom_max_cells cells and everything
+// below it runs in one block.
+static long g_tiled_min_cells = 1L << 40;  // measured: per-colour sweeps win while the levels fit in L2
+// Measured on B200 (128x192x128 and 16x24x16 hierarchies): the one-block solve from the first level of at
+// most 8192 cells beats the 8-CTA cluster solve, whose passes are bound by barrier latency.
+static long g_bottom_max_cells = 8192;
+static int g_bottom_kind = 0;  // 0: the one-block solve, 1: the cluster solve
+constexpr size_t BOTTOM_MAX_SMEM = 200 * 1024;
+
+
+// One full red-black sweep of a tile; with PROLONG the tile first adds the coarse correction
+// (prolong_add_kernel, multigrid.py:63-68) to every pressure it loads.
+// The sweep reads `q_in` and writes `q_out` (different arrays): a tile's halo belongs to its neighbours, which
+// may already have written their cells in the same launch.
+template <bool PROLONG, bool UNIFORM>
+__global__ void __launch_bounds__(SWEEP_THREADS)
+    k_rb_sweep(PlumeGridInfo info, const float* __restrict__ q_in, float* __restrict__ q_out,
+               const float* __restrict__ rhs, float relaxation, const float* __restrict__ coarse_q, Dims coarse) {
+  __shared__ float sq[QI * QJ * QK];
+  __shared__ float sr[RI * RJ * RK];
+  const int n0 = info.dims[0], n1 = info.dims[1], n2 = info.dims[2];
+  const int i0 = blockIdx.z * TILE_I, j0 = blockIdx.y * TILE_J, k0 = blockIdx.x * TILE_K;
+  const int t = threadIdx.x;
+  for (int idx = t; idx < QI * QJ * QK; idx += SWEEP_THREADS) {
+    const int a = idx / (QJ * QK), rem = idx - a * (QJ * QK), b = rem / QK, c = rem - b * QK;
+    const int gi = i0 - HALO + a, gj = j0 - HALO + b, gk = k0 - HALO + c;
+    float value = 0.0f;
+    if (gi >= 0 && gi < n0 && gj >= 0 && gj < n1 && gk >= 0 && gk < n2) {
+      value = __ldg(q_in + (gi * n1 + gj) * n2 + gk);
+      if (PROLONG) value = value + sample_index_space(coarse_q, coarse, prolong_point(gi, gj, gk));
+    }
+    sq[idx] = value;
+  }
+  for (int idx = t; idx < RI * RJ * RK; idx += SWEEP_THREADS) {
+    const int a = idx / (RJ * RK), rem = idx - a * (RJ * RK), b = rem / RK, c = rem - b * RK;
+    const int gi = i0 - 1 + a, gj = j0 - 1 + b, gk = k0 - 1 + c;
+    sr[idx] = (gi >= 0 && gi < n0 && gj >= 0 && gj < n1 && gk >= 0 && gk < n2) ? __ldg(rhs + (gi * n1 + gj) * n2 + gk)
+                                                                              : 0.0f;
+  }
+  __syncthreads();
+  auto qi = [&](int gi, int gj, int gk) { return ((gi - i0 + HALO) * QJ + (gj - j0 + HALO)) * QK + (gk - k0 + HALO); };
+  auto load = [&](int gi, int gj, int gk) { return sq[qi(gi, gj, gk)]; };
+  const float ghost = ghost_coupling(info);
+  // red (colour 0: i + j + k even) on the tile and its 1-cell shell; one red cell per pair along k
+  constexpr int RPK = RK / 2;
+  for (int p = t; p < RI * RJ * RPK; p += SWEEP_THREADS) {
+    const int a = p / (RJ * RPK), rem = p - a * (RJ * RPK), b = rem / RPK, kp = rem - b * RPK;
+    const int gi = i0 - 1 + a, gj = j0 - 1 + b, kbase = k0 - 1 + 2 * kp;
+    const int gk = kbase + ((gi + gj + kbase) & 1);
+    if (gi < 0 || gi >= n0 || gj < 0 || gj >= n1 || gk < 0 || gk >= n2) continue;
+    const int at_q = qi(gi, gj, gk);
+    const float r = sr[((gi - i0 + 1) * RJ + (gj - j0 + 1)) * RK + (gk - k0 + 1)];
+    float out;
+    if (relax_cell(UNIFORM, info, ghost, gi, gj, gk, sq[at_q], r, relaxation, load, out)) sq[at_q] = out;
+  }
+  __syncthreads();
+  // black (colour 1) on the tile
+  constexpr int TPK = TILE_K / 2;
+  for (int p = t; p < TILE_I * TILE_J * TPK; p += SWEEP_THREADS) {
+    const int a = p / (TILE_J * TPK), rem = p - a * (TILE_J * TPK), b = rem / TPK, kp = rem - b * TPK;
+    const int gi = i0 + a, gj = j0 + b, kbase = k0 + 2 * kp;
+    const int gk = kbase + (((gi + gj + kbase) & 1) ^ 1);
+    if (gi >= n0 || gj >= n1 || gk >= n2) continue;
+    const int at_q = qi(gi, gj, gk);
+    const float r = sr[((gi - i0 + 1) * RJ + (gj - j0 + 1)) * RK + (gk - k0 + 1)];
+    float out;
+    if (relax_cell(UNIFORM, info, ghost, gi, gj, gk, sq[at_q], r, relaxation, load, out)) sq[at_q] = out;
+  }
+  __syncthreads();
+  for (int idx = t; idx < TILE_I * TILE_J * TILE_K; idx += SWEEP_THREADS) {
+    const int a = idx / (TILE_J * TILE_K), rem = idx - a * (TILE_J * TILE_K), b = rem / TILE_K, c = rem - b * TILE_K;
+    const int gi = i0 + a, gj = j0 + b, gk = k0 + c;
+    if (gi < n0 && gj < n1 && gk < n2) q_out[(gi * n1 + gj) * n2 + gk] = sq[qi(gi, gj, gk)];
+  }
+}
+
+// One colour of a sweep in place (red_black_sweep_kernel, pressure.py:80-92): for levels too small to fill
+// the GPU with tiles. A colour reads only the other colour, so the in-place update is race-free.
+template <bool UNIFORM>
+__global__ void k_rb_colour(PlumeGridInfo info, float* q, const float* __restrict__ rhs, int color, float relaxation,
+                            const float* __restrict__ coarse_q, Dims coarse) {
+  const int ny = info.dims[1], nz = info.dims[2];
+  const int i = blockIdx.z, j = blockIdx.y * blockDim.y + threadIdx.y;
+  const int k = 2 * (blockIdx.x * blockDim.x + threadIdx.x) + ((i + j + color) & 1);
+  if (j >= ny || k >= nz) return;
+  const Dims d = dims_of(info);
+  auto load = [&](int a, int b, int c) { return q[at(d, a, b, c)]; };
+  const int idx = at(d, i, j, k);
+  float out;
+  if (relax_cell(UNIFORM, info, ghost_coupling(info), i, j, k, q[idx], __ldg(rhs + idx), relaxation, load, out))
+    q[idx] = out;
+}
+
+// prolong_add_kernel (multigrid.py:63-68), used when a level has no post-smoothing sweep to fold it into.
+__global__ void k_prolong_add(Dims coarse, Dims fine, const float* __restrict__ cq, float* __restrict__ q) {
+  const int i = blockIdx.z, j = blockIdx.y * blockDim.y + threadIdx.y, k = blockIdx.x * blockDim.x + threadIdx.x;
+  if (j >= fine.n1 || k >= fine.n2) return;
+  const int idx = at(fine, i, j, k);
+  q[idx] = q[idx] + sample_index_space(cq, coarse, prolong_point(i, j, k));
+}
+
+// residual_kernel + restrict_kernel (multigrid.py:36-60) + coarse.q.zero_() (:143): each coarse cell averages
+// the residuals of its (up to 8) children, summed in the reference's child order.
+__global__ void k_residual_restrict(PlumeGridInfo fine, const float* __restrict__ q, const float* __restrict__ rhs,
+                                    Dims coarse, float* __restrict__ coarse_rhs, float* __restrict__ coarse_q) {
+  const int i = blockIdx.z, j = blockIdx.y * blockDim.y + threadIdx.y, k = blockIdx.x * blockDim.x + threadIdx.x;
+  if (j >= coarse.n1 || k >= coarse.n2) return;
+  const Dims fd = dims_of(fine);
+  auto load = [&](int a, int b, int c) { return __ldg(q + at(fd, a, b, c)); };
+  const bool uniform = is_uniform(fine);
+  const float ghost = ghost_coupling(fine);
+  float total = 0.0f, count = 0.0f;
+#pragma unroll
+  for (int di = 0; di < 2; ++di)
+#pragma unroll
+    for (int dj = 0; dj < 2; ++dj)
+#pragma unroll
+      for (int dk = 0; dk < 2; ++dk) {
+        const int fi = 2 * i + di, fj = 2 * j + dj, fk = 2 * k + dk;
+        if (fi < fd.n0 && fj < fd.n1 && fk < fd.n2) {
+          const int idx = at(fd, fi, fj, fk);
+          total = total + residual_cell(uniform, fine, ghost, fi, fj, fk, __ldg(q + idx), __ldg(rhs + idx), load);
+          count = count + 1.0f;
+        }
+      }
+  const int out = at(coarse, i, j, k);
+  coarse_rhs[out] = total / count;
+  coarse_q[out] = 0.0f;
+}
+
+// ---- the cluster coarse solve --------------------------------------------------------------------------------
+// Every level from `first` down runs in one launch of one thread-block cluster (CLUSTER CTAs, one per SM).
+// A level above SINGLE_MAX_CELLS cells is split into slabs of whole x-planes, one slab per CTA, held in that
+// CTA's shared memory; a CTA reads its neighbours' boundary planes through distributed shared memory and
+// the cluster barrier separates the passes. Smaller levels live in CTA 0 alone and run with block or warp
+// barriers while the other CTAs wait at the next cluster barrier. Every cell gets exactly the reference's
+// update; only where the values are stored differs.
+
+constexpr int CLUSTER = 8;
+constexpr long SINGLE_MAX_CELLS = 1024;
+
+struct LevelView {
+  PlumeGridInfo info;
+  float* q;        // global arrays (loaded for the first level, written back for all)
+  float* rhs;
+  int planes;      // x-planes per CTA (the whole level when single)
+  int single;      // 1: the level lives in CTA 0
+  int offset;      // shared-memory float offset of the level's q block; its rhs block follows
+};
+
+struct ClusterArgs {
+  int count;
+  int sweeps;
+  LevelView lv[BOTTOM_MAX_LEVELS];
+};
+
+namespace cg = cooperative_groups;
+
+struct ClusterCtx {
+  cg::cluster_group cluster;
+  float* smem;
+  int rank;
+};
+
+// The CTA holding plane i (no division: slabs are `planes` planes long, CLUSTER of them).
+__device__ __forceinline__ int owner_of(const LevelView& L, int i) {
+  if (L.single) return 0;
+  int owner = 0;
+#pragma unroll
+  for (int r = 1; r < CLUSTER; ++r) owner += i >= r * L.planes;
+  return owner;
+}
+
+__device__ __forceinline__ int local_index(const LevelView& L, int owner, int i, int j, int k, bool rhs) {
+  const int n1 = L.info.dims[1], n2 = L.info.dims[2];
+  const int li = L.single ? i : i - owner * L.planes;
+  return L.offset + (rhs ? L.planes * n1 * n2 : 0) + (li * n1 + j) * n2 + k;
+}
+
+// q (or rhs) of a cell, read from whichever CTA holds its plane: a shared-memory load when it is this CTA.
+__device__ __forceinline__ float cell_load(const ClusterCtx& c, const LevelView& L, int i, int j, int k, bool rhs) {
+  const int owner = owner_of(L, i);
+  const int idx = local_index(L, owner, i, j, k, rhs);
+  if (owner == c.rank) return c.smem[idx];
+  return *c.cluster.map_shared_rank(c.smem + idx, owner);
+}
+
+__device__ __forceinline__ void cell_store(const ClusterCtx& c, const LevelView& L, int i, int j, int k, bool rhs,
+                                           float value) {
+  const int owner = owner_of(L, i);
+  const int idx = local_index(L, owner, i, j, k, rhs);
+  if (owner == c.rank) c.smem[idx] = value;
+  else *c.cluster.map_shared_rank(c.smem + idx, owner) = value;
+}
+
+// The x-planes [lo, hi) a CTA works on in a pass over level L: its own slab, or everything in CTA 0.
+__device__ __forceinline__ void my_planes(const ClusterCtx& c, const LevelView& L, int& lo, int& hi) {
+  const int n0 = L.info.dims[0];
+  if (L.single) {
+    lo = 0;
+    hi = c.rank == 0 ? n0 : 0;
+    return;
+  }
+  lo = imin_(c.rank * L.planes, n0);
+  hi = imin_(lo + L.planes, n0);
+}
+
+// One pass of cells of one colour over the planes [lo, hi), `threads` threads from thread 0.
+template <class Update>
+__device__ __forceinline__ void for_colour(const LevelView& L, int lo, int hi, int color, int threads, Update update) {
+  const int n1 = L.info.dims[1], n2 = L.info.dims[2];
+  const int pairs_k = (n2 + 1) / 2;
+  const int per_plane = n1 * pairs_k;
+  const int pairs = (hi - lo) * per_plane;
+  for (int p = threadIdx.x; p < pairs; p += threads) {
+    const int a = p / per_plane, rem = p - a * per_plane, j = rem / pairs_k, kp = rem - j * pairs_k;
+    const int i = lo + a;
+    const int k = 2 * kp + ((i + j + color) & 1);
+    if (k < n2) update(i, j, k);
+  }
+}
+
+// `sweeps` red-black sweeps of level L. Neighbours in the same x-plane are always this CTA's; the x-1 and
+// x+1 planes come from the neighbouring CTAs' shared memory at the slab edges. A single level small enough
+// for one warp syncs at warp level.
+__device__ void cluster_smooth(const ClusterCtx& c, const LevelView& L, int sweeps, float relaxation) {
+  const PlumeGridInfo& info = L.info;
+  const bool uniform = is_uniform(info);
+  const float ghost = ghost_coupling(info);
+  const int n0 = info.dims[0], n1 = info.dims[1], n2 = info.dims[2];
+  const int plane = n1 * n2;
+  int lo, hi;
+  my_planes(c, L, lo, hi);
+  float* q = c.smem + L.offset;               // this CTA's planes [lo, hi), then their rhs
+  const float* rhs = q + L.planes * plane;
+  const float* q_prev = (!L.single && lo > 0 && lo < hi) ? c.cluster.map_shared_rank(q + (L.planes - 1) * plane, c.rank - 1)
+                                                         : nullptr;
+  const float* q_next = (!L.single && hi < n0 && lo < hi) ? c.cluster.map_shared_rank(q, c.rank + 1) : nullptr;
+  auto update = [&](int i, int j, int k) {
+    const int idx = (i - lo) * plane + j * n2 + k;
+    auto load = [&](int a, int b, int cc) {
+      if (a == i) return q[idx + (b - j) * n2 + (cc - k)];
+      if (a == i - 1) return i - 1 >= lo ? q[idx - plane] : q_prev[j * n2 + k];
+      return i + 1 < hi ? q[idx + plane] : q_next[j * n2 + k];
+    };
+    float out;
+    if (relax_cell(uniform, info, ghost, i, j, k, q[idx], rhs[idx], relaxation, load, out)) q[idx] = out;
+  };
+  const int pairs_k = (n2 + 1) / 2;
+  const int per_plane = n1 * pairs_k;
+  const int t = threadIdx.x;
+  auto colour_pass = [&](int color, int threads) {
+    if (per_plane <= threads && (hi - lo) * per_plane > threads) {  // each thread owns a column of every plane
+      if (t < per_plane) {
+        const int j = t / pairs_k, kp = t - j * pairs_k;
+        for (int i = lo; i < hi; ++i) {
+          const int k = 2 * kp + ((i + j + color) & 1);
+          if (k < n2) update(i, j, k);
+        }
+      }
+    } else {
+      for_colour(L, lo, hi, color, threads, update);
+    }
+  };
+  if (L.single) {
+    const int pairs = n0 * per_plane;
+    const bool one_warp = pairs <= BOTTOM_WARP_PAIRS;
+    if (c.rank == 0 && (!one_warp || t < 32)) {
+      for (int s = 0; s < sweeps; ++s)
+        for (int color = 0; color < 2; ++color) {
+          if (one_warp) {
+            for_colour(L, lo, hi, color, 32, update);
+            __syncwarp();
+          } else {
+            colour_pass(color, BOTTOM_THREADS);
+            __syncthreads();
+          }
+        }
+    }
+    if (c.rank == 0) __syncthreads();  // the rest of CTA 0 waits for the warp that did the work
+    return;
+  }
+  for (int s = 0; s < sweeps; ++s)
+    for (int color = 0; color < 2; ++color) {
+      colour_pass(color, BOTTOM_THREADS);
+      c.cluster.sync();
+    }
+}
+
+// residual + restriction + zero coarse pressure (multigrid.py:36-60, :143) from F into C. Coarse planes are
+// shared out over the CTAs by slab; each writes into whichever CTA holds the coarse plane.
+__device__ void cluster_restrict(const ClusterCtx& c, const LevelView& F, const LevelView& C, bool single_only) {
+  const PlumeGridInfo& info = F.info;
+  const Dims fd = dims_of(info), cd = dims_of(C.info);
+  const bool uniform = is_uniform(info);
+  const float ghost = ghost_coupling(info);
+  auto load = [&](int a, int b, int k) { return cell_load(c, F, a, b, k, false); };
+  int lo, hi;
+  if (single_only) {
+    lo = 0;
+    hi = c.rank == 0 ? cd.n0 : 0;
+  } else {
+    const int per = (cd.n0 + CLUSTER - 1) / CLUSTER;
+    lo = imin_(c.rank * per, cd.n0);
+    hi = imin_(lo + per, cd.n0);
+  }
+  const int cells = (hi - lo) * cd.n1 * cd.n2;
+  for (int idx = threadIdx.x; idx < cells; idx += BOTTOM_THREADS) {
+    const int a = idx / (cd.n1 * cd.n2), rem = idx - a * (cd.n1 * cd.n2), j = rem / cd.n2, k = rem - j * cd.n2;
+    const int i = lo + a;
+    float total = 0.0f, count = 0.0f;
+    for (int di = 0; di < 2; ++di)
+      for (int dj = 0; dj < 2; ++dj)
+        for (int dk = 0; dk < 2; ++dk) {
+          const int fi = 2 * i + di, fj = 2 * j + dj, fk = 2 * k + dk;
+          if (fi < fd.n0 && fj < fd.n1 && fk < fd.n2) {
+            total = total + residual_cell(uniform, info, ghost, fi, fj, fk, cell_load(c, F, fi, fj, fk, false),
+                                          cell_load(c, F, fi, fj, fk, true), load);
+            count = count + 1.0f;
+          }
+        }
+    cell_store(c, C, i, j, k, true, total / count);
+    cell_store(c, C, i, j, k, false, 0.0f);
+  }
+}
+
+// prolong_add_kernel (multigrid.py:63-68): each CTA adds the coarse correction to the fine planes it holds.
+__device__ void cluster_prolong(const ClusterCtx& c, const LevelView& F, const LevelView& C) {
+  const Dims fd = dims_of(F.info), cd = dims_of(C.info);
+  int lo, hi;
+  my_planes(c, F, lo, hi);
+  const int cells = (hi - lo) * fd.n1 * fd.n2;
+  for (int idx = threadIdx.x; idx < cells; idx += BOTTOM_THREADS) {
+    const int a = idx / (fd.n1 * fd.n2), rem = idx - a * (fd.n1 * fd.n2), j = rem / fd.n2, k = rem - j * fd.n2;
+    const int i = lo + a;
+    const F3 g = prolong_point(i, j, k);  // sample_index_space (sample.py:10-29) on the coarse level
+    const float x = clampf_(g[0], 0.0f, (float)(cd.n0 - 1)), y = clampf_(g[1], 0.0f, (float)(cd.n1 - 1)),
+                z = clampf_(g[2], 0.0f, (float)(cd.n2 - 1));
+    const int i0 = (int)x, j0 = (int)y, k0 = (int)z;
+    const int i1 = imin_(i0 + 1, cd.n0 - 1), j1 = imin_(j0 + 1, cd.n1 - 1), k1 = imin_(k0 + 1, cd.n2 - 1);
+    const float tx = x - (float)i0, ty = y - (float)j0, tz = z - (float)k0;
+    auto cq = [&](int a2, int b2, int k2) { return cell_load(c, C, a2, b2, k2, false); };
+    const float c00 = lerpf_(cq(i0, j0, k0), cq(i1, j0, k0), tx);
+    const float c10 = lerpf_(cq(i0, j1, k0), cq(i1, j1, k0), tx);
+    const float c01 = lerpf_(cq(i0, j0, k1), cq(i1, j0, k1), tx);
+    const float c11 = lerpf_(cq(i0, j1, k1), cq(i1, j1, k1), tx);
+    const int at_q = local_index(F, c.rank, i, j, k, false);  // a plane this CTA holds
+    c.smem[at_q] = c.smem[at_q] + lerpf_(lerpf_(c00, c10, ty), lerpf_(c01, c11, ty), tz);
+  }
+}
+
+// A barrier for the level just processed: the cluster for split levels, CTA 0's block for single ones.
+__device__ __forceinline__ void level_barrier(const ClusterCtx& c, bool cluster_wide) {
+  if (cluster_wide) c.cluster.sync();
+  else if (c.rank == 0) __syncthreads();
+}
+
+__global__ void __launch_bounds__(BOTTOM_THREADS) k_cluster_solve(ClusterArgs b) {
+  extern __shared__ float smem[];
+  ClusterCtx c{cg::this_cluster(), smem, (int)cg::this_cluster().block_rank()};
+  {  // the first level's pressure and right-hand side, each CTA its planes
+    const LevelView& L = b.lv[0];
+    int lo, hi;
+    my_planes(c, L, lo, hi);
+    const int n1 = L.info.dims[1], n2 = L.info.dims[2];
+    const int cells = (hi - lo) * n1 * n2;
+    const long base = (long)lo * n1 * n2;
+    float* q = smem + L.offset;
+    float* rhs = q + L.planes * n1 * n2;
+    for (int idx = threadIdx.x; idx < cells; idx += BOTTOM_THREADS) {
+      q[idx] = L.q[base + idx];
+      rhs[idx] = L.rhs[base + idx];
+    }
+  }
+  c.cluster.sync();
+  const int last = b.count - 1;
+  for (int l = 0; l < last; ++l) {  // down: smooth, then residual and restriction into the next level
+    const LevelView& F = b.lv[l];
+    const LevelView& C = b.lv[l + 1];
+    cluster_smooth(c, F, b.sweeps, 1.0f);
+    cluster_restrict(c, F, C, F.single != 0);
+    level_barrier(c, F.single == 0);
+  }
+  {  // the coarsest solve (multigrid.py:132-136)
+    const LevelView& L = b.lv[last];
+    const int longest = imax_(L.info.dims[0], imax_(L.info.dims[1], L.info.dims[2]));
+    cluster_smooth(c, L, imax_(COARSEST_SWEEPS, COARSEST_SWEEPS_PER_CELL * longest), 1.5f);
+  }
+  for (int l = last - 1; l >= 0; --l) {  // up: prolong the coarse correction, smooth
+    const LevelView& F = b.lv[l];
+    const LevelView& C = b.lv[l + 1];
+    if (F.single == 0 && C.single) c.cluster.sync();  // the single part is done before its correction is read
+    cluster_prolong(c, F, C);
+    level_barrier(c, F.single == 0);
+    cluster_smooth(c, F, b.sweeps, 1.0f);
+  }
+  c.cluster.sync();
+  for (int l = 0; l < b.count; ++l) {  // every level's pressure (and the coarse right-hand sides) back out
+    const LevelView& L = b.lv[l];
+    int lo, hi;
+    my_planes(c, L, lo, hi);
+    const int n1 = L.info.dims[1], n2 = L.info.dims[2];
+    const int cells = (hi - lo) * n1 * n2;
+    const long base = (long)lo * n1 * n2;
+    const float* q = smem + L.offset;
+    const float* rhs = q + L.planes * n1 * n2;
+    for (int idx = threadIdx.x; idx < cells; idx += BOTTOM_THREADS) {
+      L.q[base + idx] = q[idx];
+      if (l > 0) L.rhs[base + idx] = rhs[idx];
+    }
+  }
+  c.cluster.sync();  // no CTA leaves while another may still read its shared memory
+}
+
+// ---- the one-block coarse solve (alternative bottom: every level in one CTA's shared memory) --------------
+
+struct BlockArgs {
+  int count;
+  int sweeps;
+  PlumeLevel lv[BOTTOM_MAX_LEVELS];
+  int offset[BOTTOM_MAX_LEVELS];
+};
+
+__device__ void block_smooth(const PlumeGridInfo& info, float* q, const float* rhs, int sweeps, float relaxation) {
+  const Dims d = dims_of(info);
+  const int pairs_k = (d.n2 + 1) / 2;
+  const int pairs = d.n0 * d.n1 * pairs_k;
+  auto load = [&](int a, int b, int c) { return q[at(d, a, b, c)]; };
+  const bool uniform = is_uniform(info);
+  const float ghost = ghost_coupling(info);
+  const bool one_warp = pairs <= BOTTOM_WARP_PAIRS;
+  if (!one_warp || threadIdx.x < 32) {
+    for (int s = 0; s < sweeps; ++s)
+      for (int color = 0; color < 2; ++color) {
+        for (int p = threadIdx.x; p < pairs; p += one_warp ? 32 : BOTTOM_THREADS) {
+          const int i = p / (d.n1 * pairs_k), rem = p - i * (d.n1 * pairs_k), j = rem / pairs_k, kp = rem - j * pairs_k;
+          const int k = 2 * kp + ((i + j + color) & 1);
+          if (k >= d.n2) continue;
+          const int idx = at(d, i, j, k);
+          float out;
+          if (relax_cell(uniform, info, ghost, i, j, k, q[idx], rhs[idx], relaxation, load, out)) q[idx] = out;
+        }
+        if (one_warp) __syncwarp();
+        else __syncthreads();
+      }
+  }
+  __syncthreads();
+}
+
+__global__ void __launch_bounds__(BOTTOM_THREADS) k_block_solve(BlockArgs b) {
+  extern __shared__ float smem[];
+  const int t = threadIdx.x;
+  {
+    const Dims d = dims_of(b.lv[0].info);
+    const int n = d.n0 * d.n1 * d.n2;
+    float* q = smem + b.offset[0];
+    for (int idx = t; idx < n; idx += BOTTOM_THREADS) {
+      q[idx] = b.lv[0].q[idx];
+      q[n + idx] = b.lv[0].rhs[idx];
+    }
+  }
+  __syncthreads();
+  for (int l = 0; l + 1 < b.count; ++l) {
+    const PlumeGridInfo& info = b.lv[l].info;
+    const Dims fd = dims_of(info), cd = dims_of(b.lv[l + 1].info);
+    float* q = smem + b.offset[l];
+    float* rhs = q + fd.n0 * fd.n1 * fd.n2;
+    float* cq = smem + b.offset[l + 1];
+    float* crhs = cq + cd.n0 * cd.n1 * cd.n2;
+    block_smooth(info, q, rhs, b.sweeps, 1.0f);
+    auto load = [&](int a, int bb, int c) { return q[at(fd, a, bb, c)]; };
+    const bool uniform = is_uniform(info);
+    const float ghost = ghost_coupling(info);
+    const int coarse_cells = cd.n0 * cd.n1 * cd.n2;
+    for (int idx = t; idx < coarse_cells; idx += BOTTOM_THREADS) {
+      const int i = idx / (cd.n1 * cd.n2), rem = idx - i * (cd.n1 * cd.n2), j = rem / cd.n2, k = rem - j * cd.n2;
+      float total = 0.0f, count = 0.0f;
+      for (int di = 0; di < 2; ++di)
+        for (int dj = 0; dj < 2; ++dj)
+          for (int dk = 0; dk < 2; ++dk) {
+            const int fi = 2 * i + di, fj = 2 * j + dj, fk = 2 * k + dk;
+            if (fi < fd.n0 && fj < fd.n1 && fk < fd.n2) {
+              const int f = at(fd, fi, fj, fk);
+              total = total + residual_cell(uniform, info, ghost, fi, fj, fk, q[f], rhs[f], load);
+              count = count + 1.0f;
+            }
+          }
+      crhs[idx] = total / count;
+      cq[idx] = 0.0f;
+    }
+    __syncthreads();
+  }
+  {
+    const PlumeGridInfo& info = b.lv[b.count - 1].info;
+    const Dims d = dims_of(info);
+    float* q = smem + b.offset[b.count - 1];
+    const int longest = imax_(d.n0, imax_(d.n1, d.n2));
+    block_smooth(info, q, q + d.n0 * d.n1 * d.n2, imax_(COARSEST_SWEEPS, COARSEST_SWEEPS_PER_CELL * longest), 1.5f);
+  }
+  for (int l = b.count - 2; l >= 0; --l) {
+    const PlumeGridInfo& info = b.lv[l].info;
+    const Dims fd = dims_of(info), cd = dims_of(b.lv[l + 1].info);
+    float* q = smem + b.offset[l];
+    const float* cq = smem + b.offset[l + 1];
+    const int n = fd.n0 * fd.n1 * fd.n2;
+    for (int idx = t; idx < n; idx += BOTTOM_THREADS) {
+      const int i = idx / (fd.n1 * fd.n2), rem = idx - i * (fd.n1 * fd.n2), j = rem / fd.n2, k = rem - j * fd.n2;
+      q[idx] = q[idx] + sample_plain(cq, cd, prolong_point(i, j, k));
+    }
+    __syncthreads();
+    block_smooth(info, q, q + n, b.sweeps, 1.0f);
+  }
+  for (int l = 0; l < b.count; ++l) {
+    const Dims d = dims_of(b.lv[l].info);
+    const int n = d.n0 * d.n1 * d.n2;
+    const float* q = smem + b.offset[l];
+    for (int idx = t; idx < n; idx += BOTTOM_THREADS) {
+      b.lv[l].q[idx] = q[idx];
+      if (l > 0) b.lv[l].rhs[idx] = q[n + idx];
+    }
+  }
+}
+
+// ---- host side --------------------------------------------------------------------------------------------
+
+static long cells_of(const PlumeGridInfo& info) { return (long)info.dims[0] * info.dims[1] * info.dims[2]; }
+
+static dim3 tile_grid(const PlumeGridInfo& info) {
+  return dim3((info.dims[2] + TILE_K - 1) / TILE_K, (info.dims[1] + TILE_J - 1) / TILE_J,
+              (info.dims[0] + TILE_I - 1) / TILE_I);
+}
+
+// A level's pressure lives in two arrays: sweeps alternate between them. `cur` holds the current values.
+struct Pressure {
+  float* cur;
+  float* other;
+  void flip() { std::swap(cur, other); }
+};
+
+static bool uniform_level(const PlumeGridInfo& info) {
+  return info.fill_hi[0] == 1.0f && info.fill_hi[1] == 1.0f && info.fill_hi[2] == 1.0f;
+}
+
+template <bool PROLONG>
+static void launch_tiled(const PlumeGridInfo& info, Pressure& q, const float* rhs, float relaxation,
+                         const float* coarse_q, Dims cd, cudaStream_t st) {
+  if (uniform_level(info))
+    k_rb_sweep<PROLONG, true><<<tile_grid(info), SWEEP_THREADS, 0, st>>>(info, q.cur, q.other, rhs, relaxation, coarse_q, cd);
+  else
+    k_rb_sweep<PROLONG, false><<<tile_grid(info), SWEEP_THREADS, 0, st>>>(info, q.cur, q.other, rhs, relaxation, coarse_q, cd);
+}
+
+static int colour_sweep(const PlumeGridInfo& info, float* q, const float* rhs, float relaxation, cudaStream_t st) {
+  const Dims d = dims_of(info);
+  const dim3 grid(((d.n2 + 1) / 2 + TZ - 1) / TZ, (d.n1 + TY - 1) / TY, d.n0);
+  for (int color = 0; color < 2; ++color) {
+    if (uniform_level(info))
+      k_rb_colour<true><<<grid, cell_block(), 0, st>>>(info, q, rhs, color, relaxation, nullptr, Dims{1, 1, 1});
+    else
+      k_rb_colour<false><<<grid, cell_block(), 0, st>>>(info, q, rhs, color, relaxation, nullptr, Dims{1, 1, 1});
+    int status = launch_status("red-black colour");
+    if (status != PLUME_OK) return status;
+  }
+  return PLUME_OK;
+}
+
+// `sweeps` full sweeps; when `coarse` is given its correction is prolonged first (folded into the first tiled
+// sweep on large levels).
+static int sweeps_with_prolong(const PlumeGridInfo& info, Pressure& q, const float* rhs, int sweeps, float relaxation,
+                               const float* coarse_q, const PlumeGridInfo* coarse, cudaStream_t st) {
+  int s = 0;
+  const bool tiled = cells_of(info) >= g_tiled_min_cells;
+  if (coarse) {
+    const Dims cd = dims_of(*coarse);
+    if (sweeps == 0 || !tiled) {
+      const Dims fd = dims_of(info);
+      k_prolong_add<<<cell_grid(fd.n0, fd.n1, fd.n2), cell_block(), 0, st>>>(cd, fd, coarse_q, q.cur);
+      int status = launch_status("prolong");
+      if (status != PLUME_OK) return status;
+    } else {
+      launch_tiled<true>(info, q, rhs, relaxation, coarse_q, cd, st);
+      int status = launch_status("red-black sweep with prolongation");
+      if (status != PLUME_OK) return status;
+      q.flip();
+      s = 1;
+    }
+  }
+  for (; s < sweeps; ++s) {
+    if (tiled) {
+      launch_tiled<false>(info, q, rhs, relaxation, nullptr, Dims{1, 1, 1}, st);
+      int status = launch_status("red-black sweep");
+      if (status != PLUME_OK) return status;
+      q.flip();
+    } else {
+      int status = colour_sweep(info, q.cur, rhs, relaxation, st);
+      if (status != PLUME_OK) return status;
+    }
+  }
+  return PLUME_OK;
+}
+
+// Sweeps on `q` with `scratch` as the second array; the result always ends in `q`.
+int red_black_sweeps(const PlumeGridInfo& info, float* q, float* scratch, const float* rhs, int sweeps,
+                     float relaxation, cudaStream_t st) {
+  Pressure p{q, scratch};
+  int status = sweeps_with_prolong(info, p, rhs, sweeps, relaxation, nullptr, nullptr, st);
+  if (status != PLUME_OK || p.cur == q) return status;
+  return runtime_status("pressure copy-back", cudaMemcpyAsync(q, p.cur, sizeof(float) * (size_t)cells_of(info),
+                                                              cudaMemcpyDeviceToDevice, st));
+}
+
+// The first level from which the rest of the hierarchy runs in one cluster launch (count when none fits),
+// and that launch's per-CTA shared memory.
+static int bottom_start(const PlumeLevel* levels, int count, size_t* smem_bytes) {
+  for (int first = 0; first < count; ++first) {
+    if (count - first > BOTTOM_MAX_LEVELS || cells_of(levels[first].info) > g_bottom_max_cells) continue;
+    size_t bytes = 0;
+    for (int l = first; l < count; ++l) {
+      const PlumeGridInfo& info = levels[l].info;
+      const bool single = g_bottom_kind == 0 || cells_of(info) <= SINGLE_MAX_CELLS;
+      const long planes = single ? info.dims[0] : (info.dims[0] + CLUSTER - 1) / CLUSTER;
+      bytes += 2 * sizeof(float) * (size_t)planes * info.dims[1] * info.dims[2];
+    }
+    if (bytes > BOTTOM_MAX_SMEM) continue;
+    *smem_bytes = bytes;
+    return first;
+  }
+  return count;
+}
+
+static int launch_bottom(const PlumeLevel* levels, int count, int sweeps, size_t smem, cudaStream_t st) {
+  static std::mutex mutex;
+  static bool configured[64] = {};
+  int device = 0;
+  int status = runtime_status("current device", cudaGetDevice(&device));
+  if (status != PLUME_OK) return status;
+  {
+    std::lock_guard<std::mutex> lock(mutex);
+    if (device >= 0 && device < 64 && !configured[device]) {
+      status = runtime_status("coarse solve shared memory",
+                              cudaFuncSetAttribute(k_cluster_solve, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                                   (int)BOTTOM_MAX_SMEM));
+      if (status == PLUME_OK)
+        status = runtime_status("coarse solve shared memory",
+                                cudaFuncSetAttribute(k_block_solve, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                                     (int)BOTTOM_MAX_SMEM));
+      if (status != PLUME_OK) return status;
+      configured[device] = true;
+    }
+  }
+  if (g_bottom_kind == 0) {
+    BlockArgs b{};
+    b.count = count;
+    b.sweeps = sweeps;
+    int offset = 0;
+    for (int l = 0; l < count; ++l) {
+      b.lv[l] = levels[l];
+      b.offset[l] = offset;
+      offset += 2 * (int)cells_of(levels[l].info);
+    }
+    k_block_solve<<<1, BOTTOM_THREADS, smem, st>>>(b);
+    return launch_status("coarse-level block solve");
+  }
+  ClusterArgs b{};
+  b.count = count;
+  b.sweeps = sweeps;
+  int offset = 0;
+  for (int l = 0; l < count; ++l) {
+    LevelView& L = b.lv[l];
+    L.info = levels[l].info;
+    L.q = levels[l].q;
+    L.rhs = levels[l].rhs;
+    L.single = cells_of(L.info) <= SINGLE_MAX_CELLS ? 1 : 0;
+    L.planes = L.single ? L.info.dims[0] : (L.info.dims[0] + CLUSTER - 1) / CLUSTER;
+    L.offset = offset;
+    offset += 2 * L.planes * L.info.dims[1] * L.info.dims[2];
+  }
+  cudaLaunchConfig_t config = {};
+  config.gridDim = dim3(CLUSTER, 1, 1);
+  config.blockDim = dim3(BOTTOM_THREADS, 1, 1);
+  config.dynamicSmemBytes = smem;
+  config.stream = st;
+  cudaLaunchAttribute attribute[1];
+  attribute[0].id = cudaLaunchAttributeClusterDimension;
+  attribute[0].val.clusterDim.x = CLUSTER;
+  attribute[0].val.clusterDim.y = 1;
+  attribute[0].val.clusterDim.z = 1;
+  config.attrs = attribute;
+  config.numAttrs = 1;
+  status = runtime_status("coarse-level cluster solve", cudaLaunchKernelEx(&config, k_cluster_solve, b));
+  if (status != PLUME_OK) return status;
+  return launch_status("coarse-level cluster solve");
+}
+
+// One V-cycle below `index` (multigrid.py:130-147). Every level keeps its pressure in q and uses its residual
+// array as the sweeps' second array; the residual itself is never stored (k_residual_restrict).
+static int v_cycle(const PlumeLevel* levels, int count, int index, Pressure& q, int bottom, size_t smem, int sweeps,
+                   cudaStream_t st) {
+  const PlumeLevel& lv = levels[index];
+  if (index == bottom) {
+    PlumeLevel first[BOTTOM_MAX_LEVELS];
+    for (int l = bottom; l < count && l - bottom < BOTTOM_MAX_LEVELS; ++l) first[l - bottom] = levels[l];
+    first[0].q = q.cur;
+    return launch_bottom(first, count - bottom, sweeps, smem, st);
+  }
+  if (index == count - 1) {
+    const int longest = std::max(lv.info.dims[0], std::max(lv.info.dims[1], lv.info.dims[2]));
+    return sweeps_with_prolong(lv.info, q, lv.rhs, std::max(COARSEST_SWEEPS, COARSEST_SWEEPS_PER_CELL * longest), 1.5f,
+                               nullptr, nullptr, st);
+  }
+  int status = sweeps_with_prolong(lv.info, q, lv.rhs, sweeps, 1.0f, nullptr, nullptr, st);
+  if (status != PLUME_OK) return status;
+  const PlumeLevel& coarse = levels[index + 1];
+  const Dims cd = dims_of(coarse.info);
+  k_residual_restrict<<<cell_grid(cd.n0, cd.n1, cd.n2), cell_block(), 0, st>>>(lv.info, q.cur, lv.rhs, cd, coarse.rhs,
+                                                                             coarse.q);
+  if ((status = launch_status("residual and restriction")) != PLUME_OK) return status;
+  Pressure coarse_q{coarse.q, coarse.residual};
+  if ((status = v_cycle(levels, count, index + 1, coarse_q, bottom, smem, sweeps, st)) != PLUME_OK) return status;
+  if (coarse_q.cur != coarse.q) {  // an odd number of coarsest sweeps left the result in the second array
+    status = runtime_status("coarse pressure copy", cudaMemcpyAsync(coarse.q, coarse_q.cur, sizeof(float) * cd.n0 * cd.n1 * cd.n2,
+                                                                    cudaMemcpyDeviceToDevice, st));
+    if (status != PLUME_OK) return status;
+  }
+  return sweeps_with_prolong(lv.info, q, lv.rhs, sweeps, 1.0f, coarse.q, &coarse.info, st);
+}
+
+int multigrid_cycles(const PlumeLevel* levels, int count, int cycles, int sweeps, cudaStream_t st) {
+  size_t smem = 0;
+  const int bottom = bottom_start(levels, count, &smem);
+  Pressure q{levels[0].q, levels[0].residual};
+  for (int c = 0; c < cycles; ++c) {
+    int status = v_cycle(levels, count, 0, q, bottom, smem, sweeps, st);
+    if (status != PLUME_OK) return status;
+  }
+  if (q.cur == levels[0].q) return PLUME_OK;
+  return runtime_status("pressure copy-back", cudaMemcpyAsync(levels[0].q, q.cur, sizeof(float) * (size_t)cells_of(levels[0].info),
+                                                              cudaMemcpyDeviceToDevice, st));
+}
+
+}  // namespace plume
+
+extern "C" int plume_tune_solver(long long tiled_min_cells, long long bottom_max_cells, int32_t bottom_kind) {
+  if (tiled_min_cells < 1 || bottom_max_cells < 0 || bottom_kind < 0 || bottom_kind > 1)
+    return plume::fail(PLUME_ERR_INVALID, "tune_solver: thresholds must be positive, bottom_kind 0 or 1");
+  plume::g_tiled_min_cells = (long)tiled_min_cells;
+  plume::g_bottom_max_cells = (long)bottom_max_cells;
+  plume::g_bottom_kind = bottom_kind;
+  return PLUME_OK;
+}

@@ -1,0 +1,178 @@
+// The variable-coefficient 7-point Poisson stencil of the pressure solve (chadmv/plume
+// src/plume/sim/pressure.py:39-92, multigrid.py:36-43), written once for every place that evaluates it:
+// global memory, shared-memory tiles and the single-block coarse solve. `load(i, j, k)` returns the
+// pressure of an in-grid neighbour; the order of float operations is the reference's.
+#pragma once
+
+#include "common.cuh"
+
+namespace plume {
+
+// The share of a cell's width along `axis` inside the domain: 1 except a coarse level's overhang.
+__device__ __forceinline__ float cell_fill(const PlumeGridInfo& info, int axis, int index) {
+  return index == info.dims[axis] - 1 ? info.fill_hi[axis] : 1.0f;
+}
+
+__device__ __forceinline__ float cell_volume(const PlumeGridInfo& info, int i, int j, int k) {
+  return cell_fill(info, 0, i) * cell_fill(info, 1, j) * cell_fill(info, 2, k);
+}
+
+// neighbor_sum (pressure.py:52-77): (sum of coupling * neighbour pressure, sum of couplings). Open-face ghosts
+// hold pressure 0 at ghost_gap; closed faces couple nothing.
+template <class Load>
+__device__ __forceinline__ void neighbor_sum(const PlumeGridInfo& info, int i, int j, int k, Load load, float& sq,
+                                             float& sc) {
+  const int c[3] = {i, j, k};
+  sq = 0.0f;
+  sc = 0.0f;
+#pragma unroll
+  for (int axis = 0; axis < 3; ++axis) {
+    float area = 1.0f;
+#pragma unroll
+    for (int other = 0; other < 3; ++other)
+      if (other != axis) area = area * cell_fill(info, other, c[other]);
+    const float own = cell_fill(info, axis, c[axis]);
+    float tq[2], tc[2];
+#pragma unroll
+    for (int side = 0; side < 2; ++side) {
+      const int step = side == 0 ? -1 : 1;
+      const int n = c[axis] + step;
+      if (n >= 0 && n < info.dims[axis]) {
+        float coupling = area / (0.5f * (own + cell_fill(info, axis, n)));
+        const float neighbour = axis == 0 ? load(n, j, k) : (axis == 1 ? load(i, n, k) : load(i, j, n));
+        tq[side] = coupling * neighbour;
+        tc[side] = coupling;
+      } else if ((step < 0 && info.open_lo[axis] == 1) || (step > 0 && info.open_hi[axis] == 1)) {
+        tq[side] = 0.0f;
+        tc[side] = area / (0.5f * own + info.ghost_gap);
+      } else {
+        tq[side] = 0.0f;
+        tc[side] = 0.0f;
+      }
+    }
+    sq = (sq + tq[0]) + tq[1];
+    sc = (sc + tc[0]) + tc[1];
+  }
+}
+
+// One red-black update (red_black_sweep_kernel, pressure.py:80-92). Returns false, leaving `out` alone, for
+// a cell with no coupling at all.
+template <class Load>
+__device__ __forceinline__ bool relaxed(const PlumeGridInfo& info, int i, int j, int k, float q, float rhs,
+                                        float relaxation, Load load, float& out) {
+  float sq, sc;
+  neighbor_sum(info, i, j, k, load, sq, sc);
+  if (sc == 0.0f) return false;
+  float source = cell_volume(info, i, j, k) * info.cell_m * info.cell_m * rhs;
+  float target = (sq - source) / sc;
+  out = q + relaxation * (target - q);
+  return true;
+}
+
+// residual_kernel (multigrid.py:36-43): rhs - A q.
+template <class Load>
+__device__ __forceinline__ float residual_at(const PlumeGridInfo& info, int i, int j, int k, float q, float rhs,
+                                             Load load) {
+  float sq, sc;
+  neighbor_sum(info, i, j, k, load, sq, sc);
+  float scale = cell_volume(info, i, j, k) * info.cell_m * info.cell_m;
+  return rhs - (sq - sc * q) / scale;
+}
+
+// ---- the uniform-coefficient case ---------------------------------------------------------------------------
+// When every fill is 1 (the simulation grid, and every coarse level of an axis that halves evenly), each
+// interior coupling is area / (0.5 * (own + neighbour)) = 1 / (0.5 * 2) = 1 exactly, so coupling * q == q, and
+// an open face's ghost couples with 1 / (0.5 + ghost_gap). The functions below skip the per-neighbour
+// divisions but produce the same floats as the general ones.
+__device__ __forceinline__ bool is_uniform(const PlumeGridInfo& info) {
+  return info.fill_hi[0] == 1.0f && info.fill_hi[1] == 1.0f && info.fill_hi[2] == 1.0f;
+}
+
+__device__ __forceinline__ float ghost_coupling(const PlumeGridInfo& info) { return 1.0f / (0.5f + info.ghost_gap); }
+
+template <class Load>
+__device__ __forceinline__ void neighbor_sum_uniform(const PlumeGridInfo& info, float ghost, int i, int j, int k,
+                                                     Load load, float& sq, float& sc) {
+  const int c[3] = {i, j, k};
+  sq = 0.0f;
+  sc = 0.0f;
+#pragma unroll
+  for (int axis = 0; axis < 3; ++axis) {
+    float tq0 = 0.0f, tc0 = 0.0f, tq1 = 0.0f, tc1 = 0.0f;
+    if (c[axis] > 0) {
+      tq0 = axis == 0 ? load(i - 1, j, k) : (axis == 1 ? load(i, j - 1, k) : load(i, j, k - 1));
+      tc0 = 1.0f;
+    } else if (info.open_lo[axis] == 1) {
+      tc0 = ghost;
+    }
+    if (c[axis] < info.dims[axis] - 1) {
+      tq1 = axis == 0 ? load(i + 1, j, k) : (axis == 1 ? load(i, j + 1, k) : load(i, j, k + 1));
+      tc1 = 1.0f;
+    } else if (info.open_hi[axis] == 1) {
+      tc1 = ghost;
+    }
+    sq = (sq + tq0) + tq1;
+    sc = (sc + tc0) + tc1;
+  }
+}
+
+template <class Load>
+__device__ __forceinline__ bool relaxed_uniform(const PlumeGridInfo& info, float ghost, int i, int j, int k, float q,
+                                                float rhs, float relaxation, Load load, float& out) {
+  float sq, sc;
+  neighbor_sum_uniform(info, ghost, i, j, k, load, sq, sc);
+  if (sc == 0.0f) return false;
+  float source = info.cell_m * info.cell_m * rhs;  // cell volume 1: (1 * cell_m) * cell_m == cell_m * cell_m
+  float target = (sq - source) / sc;
+  out = q + relaxation * (target - q);
+  return true;
+}
+
+template <class Load>
+__device__ __forceinline__ float residual_uniform(const PlumeGridInfo& info, float ghost, int i, int j, int k, float q,
+                                                  float rhs, Load load) {
+  float sq, sc;
+  neighbor_sum_uniform(info, ghost, i, j, k, load, sq, sc);
+  return rhs - (sq - sc * q) / (info.cell_m * info.cell_m);
+}
+
+// Either path, chosen per level.
+template <class Load>
+__device__ __forceinline__ bool relax_cell(bool uniform, const PlumeGridInfo& info, float ghost, int i, int j, int k,
+                                           float q, float rhs, float relaxation, Load load, float& out) {
+  return uniform ? relaxed_uniform(info, ghost, i, j, k, q, rhs, relaxation, load, out)
+                 : relaxed(info, i, j, k, q, rhs, relaxation, load, out);
+}
+
+template <class Load>
+__device__ __forceinline__ float residual_cell(bool uniform, const PlumeGridInfo& info, float ghost, int i, int j,
+                                               int k, float q, float rhs, Load load) {
+  return uniform ? residual_uniform(info, ghost, i, j, k, q, rhs, load) : residual_at(info, i, j, k, q, rhs, load);
+}
+
+// Trilinear sample with plain loads (shared memory, or global data written earlier in the same kernel).
+__device__ __forceinline__ float sample_plain(const float* f, const Dims& d, F3 g) {
+  float x = clampf_(g[0], 0.0f, (float)(d.n0 - 1));
+  float y = clampf_(g[1], 0.0f, (float)(d.n1 - 1));
+  float z = clampf_(g[2], 0.0f, (float)(d.n2 - 1));
+  int i0 = (int)x, j0 = (int)y, k0 = (int)z;
+  int i1 = imin_(i0 + 1, d.n0 - 1), j1 = imin_(j0 + 1, d.n1 - 1), k1 = imin_(k0 + 1, d.n2 - 1);
+  float tx = x - (float)i0, ty = y - (float)j0, tz = z - (float)k0;
+  float c00 = lerpf_(f[at(d, i0, j0, k0)], f[at(d, i1, j0, k0)], tx);
+  float c10 = lerpf_(f[at(d, i0, j1, k0)], f[at(d, i1, j1, k0)], tx);
+  float c01 = lerpf_(f[at(d, i0, j0, k1)], f[at(d, i1, j0, k1)], tx);
+  float c11 = lerpf_(f[at(d, i0, j1, k1)], f[at(d, i1, j1, k1)], tx);
+  return lerpf_(lerpf_(c00, c10, ty), lerpf_(c01, c11, ty), tz);
+}
+
+// Where a fine cell centre sits in its coarse level's index space (multigrid.py:66-67).
+__device__ __forceinline__ F3 prolong_point(int i, int j, int k) {
+  return sub3(mul3(f3((float)i, (float)j, (float)k), 0.5f), f3(0.25f, 0.25f, 0.25f));
+}
+
+// Host side of the pressure solve (multigrid.cu).
+int red_black_sweeps(const PlumeGridInfo& info, float* q, float* scratch, const float* rhs, int sweeps,
+                     float relaxation, cudaStream_t st);
+int multigrid_cycles(const PlumeLevel* levels, int count, int cycles, int sweeps, cudaStream_t st);
+
+}  // namespace plume

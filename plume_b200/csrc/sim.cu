@@ -3,6 +3,8 @@
 // Each kernel cites the Warp kernel(s) of chadmv/plume whose result it produces (paths relative to that
 // project). Kernels are gathers with one thread per output element, so results never depend on scheduling;
 // the only reduction (the smoke budget) adds in a fixed order.
+#include <algorithm>
+#include <cmath>
 #include <cstdarg>
 #include <cstdio>
 #include <cstring>
@@ -10,7 +12,7 @@
 #include <string>
 #include <vector>
 
-#include "common.cuh"
+#include "poisson.cuh"
 
 namespace plume {
 
@@ -99,25 +101,27 @@ __device__ __forceinline__ F3 world_position(const PlumeGridInfo& info, F3 index
 }
 
 // emit_scalars_kernel (emitters.py:90-102) over the cells, then emit_velocity_kernel (:105-121) over the
-// three face arrays, selected by blockIdx.z segments: [0, nx) cells, then nx+1, nx, nx face slices.
+// three face arrays, within a box of cells (`lo`, `n`) that contains every cell and face an active emitter can
+// cover (coverage is 0 outside each emitter's reach). blockIdx.z segments: n[0] cell slices, then n[0]+1 u
+// slices, n[0] v slices, n[0] w slices.
 __global__ void k_emit(PlumeGridInfo info, float* __restrict__ smoke, float* __restrict__ temperature,
                        float* __restrict__ u, float* __restrict__ v, float* __restrict__ w, EmitterSet set, int seed,
-                       float time_s, float dt) {
+                       float time_s, float dt, int3 lo, int3 n) {
   const int nx = info.dims[0], ny = info.dims[1], nz = info.dims[2];
   int slab = blockIdx.z;
   int part = 0;
-  if (slab >= nx) { slab -= nx; part = 1; }
-  if (part == 1 && slab >= nx + 1) { slab -= nx + 1; part = 2; }
-  if (part == 2 && slab >= nx) { slab -= nx; part = 3; }
-  const int i = slab;
-  const int j = blockIdx.y * blockDim.y + threadIdx.y;
-  const int k = blockIdx.x * blockDim.x + threadIdx.x;
+  if (slab >= n.x) { slab -= n.x; part = 1; }
+  if (part == 1 && slab >= n.x + 1) { slab -= n.x + 1; part = 2; }
+  if (part == 2 && slab >= n.x) { slab -= n.x; part = 3; }
+  const int i = lo.x + slab;
+  const int j = lo.y + blockIdx.y * blockDim.y + threadIdx.y;
+  const int k = lo.z + blockIdx.x * blockDim.x + threadIdx.x;
   if (part == 0) {
-    if (j >= ny || k >= nz) return;
+    if (i >= nx || j >= ny || k >= nz || j >= lo.y + n.y || k >= lo.z + n.z) return;
     F3 x = world_position(info, add3(f3((float)i, (float)j, (float)k), f3(0.5f, 0.5f, 0.5f)));
     const int c = (i * ny + j) * nz + k;
-    for (int n = 0; n < set.count; ++n) {
-      const PlumeEmitter& e = set.e[n];
+    for (int e_index = 0; e_index < set.count; ++e_index) {
+      const PlumeEmitter& e = set.e[e_index];
       if (!(time_s >= e.start_s && time_s < e.end_s)) continue;
       float amount = coverage(e, x, seed);
       if (amount > 0.0f) {
@@ -129,13 +133,13 @@ __global__ void k_emit(PlumeGridInfo info, float* __restrict__ smoke, float* __r
   }
   const int axis = part - 1;
   float* comp = axis == 0 ? u : (axis == 1 ? v : w);
-  const int n1 = ny + (axis == 1), n2 = nz + (axis == 2);
-  if (j >= n1 || k >= n2) return;
+  const int n0 = nx + (axis == 0), n1 = ny + (axis == 1), n2 = nz + (axis == 2);
+  if (i >= n0 || j >= n1 || k >= n2 || j > lo.y + n.y || k > lo.z + n.z) return;
   F3 offset = axis == 0 ? f3(0.0f, 0.5f, 0.5f) : (axis == 1 ? f3(0.5f, 0.0f, 0.5f) : f3(0.5f, 0.5f, 0.0f));
   F3 x = world_position(info, add3(f3((float)i, (float)j, (float)k), offset));
   const int c = (i * n1 + j) * n2 + k;
-  for (int n = 0; n < set.count; ++n) {
-    const PlumeEmitter& e = set.e[n];
+  for (int e_index = 0; e_index < set.count; ++e_index) {
+    const PlumeEmitter& e = set.e[e_index];
     if (!(time_s >= e.start_s && time_s < e.end_s)) continue;
     float amount = coverage(e, x, seed);
     if (amount > 0.0f) {
@@ -149,19 +153,45 @@ __global__ void k_emit(PlumeGridInfo info, float* __restrict__ smoke, float* __r
   }
 }
 
+// The cells (inclusive index range per axis) that can lie within reach of the emitters, with a 2-cell margin
+// for rounding; false when none is inside the grid.
+static bool emitter_box(const PlumeGridInfo& info, const PlumeEmitter* e, int count, int lo[3], int hi[3]) {
+  for (int a = 0; a < 3; ++a) {
+    lo[a] = info.dims[a];
+    hi[a] = -1;
+  }
+  for (int n = 0; n < count; ++n)
+    for (int a = 0; a < 3; ++a) {
+      const double reach = e[n].shape == 0 ? (double)e[n].radius_m : (double)e[n].half_size_m[a];
+      const double first = ((double)e[n].center_m[a] - reach - (double)info.origin_m[a]) / (double)info.cell_m;
+      const double last = ((double)e[n].center_m[a] + reach - (double)info.origin_m[a]) / (double)info.cell_m;
+      lo[a] = std::min(lo[a], (int)std::max(-1.0, std::floor(first) - 2.0));
+      hi[a] = std::max(hi[a], (int)std::min((double)info.dims[a] + 1.0, std::ceil(last) + 2.0));
+    }
+  for (int a = 0; a < 3; ++a) {
+    lo[a] = std::max(lo[a], 0);
+    hi[a] = std::min(hi[a], info.dims[a] - 1);
+    if (hi[a] < lo[a]) return false;
+  }
+  return true;
+}
+
 static int launch_emit(const PlumeGridInfo& info, float* smoke, float* temperature, float* u, float* v, float* w,
                        const PlumeEmitter* emitters, int count, int seed, float time_s, float dt, cudaStream_t st) {
   // Emitters inactive at time_s change nothing; skip them on the host (the kernel re-checks).
   std::vector<PlumeEmitter> active;
   for (int n = 0; n < count; ++n)
     if (time_s >= emitters[n].start_s && time_s < emitters[n].end_s) active.push_back(emitters[n]);
-  const int nx = info.dims[0], ny = info.dims[1], nz = info.dims[2];
   for (size_t first = 0; first < active.size(); first += PLUME_MAX_EMITTERS) {
     EmitterSet set;
     set.count = (int)std::min<size_t>(PLUME_MAX_EMITTERS, active.size() - first);
     for (int n = 0; n < set.count; ++n) set.e[n] = active[first + n];
-    dim3 grid((nz + 1 + TZ - 1) / TZ, (ny + 1 + TY - 1) / TY, nx + (nx + 1) + nx + nx);
-    k_emit<<<grid, cell_block(), 0, st>>>(info, smoke, temperature, u, v, w, set, seed, time_s, dt);
+    int lo[3], hi[3];
+    if (!emitter_box(info, set.e, set.count, lo, hi)) continue;
+    const int3 box_lo = make_int3(lo[0], lo[1], lo[2]);
+    const int3 box_n = make_int3(hi[0] - lo[0] + 1, hi[1] - lo[1] + 1, hi[2] - lo[2] + 1);
+    dim3 grid((box_n.z + 1 + TZ - 1) / TZ, (box_n.y + 1 + TY - 1) / TY, box_n.x + (box_n.x + 1) + box_n.x + box_n.x);
+    k_emit<<<grid, cell_block(), 0, st>>>(info, smoke, temperature, u, v, w, set, seed, time_s, dt, box_lo, box_n);
     CHECK_LAUNCH("emit");
   }
   return PLUME_OK;
@@ -284,6 +314,40 @@ struct FaceForces {
 
 // One pass over the three face arrays applying, per face and in the reference's order, the confinement push,
 // the turbulence push and drag. blockIdx.z segments: nx+1 u slices, nx v slices, nx w slices.
+template <int AXIS>
+__device__ __forceinline__ void face_forces_at(const PlumeGridInfo& info, float* __restrict__ f, int i, int j, int k,
+                                               int n1, int n2, const FaceForces& ff) {
+  const int nx = info.dims[0], ny = info.dims[1], nz = info.dims[2];
+  const int c = (i * n1 + j) * n2 + k;
+  float value = f[c];
+  if (ff.confinement) {
+    const int index = AXIS == 0 ? i : (AXIS == 1 ? j : k);
+    const int lo = imax_(index - 1, 0), hi = imin_(index, info.dims[AXIS] - 1);
+    const Dims d{nx, ny, nz};
+    const int at_lo = AXIS == 0 ? at(d, lo, j, k) : (AXIS == 1 ? at(d, i, lo, k) : at(d, i, j, lo));
+    const int at_hi = AXIS == 0 ? at(d, hi, j, k) : (AXIS == 1 ? at(d, i, hi, k) : at(d, i, j, hi));
+    const float* p = ff.push[AXIS];
+    float average = 0.5f * (__ldg(p + at_lo) + __ldg(p + at_hi));
+    value = value + average * ff.dt;
+  }
+  if (ff.turbulence) {
+    const F3 offset = AXIS == 0 ? f3(0.0f, 0.5f, 0.5f) : (AXIS == 1 ? f3(0.5f, 0.0f, 0.5f) : f3(0.5f, 0.5f, 0.0f));
+    const F3 face = add3(f3((float)i, (float)j, (float)k), offset);
+    constexpr int B = (AXIS + 1) % 3, C = (AXIS + 2) % 3;
+    const F3 half_b = f3(B == 0 ? 0.5f : 0.0f, B == 1 ? 0.5f : 0.0f, B == 2 ? 0.5f : 0.0f);
+    const F3 half_c = f3(C == 0 ? 0.5f : 0.0f, C == 1 ? 0.5f : 0.0f, C == 2 ? 0.5f : 0.0f);
+    float to_lattice = info.cell_m / ff.scale_m;
+    float c_plus = potential(ff.seed, C, mul3(add3(face, half_b), to_lattice), ff.pattern_time);
+    float c_minus = potential(ff.seed, C, mul3(sub3(face, half_b), to_lattice), ff.pattern_time);
+    float b_plus = potential(ff.seed, B, mul3(add3(face, half_c), to_lattice), ff.pattern_time);
+    float b_minus = potential(ff.seed, B, mul3(sub3(face, half_c), to_lattice), ff.pattern_time);
+    float curl = ((c_plus - c_minus) - (b_plus - b_minus)) / to_lattice;
+    value = value + ff.strength * curl * ff.dt;
+  }
+  if (ff.drag) value = ff.wind[AXIS] + (value - ff.wind[AXIS]) * ff.keep;
+  f[c] = value;
+}
+
 __global__ void k_face_forces(PlumeGridInfo info, float* __restrict__ u, float* __restrict__ v,
                               float* __restrict__ w, FaceForces ff) {
   const int nx = info.dims[0], ny = info.dims[1], nz = info.dims[2];
@@ -293,35 +357,9 @@ __global__ void k_face_forces(PlumeGridInfo info, float* __restrict__ u, float* 
   const int i = slab, j = blockIdx.y * blockDim.y + threadIdx.y, k = blockIdx.x * blockDim.x + threadIdx.x;
   const int n1 = ny + (axis == 1), n2 = nz + (axis == 2);
   if (j >= n1 || k >= n2) return;
-  float* f = axis == 0 ? u : (axis == 1 ? v : w);
-  const int c = (i * n1 + j) * n2 + k;
-  float value = f[c];
-  if (ff.confinement) {
-    int below[3] = {i, j, k}, above[3] = {i, j, k};
-    below[axis] = imax_(below[axis] - 1, 0);
-    above[axis] = imin_(above[axis], info.dims[axis] - 1);
-    const Dims d{nx, ny, nz};
-    const float* p = ff.push[axis];
-    float average = 0.5f * (__ldg(p + at(d, below[0], below[1], below[2])) + __ldg(p + at(d, above[0], above[1], above[2])));
-    value = value + average * ff.dt;
-  }
-  if (ff.turbulence) {
-    F3 offset = axis == 0 ? f3(0.0f, 0.5f, 0.5f) : (axis == 1 ? f3(0.5f, 0.0f, 0.5f) : f3(0.5f, 0.5f, 0.0f));
-    F3 face = add3(f3((float)i, (float)j, (float)k), offset);
-    const int b = (axis + 1) % 3, cc = (axis + 2) % 3;
-    F3 half_b = f3(0.0f, 0.0f, 0.0f), half_c = f3(0.0f, 0.0f, 0.0f);
-    half_b[b] = 0.5f;
-    half_c[cc] = 0.5f;
-    float to_lattice = info.cell_m / ff.scale_m;
-    float c_plus = potential(ff.seed, cc, mul3(add3(face, half_b), to_lattice), ff.pattern_time);
-    float c_minus = potential(ff.seed, cc, mul3(sub3(face, half_b), to_lattice), ff.pattern_time);
-    float b_plus = potential(ff.seed, b, mul3(add3(face, half_c), to_lattice), ff.pattern_time);
-    float b_minus = potential(ff.seed, b, mul3(sub3(face, half_c), to_lattice), ff.pattern_time);
-    float curl = ((c_plus - c_minus) - (b_plus - b_minus)) / to_lattice;
-    value = value + ff.strength * curl * ff.dt;
-  }
-  if (ff.drag) value = ff.wind[axis] + (value - ff.wind[axis]) * ff.keep;
-  f[c] = value;
+  if (axis == 0) face_forces_at<0>(info, u, i, j, k, n1, n2, ff);
+  else if (axis == 1) face_forces_at<1>(info, v, i, j, k, n1, n2, ff);
+  else face_forces_at<2>(info, w, i, j, k, n1, n2, ff);
 }
 
 static dim3 face_grid(const PlumeGridInfo& info) {
@@ -344,18 +382,28 @@ static int launch_confinement_push(const PlumeGridInfo& info, const float* u, co
 }
 
 // ---- advection: advect.py -----------------------------------------------------------------------------------
+//
+// Every trace starts at a sample position p = index + offset, where each velocity component's trilinear
+// weights are 0 or 1/2: velocity_at_node blends only the corners with a non-zero weight (6 to 9 loads instead
+// of 24; the same values, up to the sign of a zero). The forward and backward traces of one element share
+// that first sample, and fields with the same positions (smoke and temperature) share whole traces.
 
+// Up to two fields sampled at the same positions (same shape and offset, e.g. smoke and temperature).
+// `range`, when set, holds per element the (lo, hi) clamp bounds the forward pass found (2 floats), so the
+// correction does not trace forward again.
 struct FieldDesc {
-  const float* data;
-  float* hat;
-  float* next;
+  const float* data[2];
+  float* hat[2];
+  float* next[2];
+  float2* range[2];
+  float outside[2];
+  int fields;
   Dims d;
   F3 offset;
-  float outside;
   int uses_outside;
 };
 
-// semi_lagrangian_kernel (advect.py:24-31) for up to three fields in one launch (blockIdx.z segments).
+// Up to three groups (the three velocity components) in one launch (blockIdx.z segments).
 struct FieldSet {
   FieldDesc f[3];
   int count;
@@ -370,39 +418,93 @@ __device__ __forceinline__ int pick_field(const FieldSet& set, int& slab) {
   return which;
 }
 
-__global__ void k_semi_lagrangian(PlumeGridInfo info, Vel vel, FieldSet set, float dt_over_cell, int write_next) {
-  int slab = blockIdx.z;
-  const FieldDesc& fd = set.f[pick_field(set, slab)];
-  const int i = slab, j = blockIdx.y * blockDim.y + threadIdx.y, k = blockIdx.x * blockDim.x + threadIdx.x;
-  if (j >= fd.d.n1 || k >= fd.d.n2) return;
-  F3 p = add3(f3((float)i, (float)j, (float)k), fd.offset);
-  F3 src = trace(vel, p, dt_over_cell);
-  float value;
-  if (fd.uses_outside == 1 && is_outside_open_face(src, info)) value = fd.outside;
-  else value = sample_index_space(fd.data, fd.d, sub3(src, fd.offset));
-  (write_next ? fd.next : fd.hat)[at(fd.d, i, j, k)] = value;
+// Trilinear sample that skips the corners whose weight is exactly 0 (sample.py:10-29 otherwise unchanged).
+__device__ __forceinline__ float sample_sparse(const float* __restrict__ f, const Dims& d, F3 g) {
+  float x = clampf_(g[0], 0.0f, (float)(d.n0 - 1));
+  float y = clampf_(g[1], 0.0f, (float)(d.n1 - 1));
+  float z = clampf_(g[2], 0.0f, (float)(d.n2 - 1));
+  const int i0 = (int)x, j0 = (int)y, k0 = (int)z;
+  const int i1 = imin_(i0 + 1, d.n0 - 1), j1 = imin_(j0 + 1, d.n1 - 1), k1 = imin_(k0 + 1, d.n2 - 1);
+  const float tx = x - (float)i0, ty = y - (float)j0, tz = z - (float)k0;
+  auto along_x = [&](int j, int k) {
+    const float a = __ldg(f + at(d, i0, j, k));
+    return tx == 0.0f ? a : lerpf_(a, __ldg(f + at(d, i1, j, k)), tx);
+  };
+  const float c00 = along_x(j0, k0);
+  const float y0 = ty == 0.0f ? c00 : lerpf_(c00, along_x(j1, k0), ty);
+  if (tz == 0.0f) return y0;
+  const float c01 = along_x(j0, k1);
+  const float y1 = ty == 0.0f ? c01 : lerpf_(c01, along_x(j1, k1), ty);
+  return lerpf_(y0, y1, tz);
 }
 
-// maccormack_correct_kernel (advect.py:34-50) with the backward pass (advect.py:64) evaluated in place:
-// back = sample(hat, trace(p, -dt)) at this element, then the clamp to the range at the forward trace.
-__global__ void k_maccormack(PlumeGridInfo info, Vel vel, FieldSet set, float dt_over_cell) {
+__device__ __forceinline__ F3 velocity_at_node(const Vel& vel, F3 p) {  // velocity_at (sample.py:74-82) at p
+  return f3(sample_sparse(vel.u, vel.du, sub3(p, f3(0.0f, 0.5f, 0.5f))),
+            sample_sparse(vel.v, vel.dv, sub3(p, f3(0.5f, 0.0f, 0.5f))),
+            sample_sparse(vel.w, vel.dw, sub3(p, f3(0.5f, 0.5f, 0.0f))));
+}
+
+// trace (advect.py:16-21) given the velocity at p.
+__device__ __forceinline__ F3 trace_from(const Vel& vel, F3 p, F3 vp, float dt_over_cell) {
+  F3 mid = sub3(p, mul3(vp, 0.5f * dt_over_cell));
+  return sub3(p, mul3(velocity_at(vel, mid), dt_over_cell));
+}
+
+// semi_lagrangian_kernel (advect.py:24-31): the forward pass into `hat` (or, for plain semi-Lagrangian
+// advection, into `next`).
+__global__ void k_advect_forward(PlumeGridInfo info, Vel vel, FieldSet set, float dt_over_cell, int write_next) {
   int slab = blockIdx.z;
   const FieldDesc& fd = set.f[pick_field(set, slab)];
   const int i = slab, j = blockIdx.y * blockDim.y + threadIdx.y, k = blockIdx.x * blockDim.x + threadIdx.x;
   if (j >= fd.d.n1 || k >= fd.d.n2) return;
   const int c = at(fd.d, i, j, k);
-  F3 p = add3(f3((float)i, (float)j, (float)k), fd.offset);
-  F3 back_src = trace(vel, p, -dt_over_cell);
-  float back;
-  if (fd.uses_outside == 1 && is_outside_open_face(back_src, info)) back = fd.outside;
-  else back = sample_index_space(fd.hat, fd.d, sub3(back_src, fd.offset));
-  float corrected = __ldg(fd.hat + c) + 0.5f * (__ldg(fd.data + c) - back);
-  F3 source = trace(vel, p, dt_over_cell);
-  float lo = fd.outside, hi = fd.outside;
-  if (fd.uses_outside == 0 || !is_outside_open_face(source, info)) {
-    sample_with_range(fd.data, fd.d, sub3(source, fd.offset), lo, hi);
+  const F3 p = add3(f3((float)i, (float)j, (float)k), fd.offset);
+  const F3 src = trace_from(vel, p, velocity_at_node(vel, p), dt_over_cell);
+  const bool outside = fd.uses_outside == 1 && is_outside_open_face(src, info);
+  const F3 g = sub3(src, fd.offset);
+  for (int n = 0; n < fd.fields; ++n) {
+    float value = fd.outside[n], lo = fd.outside[n], hi = fd.outside[n];
+    if (!outside) value = sample_with_range(fd.data[n], fd.d, g, lo, hi);
+    (write_next ? fd.next[n] : fd.hat[n])[c] = value;
+    if (fd.range[n]) fd.range[n][c] = make_float2(lo, hi);
   }
-  fd.next[c] = clampf_(corrected, lo, hi);
+}
+
+// maccormack_correct_kernel (advect.py:34-50) with the backward pass (advect.py:64) evaluated in place:
+// back = sample(hat, trace(p, -dt)), corrected = hat + (data - back) / 2, clamped to the range of the eight
+// values the forward sample blended.
+template <bool STORED_RANGE>
+__global__ void k_advect_correct(PlumeGridInfo info, Vel vel, FieldSet set, float dt_over_cell) {
+  int slab = blockIdx.z;
+  const FieldDesc& fd = set.f[pick_field(set, slab)];
+  const int i = slab, j = blockIdx.y * blockDim.y + threadIdx.y, k = blockIdx.x * blockDim.x + threadIdx.x;
+  if (j >= fd.d.n1 || k >= fd.d.n2) return;
+  const int c = at(fd.d, i, j, k);
+  const F3 p = add3(f3((float)i, (float)j, (float)k), fd.offset);
+  const F3 vp = velocity_at_node(vel, p);
+  const F3 back_src = trace_from(vel, p, vp, -dt_over_cell);
+  const bool back_outside = fd.uses_outside == 1 && is_outside_open_face(back_src, info);
+  const F3 gb = sub3(back_src, fd.offset);
+  F3 gs = f3(0.0f, 0.0f, 0.0f);
+  bool source_outside = false;
+  if (!STORED_RANGE) {
+    const F3 source = trace_from(vel, p, vp, dt_over_cell);
+    source_outside = fd.uses_outside == 1 && is_outside_open_face(source, info);
+    gs = sub3(source, fd.offset);
+  }
+  for (int n = 0; n < fd.fields; ++n) {
+    const float back = back_outside ? fd.outside[n] : sample_index_space(fd.hat[n], fd.d, gb);
+    const float corrected = __ldg(fd.hat[n] + c) + 0.5f * (__ldg(fd.data[n] + c) - back);
+    float lo = fd.outside[n], hi = fd.outside[n];
+    if (STORED_RANGE) {
+      const float2 r = __ldg(fd.range[n] + c);
+      lo = r.x;
+      hi = r.y;
+    } else if (!source_outside) {
+      sample_with_range(fd.data[n], fd.d, gs, lo, hi);
+    }
+    fd.next[n][c] = clampf_(corrected, lo, hi);
+  }
 }
 
 static int launch_advect(const PlumeGridInfo& info, const Vel& vel, const FieldSet& set, float dt_over_cell,
@@ -415,15 +517,30 @@ static int launch_advect(const PlumeGridInfo& info, const Vel& vel, const FieldS
   }
   dim3 grid((n2 + TZ - 1) / TZ, (n1 + TY - 1) / TY, slabs);
   if (!maccormack) {
-    k_semi_lagrangian<<<grid, cell_block(), 0, st>>>(info, vel, set, dt_over_cell, 1);
+    k_advect_forward<<<grid, cell_block(), 0, st>>>(info, vel, set, dt_over_cell, 1);
     CHECK_LAUNCH("semi-Lagrangian advection");
     return PLUME_OK;
   }
-  k_semi_lagrangian<<<grid, cell_block(), 0, st>>>(info, vel, set, dt_over_cell, 0);
+  k_advect_forward<<<grid, cell_block(), 0, st>>>(info, vel, set, dt_over_cell, 0);
   CHECK_LAUNCH("MacCormack forward pass");
-  k_maccormack<<<grid, cell_block(), 0, st>>>(info, vel, set, dt_over_cell);
+  if (set.f[0].range[0]) k_advect_correct<true><<<grid, cell_block(), 0, st>>>(info, vel, set, dt_over_cell);
+  else k_advect_correct<false><<<grid, cell_block(), 0, st>>>(info, vel, set, dt_over_cell);
   CHECK_LAUNCH("MacCormack correction");
   return PLUME_OK;
+}
+
+static FieldDesc single_field(const float* data, float* hat, float* next, Dims d, F3 offset, float outside,
+                              int uses_outside) {
+  FieldDesc f{};
+  f.data[0] = data;
+  f.hat[0] = hat;
+  f.next[0] = next;
+  f.outside[0] = outside;
+  f.fields = 1;
+  f.d = d;
+  f.offset = offset;
+  f.uses_outside = uses_outside;
+  return f;
 }
 
 // ---- pressure: pressure.py ----------------------------------------------------------------------------------
@@ -457,6 +574,27 @@ __global__ void k_divergence(PlumeGridInfo info, const float* __restrict__ u, co
 }
 
 // subtract_gradient_kernel (pressure.py:95-116) over the three face arrays (blockIdx.z segments).
+template <int AXIS>
+__device__ __forceinline__ void subtract_gradient_at(const PlumeGridInfo& info, float* __restrict__ f,
+                                                     const float* __restrict__ q, int i, int j, int k, int n1, int n2) {
+  const Dims d = dims_of(info);
+  const int index = AXIS == 0 ? i : (AXIS == 1 ? j : k);
+  const int below = AXIS == 0 ? at(d, i - 1, j, k) : (AXIS == 1 ? at(d, i, j - 1, k) : at(d, i, j, k - 1));
+  float q_above = 0.0f, q_below = 0.0f;
+  if (index == 0) {
+    if (info.open_lo[AXIS] == 0) return;
+    q_above = __ldg(q + at(d, i, j, k));
+  } else if (index == info.dims[AXIS]) {
+    if (info.open_hi[AXIS] == 0) return;
+    q_below = __ldg(q + below);
+  } else {
+    q_above = __ldg(q + at(d, i, j, k));
+    q_below = __ldg(q + below);
+  }
+  const int c = (i * n1 + j) * n2 + k;
+  f[c] = f[c] - (q_above - q_below) / info.cell_m;
+}
+
 __global__ void k_subtract_gradient(PlumeGridInfo info, float* __restrict__ u, float* __restrict__ v,
                                     float* __restrict__ w, const float* __restrict__ q) {
   const int nx = info.dims[0], ny = info.dims[1], nz = info.dims[2];
@@ -466,172 +604,23 @@ __global__ void k_subtract_gradient(PlumeGridInfo info, float* __restrict__ u, f
   const int i = slab, j = blockIdx.y * blockDim.y + threadIdx.y, k = blockIdx.x * blockDim.x + threadIdx.x;
   const int n1 = ny + (axis == 1), n2 = nz + (axis == 2);
   if (j >= n1 || k >= n2) return;
-  float* f = axis == 0 ? u : (axis == 1 ? v : w);
-  const int face[3] = {i, j, k};
-  const int index = face[axis];
-  int below[3] = {i, j, k};
-  below[axis] = index - 1;
-  const Dims d{nx, ny, nz};
-  float q_above = 0.0f, q_below = 0.0f;
-  if (index == 0) {
-    if (info.open_lo[axis] == 0) return;
-    q_above = __ldg(q + at(d, i, j, k));
-  } else if (index == info.dims[axis]) {
-    if (info.open_hi[axis] == 0) return;
-    q_below = __ldg(q + at(d, below[0], below[1], below[2]));
-  } else {
-    q_above = __ldg(q + at(d, i, j, k));
-    q_below = __ldg(q + at(d, below[0], below[1], below[2]));
-  }
-  const int c = (i * n1 + j) * n2 + k;
-  f[c] = f[c] - (q_above - q_below) / info.cell_m;
+  if (axis == 0) subtract_gradient_at<0>(info, u, q, i, j, k, n1, n2);
+  else if (axis == 1) subtract_gradient_at<1>(info, v, q, i, j, k, n1, n2);
+  else subtract_gradient_at<2>(info, w, q, i, j, k, n1, n2);
 }
 
-// ---- the variable-coefficient Poisson stencil (pressure.py:39-77) -------------------------------------------
-
-__device__ __forceinline__ float cell_fill(const PlumeGridInfo& info, int axis, int index) {
-  return index == info.dims[axis] - 1 ? info.fill_hi[axis] : 1.0f;
-}
-
-// q is read with ordinary loads: the red-black kernel writes other cells of the same array.
-__device__ __forceinline__ void neighbor_sum(const float* q, const PlumeGridInfo& info, const int c[3],
-                                             float& sq, float& sc) {
-  sq = 0.0f;
-  sc = 0.0f;
-  const Dims d{info.dims[0], info.dims[1], info.dims[2]};
-#pragma unroll
-  for (int axis = 0; axis < 3; ++axis) {
-    float area = 1.0f;
-#pragma unroll
-    for (int other = 0; other < 3; ++other)
-      if (other != axis) area = area * cell_fill(info, other, c[other]);
-    const float own = cell_fill(info, axis, c[axis]);
-    float tq[2], tc[2];
-#pragma unroll
-    for (int side = 0; side < 2; ++side) {
-      const int step = side == 0 ? -1 : 1;
-      int n[3] = {c[0], c[1], c[2]};
-      n[axis] = n[axis] + step;
-      if (n[axis] >= 0 && n[axis] < info.dims[axis]) {
-        float coupling = area / (0.5f * (own + cell_fill(info, axis, n[axis])));
-        tq[side] = coupling * q[at(d, n[0], n[1], n[2])];
-        tc[side] = coupling;
-      } else if ((step < 0 && info.open_lo[axis] == 1) || (step > 0 && info.open_hi[axis] == 1)) {
-        tq[side] = 0.0f;
-        tc[side] = area / (0.5f * own + info.ghost_gap);
-      } else {
-        tq[side] = 0.0f;
-        tc[side] = 0.0f;
-      }
-    }
-    sq = (sq + tq[0]) + tq[1];
-    sc = (sc + tc[0]) + tc[1];
-  }
-}
-
-__device__ __forceinline__ float cell_volume(const PlumeGridInfo& info, const int c[3]) {
-  return cell_fill(info, 0, c[0]) * cell_fill(info, 1, c[1]) * cell_fill(info, 2, c[2]);
-}
-
-// red_black_sweep_kernel (pressure.py:80-92): one colour; each thread owns one cell of that colour.
-__global__ void k_red_black(PlumeGridInfo info, float* q, const float* __restrict__ rhs, int color, float relaxation) {
-  const int ny = info.dims[1], nz = info.dims[2];
-  const int i = blockIdx.z, j = blockIdx.y * blockDim.y + threadIdx.y;
-  const int kk = blockIdx.x * blockDim.x + threadIdx.x;
-  const int k = 2 * kk + ((i + j + color) & 1);
-  if (j >= ny || k >= nz) return;
-  const int c[3] = {i, j, k};
-  float sq, sc;
-  neighbor_sum(q, info, c, sq, sc);
-  if (sc == 0.0f) return;
-  const int idx = (i * ny + j) * nz + k;
-  float source = cell_volume(info, c) * info.cell_m * info.cell_m * __ldg(rhs + idx);
-  float target = (sq - source) / sc;
-  q[idx] = q[idx] + relaxation * (target - q[idx]);
-}
-
+// ---- residual (multigrid.py:36-43), for callers that inspect it ---------------------------------------------
 __global__ void k_residual(PlumeGridInfo info, const float* __restrict__ q, const float* __restrict__ rhs,
-                           float* __restrict__ res) {  // multigrid.py:36-43
+                           float* __restrict__ res) {
   const int ny = info.dims[1], nz = info.dims[2];
   const int i = blockIdx.z, j = blockIdx.y * blockDim.y + threadIdx.y, k = blockIdx.x * blockDim.x + threadIdx.x;
   if (j >= ny || k >= nz) return;
-  const int c[3] = {i, j, k};
-  float sq, sc;
-  neighbor_sum(q, info, c, sq, sc);
-  float scale = cell_volume(info, c) * info.cell_m * info.cell_m;
+  const Dims d{info.dims[0], ny, nz};
+  auto load = [&](int a, int b, int c) { return __ldg(q + at(d, a, b, c)); };
   const int idx = (i * ny + j) * nz + k;
-  res[idx] = __ldg(rhs + idx) - (sq - sc * __ldg(q + idx)) / scale;
+  res[idx] = residual_at(info, i, j, k, __ldg(q + idx), __ldg(rhs + idx), load);
 }
 
-__global__ void k_restrict(Dims fine, Dims coarse, const float* __restrict__ f, float* __restrict__ out) {
-  const int i = blockIdx.z, j = blockIdx.y * blockDim.y + threadIdx.y, k = blockIdx.x * blockDim.x + threadIdx.x;
-  if (j >= coarse.n1 || k >= coarse.n2) return;  // multigrid.py:46-60
-  float total = 0.0f, count = 0.0f;
-#pragma unroll
-  for (int di = 0; di < 2; ++di)
-#pragma unroll
-    for (int dj = 0; dj < 2; ++dj)
-#pragma unroll
-      for (int dk = 0; dk < 2; ++dk) {
-        const int fi = 2 * i + di, fj = 2 * j + dj, fk = 2 * k + dk;
-        if (fi < fine.n0 && fj < fine.n1 && fk < fine.n2) {
-          total = total + __ldg(f + at(fine, fi, fj, fk));
-          count = count + 1.0f;
-        }
-      }
-  out[at(coarse, i, j, k)] = total / count;
-}
-
-__global__ void k_prolong_add(Dims coarse, Dims fine, const float* __restrict__ cq, float* __restrict__ q) {
-  const int i = blockIdx.z, j = blockIdx.y * blockDim.y + threadIdx.y, k = blockIdx.x * blockDim.x + threadIdx.x;
-  if (j >= fine.n1 || k >= fine.n2) return;  // multigrid.py:63-68
-  F3 g = sub3(mul3(f3((float)i, (float)j, (float)k), 0.5f), f3(0.25f, 0.25f, 0.25f));
-  const int idx = at(fine, i, j, k);
-  q[idx] = q[idx] + sample_index_space(cq, coarse, g);
-}
-
-static int red_black_sweeps(const PlumeGridInfo& info, float* q, const float* rhs, int sweeps, float relaxation,
-                            cudaStream_t st) {
-  const int nx = info.dims[0], ny = info.dims[1], nz = info.dims[2];
-  dim3 grid(((nz + 1) / 2 + TZ - 1) / TZ, (ny + TY - 1) / TY, nx);
-  for (int s = 0; s < sweeps; ++s)
-    for (int color = 0; color < 2; ++color) {
-      k_red_black<<<grid, cell_block(), 0, st>>>(info, q, rhs, color, relaxation);
-      CHECK_LAUNCH("red-black sweep");
-    }
-  return PLUME_OK;
-}
-
-constexpr int COARSEST_SWEEPS = 20;  // multigrid.py:24-33
-constexpr int COARSEST_SWEEPS_PER_CELL = 4;
-
-static Dims dims_of(const PlumeGridInfo& info) { return Dims{info.dims[0], info.dims[1], info.dims[2]}; }
-
-static int v_cycle(const PlumeLevel* levels, int count, int index, int sweeps, cudaStream_t st) {  // multigrid.py:130-147
-  const PlumeLevel& lv = levels[index];
-  int status;
-  if (index == count - 1) {
-    int longest = std::max(lv.info.dims[0], std::max(lv.info.dims[1], lv.info.dims[2]));
-    return red_black_sweeps(lv.info, lv.q, lv.rhs, std::max(COARSEST_SWEEPS, COARSEST_SWEEPS_PER_CELL * longest),
-                            1.5f, st);
-  }
-  if ((status = red_black_sweeps(lv.info, lv.q, lv.rhs, sweeps, 1.0f, st)) != PLUME_OK) return status;
-  const Dims fd = dims_of(lv.info);
-  k_residual<<<cell_grid(fd.n0, fd.n1, fd.n2), cell_block(), 0, st>>>(lv.info, lv.q, lv.rhs, lv.residual);
-  CHECK_LAUNCH("residual");
-  const PlumeLevel& coarse = levels[index + 1];
-  const Dims cd = dims_of(coarse.info);
-  k_restrict<<<cell_grid(cd.n0, cd.n1, cd.n2), cell_block(), 0, st>>>(fd, cd, lv.residual, coarse.rhs);
-  CHECK_LAUNCH("restrict");
-  if ((status = runtime_status("zero coarse pressure",
-                               cudaMemsetAsync(coarse.q, 0, sizeof(float) * (size_t)cd.n0 * cd.n1 * cd.n2, st))) !=
-      PLUME_OK)
-    return status;
-  if ((status = v_cycle(levels, count, index + 1, sweeps, st)) != PLUME_OK) return status;
-  k_prolong_add<<<cell_grid(fd.n0, fd.n1, fd.n2), cell_block(), 0, st>>>(cd, fd, coarse.q, lv.q);
-  CHECK_LAUNCH("prolong");
-  return red_black_sweeps(lv.info, lv.q, lv.rhs, sweeps, 1.0f, st);
-}
 
 // ---- smoke budget: conserve.py:33-52 + reduce.py:12-38 ------------------------------------------------------
 // Line totals along x in float (reduce.py:12-25); lines added in double in blocks of 256 by a halving tree,
@@ -757,8 +746,8 @@ extern "C" int plume_advect_semi_lagrangian(const PlumeGridInfo* info, const int
   CHECK_ARG(valid_dims(info->dims) && valid_dims(shape), "semi_lagrangian: bad dims");
   FieldSet set{};
   set.count = 1;
-  set.f[0] = FieldDesc{src, nullptr, dst, Dims{shape[0], shape[1], shape[2]}, f3(offset[0], offset[1], offset[2]),
-                       outside, uses_outside};
+  set.f[0] = single_field(src, nullptr, dst, Dims{shape[0], shape[1], shape[2]}, f3(offset[0], offset[1], offset[2]),
+                          outside, uses_outside);
   return launch_advect(*info, make_vel(u, v, w, info->dims), set, dt_over_cell, false, as_stream(stream));
 }
 
@@ -770,8 +759,8 @@ extern "C" int plume_advect_maccormack(const PlumeGridInfo* info, const int32_t 
   CHECK_ARG(valid_dims(info->dims) && valid_dims(shape), "maccormack: bad dims");
   FieldSet set{};
   set.count = 1;
-  set.f[0] = FieldDesc{data, hat, next, Dims{shape[0], shape[1], shape[2]}, f3(offset[0], offset[1], offset[2]),
-                       outside, uses_outside};
+  set.f[0] = single_field(data, hat, next, Dims{shape[0], shape[1], shape[2]}, f3(offset[0], offset[1], offset[2]),
+                          outside, uses_outside);
   return launch_advect(*info, make_vel(u, v, w, info->dims), set, dt_over_cell, true, as_stream(stream));
 }
 
@@ -870,24 +859,21 @@ extern "C" int plume_subtract_gradient(const PlumeGridInfo* info, float* u, floa
   return launch_status("subtract gradient");
 }
 
-extern "C" int plume_red_black_sweeps(const PlumeGridInfo* info, float* q, const float* rhs, int32_t sweeps,
-                                      float relaxation, void* stream) {
-  CHECK_ARG(info && q && rhs && sweeps >= 0, "red_black_sweeps: bad argument");
+extern "C" int plume_red_black_sweeps(const PlumeGridInfo* info, float* q, float* scratch, const float* rhs,
+                                      int32_t sweeps, float relaxation, void* stream) {
+  CHECK_ARG(info && q && scratch && rhs && sweeps >= 0 && scratch != q, "red_black_sweeps: bad argument");
   CHECK_ARG(valid_dims(info->dims), "red_black_sweeps: bad dims");
-  return red_black_sweeps(*info, q, rhs, sweeps, relaxation, as_stream(stream));
+  return red_black_sweeps(*info, q, scratch, rhs, sweeps, relaxation, as_stream(stream));
 }
 
 extern "C" int plume_multigrid(const PlumeLevel* levels, int32_t level_count, int32_t cycles, int32_t sweeps,
                                void* stream) {
   CHECK_ARG(levels && level_count >= 1 && cycles >= 0 && sweeps >= 0, "multigrid: bad argument");
   for (int l = 0; l < level_count; ++l)
-    CHECK_ARG(levels[l].q && levels[l].rhs && (l == level_count - 1 || levels[l].residual) && valid_dims(levels[l].info.dims),
+    CHECK_ARG(levels[l].q && levels[l].rhs && levels[l].residual && levels[l].residual != levels[l].q &&
+                  valid_dims(levels[l].info.dims),
               "multigrid: bad level %d", l);
-  for (int c = 0; c < cycles; ++c) {
-    int status = v_cycle(levels, level_count, 0, sweeps, as_stream(stream));
-    if (status != PLUME_OK) return status;
-  }
-  return PLUME_OK;
+  return multigrid_cycles(levels, level_count, cycles, sweeps, as_stream(stream));
 }
 
 extern "C" int plume_residual(const PlumeGridInfo* info, const float* q, const float* rhs, float* residual,
@@ -897,6 +883,12 @@ extern "C" int plume_residual(const PlumeGridInfo* info, const float* q, const f
   const int nx = info->dims[0], ny = info->dims[1], nz = info->dims[2];
   k_residual<<<cell_grid(nx, ny, nz), cell_block(), 0, as_stream(stream)>>>(*info, q, rhs, residual);
   return launch_status("residual");
+}
+
+extern "C" long long plume_advect_scratch_floats(const PlumeGridInfo* info) {
+  if (!info || !valid_dims(info->dims)) return fail(PLUME_ERR_INVALID, "advect_scratch_floats: bad dims");
+  const long long nx = info->dims[0], ny = info->dims[1], nz = info->dims[2];
+  return 2 * ((nx + 1) * ny * nz + nx * (ny + 1) * nz + nx * ny * (nz + 1));
 }
 
 extern "C" int plume_smoke_scratch_doubles(const PlumeGridInfo* info) {
@@ -954,9 +946,9 @@ extern "C" int plume_step(const PlumeStepState* s, const PlumeStepParams* p, voi
                 s->w.next && s->smoke.data && s->smoke.hat && s->smoke.next && s->temperature.data &&
                 s->temperature.hat && s->temperature.next && s->pressure && s->divergence && s->sums && s->factor,
             "step: null buffer");
-  CHECK_ARG(p->solver != 0 || (s->levels && s->level_count >= 1 && s->levels[0].q == s->pressure &&
-                               s->levels[0].rhs == s->divergence),
-            "step: multigrid levels must start at the grid's pressure and divergence");
+  CHECK_ARG(s->levels && s->level_count >= 1 && s->levels[0].q == s->pressure && s->levels[0].rhs == s->divergence &&
+                s->levels[0].residual && s->levels[0].residual != s->pressure,
+            "step: levels must start at the grid's pressure and divergence, with a second pressure array");
   CHECK_ARG(p->confinement == 0.0f || (s->curl[0] && s->curl[1] && s->curl[2] && s->push[0] && s->push[1] && s->push[2]),
             "step: confinement scratch missing");
   cudaStream_t st = as_stream(stream);
@@ -1014,9 +1006,15 @@ extern "C" int plume_step(const PlumeStepState* s, const PlumeStepParams* p, voi
   {
     FieldSet set{};
     set.count = 3;
-    set.f[0] = FieldDesc{s->u.data, s->u.hat, s->u.next, Dims{nx + 1, ny, nz}, f3(0.0f, 0.5f, 0.5f), 0.0f, 0};
-    set.f[1] = FieldDesc{s->v.data, s->v.hat, s->v.next, Dims{nx, ny + 1, nz}, f3(0.5f, 0.0f, 0.5f), 0.0f, 0};
-    set.f[2] = FieldDesc{s->w.data, s->w.hat, s->w.next, Dims{nx, ny, nz + 1}, f3(0.5f, 0.5f, 0.0f), 0.0f, 0};
+    set.f[0] = single_field(s->u.data, s->u.hat, s->u.next, Dims{nx + 1, ny, nz}, f3(0.0f, 0.5f, 0.5f), 0.0f, 0);
+    set.f[1] = single_field(s->v.data, s->v.hat, s->v.next, Dims{nx, ny + 1, nz}, f3(0.5f, 0.0f, 0.5f), 0.0f, 0);
+    set.f[2] = single_field(s->w.data, s->w.hat, s->w.next, Dims{nx, ny, nz + 1}, f3(0.5f, 0.5f, 0.0f), 0.0f, 0);
+    if (s->advect_scratch) {  // clamp ranges: u's, v's, w's, back to back
+      float2* r = reinterpret_cast<float2*>(s->advect_scratch);
+      set.f[0].range[0] = r;
+      set.f[1].range[0] = r + (size_t)(nx + 1) * ny * nz;
+      set.f[2].range[0] = r + (size_t)(nx + 1) * ny * nz + (size_t)nx * (ny + 1) * nz;
+    }
     if ((status = launch_advect(info, make_vel(s->u.data, s->v.data, s->w.data, info.dims), set, p->dt_over_cell, true,
                                 st)) != PLUME_OK)
       return status;
@@ -1029,9 +1027,10 @@ extern "C" int plume_step(const PlumeStepState* s, const PlumeStepParams* p, voi
   if ((status = plume_project_begin(&info, u, v, w, s->divergence, stream)) != PLUME_OK) return status;
   if ((status = mark()) != PLUME_OK) return status;
   if (p->solver == 0) {
-    for (int c = 0; c < p->solver_iterations; ++c)
-      if ((status = v_cycle(s->levels, s->level_count, 0, p->multigrid_sweeps, st)) != PLUME_OK) return status;
-  } else if ((status = red_black_sweeps(info, s->pressure, s->divergence, p->solver_iterations, 1.5f, st)) != PLUME_OK) {
+    if ((status = multigrid_cycles(s->levels, s->level_count, p->solver_iterations, p->multigrid_sweeps, st)) != PLUME_OK)
+      return status;
+  } else if ((status = red_black_sweeps(info, s->pressure, s->levels[0].residual, s->divergence, p->solver_iterations,
+                                        1.5f, st)) != PLUME_OK) {
     return status;
   }
   if ((status = mark()) != PLUME_OK) return status;
@@ -1042,10 +1041,18 @@ extern "C" int plume_step(const PlumeStepState* s, const PlumeStepParams* p, voi
   {
     Vel vel = make_vel(u, v, w, info.dims);
     FieldSet set{};
-    set.count = 2;
-    set.f[0] = FieldDesc{s->smoke.data, s->smoke.hat, s->smoke.next, Dims{nx, ny, nz}, f3(0.5f, 0.5f, 0.5f), 0.0f, 1};
-    set.f[1] = FieldDesc{s->temperature.data, s->temperature.hat, s->temperature.next, Dims{nx, ny, nz},
-                         f3(0.5f, 0.5f, 0.5f), p->ambient_k, 1};
+    set.count = 1;  // smoke and temperature share positions: one trace serves both
+    set.f[0] = single_field(s->smoke.data, s->smoke.hat, s->smoke.next, Dims{nx, ny, nz}, f3(0.5f, 0.5f, 0.5f), 0.0f, 1);
+    set.f[0].data[1] = s->temperature.data;
+    set.f[0].hat[1] = s->temperature.hat;
+    set.f[0].next[1] = s->temperature.next;
+    set.f[0].outside[1] = p->ambient_k;
+    set.f[0].fields = 2;
+    if (s->advect_scratch) {
+      float2* r = reinterpret_cast<float2*>(s->advect_scratch);
+      set.f[0].range[0] = r;
+      set.f[0].range[1] = r + (size_t)nx * ny * nz;
+    }
     if ((status = launch_advect(info, vel, set, p->dt_over_cell, true, st)) != PLUME_OK) return status;
   }
   if ((status = launch_triple_sum(dims_of(info), s->smoke.data, s->smoke.hat, s->smoke.next, s->sums, s->factor,

@@ -7,6 +7,8 @@ here, Multigrid in plume_b200.sim.multigrid.
 
 from typing import Protocol
 
+import torch
+
 from plume_b200 import _native as N
 
 RELAXATION = 1.5
@@ -22,15 +24,23 @@ class GaussSeidel:
 
     def __init__(self, iterations: int):
         self.iterations = iterations
+        self.scratch = None
+
+    def second_array(self, grid) -> torch.Tensor:
+        """The sweeps' second pressure array (each sweep reads one and writes the other)."""
+        if self.scratch is None or self.scratch.shape != grid.pressure.shape:
+            self.scratch = torch.empty_like(grid.pressure)
+        return self.scratch
 
     def __call__(self, grid) -> None:
         red_black_sweeps(grid.pressure, grid.divergence, grid.info, grid.cells, grid.device, self.iterations,
-                         RELAXATION)
+                         RELAXATION, self.second_array(grid))
 
 
-def red_black_sweeps(q, rhs, info, cells, device, sweeps: int, relaxation: float) -> None:
+def red_black_sweeps(q, rhs, info, cells, device, sweeps: int, relaxation: float, scratch=None) -> None:
     """`sweeps` red-black sweeps (colour 0 then 1) of laplacian(q) = rhs on the grid `info` describes."""
-    N.call("plume_red_black_sweeps", info, N.ptr(q), N.ptr(rhs), sweeps, relaxation, N.stream())
+    scratch = torch.empty_like(q) if scratch is None else scratch
+    N.call("plume_red_black_sweeps", info, N.ptr(q), N.ptr(scratch), N.ptr(rhs), sweeps, relaxation, N.stream())
 
 
 def project(grid, solve) -> None:

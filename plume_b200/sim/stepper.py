@@ -9,6 +9,8 @@ fields' data/next buffers are swapped here afterwards, as the reference's Advect
 import ctypes
 import math
 
+import torch
+
 from plume_b200 import _native as N
 from plume_b200.sim.conserve import SmokeBudget
 from plume_b200.sim.emitters import emitter_params
@@ -28,6 +30,9 @@ class Stepper:
         self.pressure_solve = make_pressure_solve(grid, recipe.solver)
         self.smoke_budget = SmokeBudget(grid)
         self.confinement = VorticityConfinement(grid) if recipe.forces.vorticity_confinement > 0 else None
+        # MacCormack's clamp ranges, kept between its forward pass and its correction
+        self.advect_scratch = torch.empty(N.lib().plume_advect_scratch_floats(grid.info), dtype=torch.float32,
+                                          device=grid.device)
 
     def _params(self, time_s: float, dt: float) -> N.PlumeStepParams:
         recipe, grid = self.recipe, self.grid
@@ -73,11 +78,18 @@ class Stepper:
             s.curl = (ctypes.c_void_p * 3)(*[N.ptr(t).value for t in self.confinement._curl])
             s.push = (ctypes.c_void_p * 3)(*[N.ptr(t).value for t in self.confinement._push])
         s.sums = self.smoke_budget.sums.data_ptr()
+        s.advect_scratch = N.ptr(self.advect_scratch).value
         s.factor = N.ptr(self.smoke_budget.factor).value
         if isinstance(self.pressure_solve, Multigrid):
             levels = self.pressure_solve.native_levels(grid)
-            s.levels = ctypes.cast(levels, ctypes.POINTER(N.PlumeLevel))
-            s.level_count = len(levels)
+        else:
+            levels = (N.PlumeLevel * 1)()
+            levels[0].info = grid.info
+            levels[0].q, levels[0].rhs = N.ptr(grid.pressure).value, N.ptr(grid.divergence).value
+            levels[0].residual = N.ptr(self.pressure_solve.second_array(grid)).value
+        self._levels = levels
+        s.levels = ctypes.cast(levels, ctypes.POINTER(N.PlumeLevel))
+        s.level_count = len(levels)
         return s
 
     def step(self, time_s: float, dt: float) -> None:
