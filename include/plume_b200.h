@@ -203,6 +203,11 @@ int plume_multigrid(const PlumeLevel* levels, int32_t level_count, int32_t cycle
  * 1024-thread block; at most 200 KiB of shared memory per CTA. Process-wide; defaults 2^40, 8192, 0. */
 int plume_tune_solver(long long tiled_min_cells, long long bottom_max_cells, int32_t bottom_kind);
 
+/* Pressure solves replay a CUDA graph of their launches, captured once per levels/cycles/strategy (default
+ * on). 0 turns that off (every kernel launched one by one); results are the same either way. When the
+ * caller's stream is itself being captured, launches are always made one by one into that capture. */
+int plume_use_graphs(int32_t enable);
+
 /* multigrid.py:36-43 residual_kernel. */
 int plume_residual(const PlumeGridInfo* info, const float* q, const float* rhs, float* residual, void* stream);
 

@@ -94,6 +94,7 @@ SIGNATURES = {
     "plume_multigrid": [ctypes.POINTER(PlumeLevel), _I, _I, _I, _P],
     "plume_residual": [_INFO, _P, _P, _P, _P],
     "plume_tune_solver": [ctypes.c_longlong, ctypes.c_longlong, _I],
+    "plume_use_graphs": [_I],
     "plume_smoke_scratch_doubles": [_INFO],
     "plume_advect_scratch_floats": [_INFO],
     "plume_smoke_budget": [_INFO, _P, _P, _P, _P, _P, _P, _P],

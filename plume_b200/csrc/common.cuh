@@ -18,6 +18,8 @@ namespace plume {
 int fail(int status, const char* fmt, ...);
 int launch_status(const char* what);                   // after a kernel launch: checks it and counts it
 int runtime_status(const char* what, cudaError_t err);  // after any other runtime call
+void count_launches(unsigned long long n);             // kernels enqueued another way (graph replays)
+void set_launch_counting(bool on);
 
 // ---- small vector type -----------------------------------------------------------------------------------
 struct F3 {
@@ -57,42 +59,57 @@ __host__ __device__ __forceinline__ Dims dims_of(const PlumeGridInfo& info) {
   return Dims{info.dims[0], info.dims[1], info.dims[2]};
 }
 
+// One axis of a trilinear sample: the clamped position's lower index, the step to the upper corner (0 at the
+// far edge) and the weights, computed once per axis. The clamp uses min/max, which differs from the reference's
+// comparisons only in the sign of a zero (the same values follow).
+struct Axis1 {
+  int i0;
+  int step;
+  float t, one_minus_t;
+};
+
+__device__ __forceinline__ Axis1 axis_of(float g, int n, int stride) {
+  const float x = fminf(fmaxf(g, 0.0f), (float)(n - 1));
+  Axis1 a;
+  a.i0 = (int)x;
+  a.step = a.i0 < n - 1 ? stride : 0;
+  a.t = x - (float)a.i0;
+  a.one_minus_t = 1.0f - a.t;
+  return a;
+}
+
+// lerp(a, b, t) = a*(1-t) + b*t with (1-t) precomputed: the same float operations.
+__device__ __forceinline__ float lerp_w(float a, float b, const Axis1& w) { return a * w.one_minus_t + b * w.t; }
+
 // Trilinear sample at continuous index g, clamped to the array (sim/sample.py:10-29).
 __device__ __forceinline__ float sample_index_space(const float* __restrict__ f, const Dims& d, F3 g) {
-  float x = clampf_(g[0], 0.0f, (float)(d.n0 - 1));
-  float y = clampf_(g[1], 0.0f, (float)(d.n1 - 1));
-  float z = clampf_(g[2], 0.0f, (float)(d.n2 - 1));
-  int i0 = (int)x, j0 = (int)y, k0 = (int)z;
-  int i1 = imin_(i0 + 1, d.n0 - 1), j1 = imin_(j0 + 1, d.n1 - 1), k1 = imin_(k0 + 1, d.n2 - 1);
-  float tx = x - (float)i0, ty = y - (float)j0, tz = z - (float)k0;
-  float c00 = lerpf_(__ldg(f + at(d, i0, j0, k0)), __ldg(f + at(d, i1, j0, k0)), tx);
-  float c10 = lerpf_(__ldg(f + at(d, i0, j1, k0)), __ldg(f + at(d, i1, j1, k0)), tx);
-  float c01 = lerpf_(__ldg(f + at(d, i0, j0, k1)), __ldg(f + at(d, i1, j0, k1)), tx);
-  float c11 = lerpf_(__ldg(f + at(d, i0, j1, k1)), __ldg(f + at(d, i1, j1, k1)), tx);
-  return lerpf_(lerpf_(c00, c10, ty), lerpf_(c01, c11, ty), tz);
+  const Axis1 x = axis_of(g[0], d.n0, d.n1 * d.n2), y = axis_of(g[1], d.n1, d.n2), z = axis_of(g[2], d.n2, 1);
+  const float* p = f + (x.i0 * d.n1 + y.i0) * d.n2 + z.i0;
+  const float c00 = lerp_w(__ldg(p), __ldg(p + x.step), x);
+  const float c10 = lerp_w(__ldg(p + y.step), __ldg(p + x.step + y.step), x);
+  const float c01 = lerp_w(__ldg(p + z.step), __ldg(p + x.step + z.step), x);
+  const float c11 = lerp_w(__ldg(p + y.step + z.step), __ldg(p + x.step + y.step + z.step), x);
+  return lerp_w(lerp_w(c00, c10, y), lerp_w(c01, c11, y), z);
 }
 
 // The value and the min/max of the eight values a trilinear sample blends (sample.py:10-50), from one set
-// of loads: MacCormack's forward pass and its clamp bounds read the same corners.
+// of loads: MacCormack's forward pass and its clamp bounds read the same corners. The min/max run in the
+// reference's corner order.
 __device__ __forceinline__ float sample_with_range(const float* __restrict__ f, const Dims& d, F3 g, float& lo,
                                                    float& hi) {
-  float x = clampf_(g[0], 0.0f, (float)(d.n0 - 1));
-  float y = clampf_(g[1], 0.0f, (float)(d.n1 - 1));
-  float z = clampf_(g[2], 0.0f, (float)(d.n2 - 1));
-  int i0 = (int)x, j0 = (int)y, k0 = (int)z;
-  int i1 = imin_(i0 + 1, d.n0 - 1), j1 = imin_(j0 + 1, d.n1 - 1), k1 = imin_(k0 + 1, d.n2 - 1);
-  float tx = x - (float)i0, ty = y - (float)j0, tz = z - (float)k0;
-  float a000 = __ldg(f + at(d, i0, j0, k0)), a100 = __ldg(f + at(d, i1, j0, k0));
-  float a010 = __ldg(f + at(d, i0, j1, k0)), a110 = __ldg(f + at(d, i1, j1, k0));
-  float a001 = __ldg(f + at(d, i0, j0, k1)), a101 = __ldg(f + at(d, i1, j0, k1));
-  float a011 = __ldg(f + at(d, i0, j1, k1)), a111 = __ldg(f + at(d, i1, j1, k1));
+  const Axis1 x = axis_of(g[0], d.n0, d.n1 * d.n2), y = axis_of(g[1], d.n1, d.n2), z = axis_of(g[2], d.n2, 1);
+  const float* p = f + (x.i0 * d.n1 + y.i0) * d.n2 + z.i0;
+  const float a000 = __ldg(p), a100 = __ldg(p + x.step);
+  const float a010 = __ldg(p + y.step), a110 = __ldg(p + x.step + y.step);
+  const float a001 = __ldg(p + z.step), a101 = __ldg(p + x.step + z.step);
+  const float a011 = __ldg(p + y.step + z.step), a111 = __ldg(p + x.step + y.step + z.step);
   lo = fmin_(fmin_(fmin_(fmin_(fmin_(fmin_(fmin_(a000, a000), a001), a010), a011), a100), a101), a110);
   lo = fmin_(lo, a111);
   hi = fmax_(fmax_(fmax_(fmax_(fmax_(fmax_(fmax_(a000, a000), a001), a010), a011), a100), a101), a110);
   hi = fmax_(hi, a111);
-  float c00 = lerpf_(a000, a100, tx), c10 = lerpf_(a010, a110, tx);
-  float c01 = lerpf_(a001, a101, tx), c11 = lerpf_(a011, a111, tx);
-  return lerpf_(lerpf_(c00, c10, ty), lerpf_(c01, c11, ty), tz);
+  const float c00 = lerp_w(a000, a100, x), c10 = lerp_w(a010, a110, x);
+  const float c01 = lerp_w(a001, a101, x), c11 = lerp_w(a011, a111, x);
+  return lerp_w(lerp_w(c00, c10, y), lerp_w(c01, c11, y), z);
 }
 
 __device__ __forceinline__ bool is_outside_open_face(F3 p, const PlumeGridInfo& info) {  // sample.py:53-61

@@ -15,7 +15,9 @@
 #include <cooperative_groups.h>
 
 #include <algorithm>
+#include <cstring>
 #include <mutex>
+#include <vector>
 
 #include "poisson.cuh"
 
@@ -661,26 +663,31 @@ static int bottom_start(const PlumeLevel* levels, int count, size_t* smem_bytes)
   return count;
 }
 
-static int launch_bottom(const PlumeLevel* levels, int count, int sweeps, size_t smem, cudaStream_t st) {
+// Lets the coarse solves use up to BOTTOM_MAX_SMEM of shared memory (once per device, outside any capture).
+static int prepare_bottom() {
   static std::mutex mutex;
   static bool configured[64] = {};
   int device = 0;
   int status = runtime_status("current device", cudaGetDevice(&device));
   if (status != PLUME_OK) return status;
-  {
-    std::lock_guard<std::mutex> lock(mutex);
-    if (device >= 0 && device < 64 && !configured[device]) {
+  std::lock_guard<std::mutex> lock(mutex);
+  if (device >= 0 && device < 64 && !configured[device]) {
+    status = runtime_status("coarse solve shared memory",
+                            cudaFuncSetAttribute(k_cluster_solve, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                                 (int)BOTTOM_MAX_SMEM));
+    if (status == PLUME_OK)
       status = runtime_status("coarse solve shared memory",
-                              cudaFuncSetAttribute(k_cluster_solve, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                              cudaFuncSetAttribute(k_block_solve, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                                    (int)BOTTOM_MAX_SMEM));
-      if (status == PLUME_OK)
-        status = runtime_status("coarse solve shared memory",
-                                cudaFuncSetAttribute(k_block_solve, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                                     (int)BOTTOM_MAX_SMEM));
-      if (status != PLUME_OK) return status;
-      configured[device] = true;
-    }
+    if (status != PLUME_OK) return status;
+    configured[device] = true;
   }
+  return PLUME_OK;
+}
+
+static int launch_bottom(const PlumeLevel* levels, int count, int sweeps, size_t smem, cudaStream_t st) {
+  int status = prepare_bottom();
+  if (status != PLUME_OK) return status;
   if (g_bottom_kind == 0) {
     BlockArgs b{};
     b.count = count;
@@ -758,7 +765,7 @@ static int v_cycle(const PlumeLevel* levels, int count, int index, Pressure& q, 
   return sweeps_with_prolong(lv.info, q, lv.rhs, sweeps, 1.0f, coarse.q, &coarse.info, st);
 }
 
-int multigrid_cycles(const PlumeLevel* levels, int count, int cycles, int sweeps, cudaStream_t st) {
+static int multigrid_direct(const PlumeLevel* levels, int count, int cycles, int sweeps, cudaStream_t st) {
   size_t smem = 0;
   const int bottom = bottom_start(levels, count, &smem);
   Pressure q{levels[0].q, levels[0].residual};
@@ -772,6 +779,119 @@ int multigrid_cycles(const PlumeLevel* levels, int count, int cycles, int sweeps
 }
 
 }  // namespace plume
+
+namespace plume {
+
+// ---- replaying the solve as a CUDA graph -----------------------------------------------------------------
+// The launch sequence of a solve depends only on the levels (geometry and arrays), the cycle and sweep
+// counts and the strategy, so it is captured once into a graph (on a private stream: capture records and
+// runs nothing) and replayed on the caller's stream, which saves the per-launch cost of its ~30 launches per
+// V-cycle, most of them short.
+struct GraphKey {
+  int device;
+  int count, cycles, sweeps, kind;
+  long tiled, bottom;
+  PlumeLevel levels[16];
+  bool operator==(const GraphKey& o) const { return std::memcmp(this, &o, sizeof(GraphKey)) == 0; }
+};
+
+struct GraphEntry {
+  GraphKey key;
+  cudaGraphExec_t exec;
+  size_t kernels;  // kernel nodes in the graph
+};
+
+static std::mutex g_graph_mutex;
+static std::vector<GraphEntry> g_graphs;
+static cudaStream_t g_capture_stream[64] = {};
+static bool g_use_graphs = true;
+constexpr size_t MAX_GRAPHS = 32;
+
+static int graph_for(const GraphKey& key, const PlumeLevel* levels, cudaGraphExec_t* out, size_t* kernels) {
+  for (const GraphEntry& e : g_graphs)
+    if (e.key == key) {
+      *out = e.exec;
+      *kernels = e.kernels;
+      return PLUME_OK;
+    }
+  cudaStream_t& cap = g_capture_stream[key.device];
+  int status = PLUME_OK;
+  if (!cap) status = runtime_status("capture stream", cudaStreamCreateWithFlags(&cap, cudaStreamNonBlocking));
+  if (status != PLUME_OK) return status;
+  // one-time function attributes are set outside the capture: run the smallest possible warm-up first
+  status = runtime_status("begin capture", cudaStreamBeginCapture(cap, cudaStreamCaptureModeThreadLocal));
+  if (status != PLUME_OK) return status;
+  set_launch_counting(false);
+  const int run = multigrid_direct(levels, key.count, key.cycles, key.sweeps, cap);
+  set_launch_counting(true);
+  cudaGraph_t graph = nullptr;
+  status = runtime_status("end capture", cudaStreamEndCapture(cap, &graph));
+  if (run != PLUME_OK || status != PLUME_OK) {
+    if (graph) cudaGraphDestroy(graph);
+    return run != PLUME_OK ? run : status;
+  }
+  size_t nodes = 0, kernel_nodes = 0;
+  if (cudaGraphGetNodes(graph, nullptr, &nodes) == cudaSuccess && nodes > 0) {
+    std::vector<cudaGraphNode_t> list(nodes);
+    if (cudaGraphGetNodes(graph, list.data(), &nodes) == cudaSuccess)
+      for (cudaGraphNode_t node : list) {
+        cudaGraphNodeType type;
+        if (cudaGraphNodeGetType(node, &type) == cudaSuccess && type == cudaGraphNodeTypeKernel) ++kernel_nodes;
+      }
+  }
+  cudaGraphExec_t exec = nullptr;
+  status = runtime_status("instantiate graph", cudaGraphInstantiate(&exec, graph, 0));
+  cudaGraphDestroy(graph);
+  if (status != PLUME_OK) return status;
+  if (g_graphs.size() >= MAX_GRAPHS) {
+    cudaGraphExecDestroy(g_graphs.front().exec);
+    g_graphs.erase(g_graphs.begin());
+  }
+  g_graphs.push_back(GraphEntry{key, exec, kernel_nodes});
+  *out = exec;
+  *kernels = kernel_nodes;
+  return PLUME_OK;
+}
+
+int multigrid_cycles(const PlumeLevel* levels, int count, int cycles, int sweeps, cudaStream_t st) {
+  cudaStreamCaptureStatus capturing = cudaStreamCaptureStatusNone;
+  int device = 0;
+  if (!g_use_graphs || count > 16 || cudaStreamIsCapturing(st, &capturing) != cudaSuccess ||
+      capturing != cudaStreamCaptureStatusNone || cudaGetDevice(&device) != cudaSuccess || device < 0 || device >= 64)
+    return multigrid_direct(levels, count, cycles, sweeps, st);
+  GraphKey key;
+  std::memset(&key, 0, sizeof(key));
+  key.device = device;
+  key.count = count;
+  key.cycles = cycles;
+  key.sweeps = sweeps;
+  key.kind = g_bottom_kind;
+  key.tiled = g_tiled_min_cells;
+  key.bottom = g_bottom_max_cells;
+  std::memcpy(key.levels, levels, sizeof(PlumeLevel) * count);
+  std::lock_guard<std::mutex> lock(g_graph_mutex);
+  {  // the coarse solve's shared-memory attribute must be set before its first capture
+    size_t smem = 0;
+    if (bottom_start(levels, count, &smem) < count) {
+      int prepared = prepare_bottom();
+      if (prepared != PLUME_OK) return prepared;
+    }
+  }
+  cudaGraphExec_t exec = nullptr;
+  size_t kernels = 0;
+  int status = graph_for(key, levels, &exec, &kernels);
+  if (status != PLUME_OK) return status;
+  status = runtime_status("graph launch", cudaGraphLaunch(exec, st));
+  if (status == PLUME_OK) count_launches(kernels);
+  return status;
+}
+
+}  // namespace plume
+
+extern "C" int plume_use_graphs(int32_t enable) {
+  plume::g_use_graphs = enable != 0;
+  return PLUME_OK;
+}
 
 extern "C" int plume_tune_solver(long long tiled_min_cells, long long bottom_max_cells, int32_t bottom_kind) {
   if (tiled_min_cells < 1 || bottom_max_cells < 0 || bottom_kind < 0 || bottom_kind > 1)

@@ -27,11 +27,15 @@ int fail(int status, const char* fmt, ...) {
 }
 
 static unsigned long long g_launches = 0;  // kernels enqueued by this library (host-side count)
+static thread_local bool g_counting = true;  // off while a graph is being captured (its replays are counted)
+
+void count_launches(unsigned long long n) { __atomic_add_fetch(&g_launches, n, __ATOMIC_RELAXED); }
+void set_launch_counting(bool on) { g_counting = on; }
 
 int launch_status(const char* what) {
   cudaError_t err = cudaGetLastError();
   if (err != cudaSuccess) return fail(PLUME_ERR_LAUNCH, "%s: %s", what, cudaGetErrorString(err));
-  __atomic_add_fetch(&g_launches, 1ULL, __ATOMIC_RELAXED);
+  if (g_counting) count_launches(1);
   return PLUME_OK;
 }
 
