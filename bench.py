@@ -70,7 +70,7 @@ class ClockSampler:
 
     def __enter__(self):
         try:
-            cmd = ["nvidia-smi", f"--query-gpu={self.QUERY}", "--format=csv,noheader,nounits", "-lms", "200"]
+            cmd = ["nvidia-smi", f"--query-gpu={self.QUERY}", "--format=csv,noheader,nounits", "-lms", "20"]
             if self.uuid:
                 cmd += ["-i", self.uuid]
             self.proc = subprocess.Popen(cmd, stdout=self.file, stderr=subprocess.DEVNULL)

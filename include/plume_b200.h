@@ -251,21 +251,29 @@ int plume_step(const PlumeStepState* state, const PlumeStepParams* params, void*
 
 /* ---- render ------------------------------------------------------------------------------------------ */
 
-/* light_volume.py:18-51 light_volume_kernel. */
+/* light_volume.py:18-51 light_volume_kernel. `bricks` (optional, plume_brick_floats() floats) is scratch for a
+ * map of each 4x4x4 brick's largest smoke value; with it, samples whose eight corners are all <= 0 are
+ * skipped, which leaves every result bit unchanged (they add exactly 0). */
+long long plume_brick_floats(const int32_t shape[3]);
 int plume_light_volume(const int32_t shape[3], const float* smoke, const float toward_light[3], float cell_m,
-                       float opacity_per_density, float* light, void* stream);
+                       float opacity_per_density, float* light, float* bricks, void* stream);
 
 /* normal_field.py:52-61 NormalField.compute (blur_axis_kernel x 3 + gradient_kernel); gradient is
  * (n0, n1, n2, 3). */
 int plume_normal_field(const int32_t shape[3], const float* smoke, float* blurred, float* scratch, float* gradient,
                        const float* weights_host, int32_t radius, void* stream);
 
+/* The brick map of a field (largest value of each 4x4x4 brick and the next cell past it on each axis). */
+int plume_brick_max(const int32_t shape[3], const float* field, float* bricks, void* stream);
+
 /* raymarch.py:86-140 raymarch_kernel; image is (height, width, 5). gradient/light are the unused pass's
- * 1-cell stand-in when not read (frame_renderer.py:29-35). */
+ * 1-cell stand-in when not read (frame_renderer.py:29-35). `bricks` (optional, plume_brick_floats() floats)
+ * is scratch for the marched smoke's brick map, built by this call; with it, samples with no smoke skip their
+ * smoke sample. Terms that are exactly 0 are never evaluated, so the image is the same with or without it. */
 int plume_raymarch(const PlumeGridInfo* info, const float* smoke, const float* temperature, const float* gradient,
                    const int32_t gradient_shape[3], const float* light, const int32_t light_shape[3],
                    const PlumeViewParams* view, const PlumeLookParams* look, float* image, int32_t height,
-                   int32_t width, void* stream);
+                   int32_t width, float* bricks, void* stream);
 
 #ifdef __cplusplus
 }

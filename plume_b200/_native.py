@@ -103,10 +103,12 @@ SIGNATURES = {
     "plume_dissipate": [_INFO, _P, _P, _F, _F, _F, _P],
     "plume_grid_speed": [_INFO, _P, _P, _P, _P, _P],
     "plume_step": [ctypes.POINTER(PlumeStepState), ctypes.POINTER(PlumeStepParams), _P],
-    "plume_light_volume": [_SHAPE, _P, _F3P, _F, _F, _P, _P],
+    "plume_brick_floats": [_SHAPE],
+    "plume_light_volume": [_SHAPE, _P, _F3P, _F, _F, _P, _P, _P],
     "plume_normal_field": [_SHAPE, _P, _P, _P, _P, _F3P, _I, _P],
+    "plume_brick_max": [_SHAPE, _P, _P, _P],
     "plume_raymarch": [_INFO, _P, _P, _P, _SHAPE, _P, _SHAPE, ctypes.POINTER(PlumeViewParams),
-                       ctypes.POINTER(PlumeLookParams), _P, _I, _I, _P],
+                       ctypes.POINTER(PlumeLookParams), _P, _I, _I, _P, _P],
 }
 
 _lib = None
@@ -126,7 +128,8 @@ def lib() -> ctypes.CDLL:
         for name, argtypes in SIGNATURES.items():
             fn = getattr(loaded, name)
             fn.argtypes = argtypes
-            fn.restype = ctypes.c_longlong if name == "plume_advect_scratch_floats" else ctypes.c_int
+            wide = name in ("plume_advect_scratch_floats", "plume_brick_floats")
+            fn.restype = ctypes.c_longlong if wide else ctypes.c_int
         _lib = loaded
     return _lib
 

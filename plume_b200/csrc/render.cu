@@ -27,10 +27,33 @@ __device__ __forceinline__ void slab_range(F3 origin, F3 dir, F3 bmin, F3 bmax, 
   t1out = t_exit;
 }
 
+// ---- empty-space skipping ------------------------------------------------------------------------------------
+// A brick map holds, for each 4x4x4 brick of cells, the largest smoke value of the brick and of the next cell
+// past it on each axis: every corner a trilinear sample with lower corner in the brick can blend. When that
+// is <= 0, every corner is <= 0, their blend is <= 0 (each weighted term is), max(sample, 0) is +0 and the
+// sample adds exactly nothing: skipping it changes no bit of the result.
+constexpr int BRICK = 4;
+
+__host__ __device__ __forceinline__ Dims brick_dims(const Dims& d) {
+  return Dims{(d.n0 + BRICK - 1) / BRICK, (d.n1 + BRICK - 1) / BRICK, (d.n2 + BRICK - 1) / BRICK};
+}
+
+__global__ void k_brick_max(Dims d, const float* __restrict__ f, float* __restrict__ bricks) {
+  const Dims b = brick_dims(d);
+  const int bi = blockIdx.z, bj = blockIdx.y * blockDim.y + threadIdx.y, bk = blockIdx.x * blockDim.x + threadIdx.x;
+  if (bj >= b.n1 || bk >= b.n2) return;
+  float best = -3.0e38f;
+  for (int i = bi * BRICK; i <= imin_(bi * BRICK + BRICK, d.n0 - 1); ++i)
+    for (int j = bj * BRICK; j <= imin_(bj * BRICK + BRICK, d.n1 - 1); ++j)
+      for (int k = bk * BRICK; k <= imin_(bk * BRICK + BRICK, d.n2 - 1); ++k) best = fmaxf(best, __ldg(f + at(d, i, j, k)));
+  bricks[at(b, bi, bj, bk)] = best;
+}
+
 // light_volume_kernel (light_volume.py:18-33): one thread per cell marches toward the light in at most
-// half-cell steps to the box edge and writes exp(-opacity * column * cell_m).
+// half-cell steps to the box edge and writes exp(-opacity * column * cell_m). With `bricks`, samples whose
+// corners are all <= 0 are skipped (they add exactly 0).
 __global__ void k_light_volume(Dims d, const float* __restrict__ smoke, F3 toward, float cell_m, float opacity,
-                               float* __restrict__ light) {
+                               float* __restrict__ light, const float* __restrict__ bricks) {
   const int i = blockIdx.z, j = blockIdx.y * blockDim.y + threadIdx.y, k = blockIdx.x * blockDim.x + threadIdx.x;
   if (j >= d.n1 || k >= d.n2) return;
   const F3 half = f3(0.5f, 0.5f, 0.5f);
@@ -42,9 +65,17 @@ __global__ void k_light_volume(Dims d, const float* __restrict__ smoke, F3 towar
   float column = 0.0f;
   if (steps > 0) {
     float step = length / (float)steps;
+    const Dims bd = brick_dims(d);
     for (int s = 0; s < steps; ++s) {
       F3 position = add3(start, mul3(toward, ((float)s + 0.5f) * step));
-      column = column + fmax_(sample_index_space(smoke, d, sub3(position, half)), 0.0f) * step;
+      const F3 g = sub3(position, half);
+      if (bricks) {
+        const int i0 = (int)fminf(fmaxf(g[0], 0.0f), (float)(d.n0 - 1));
+        const int j0 = (int)fminf(fmaxf(g[1], 0.0f), (float)(d.n1 - 1));
+        const int k0 = (int)fminf(fmaxf(g[2], 0.0f), (float)(d.n2 - 1));
+        if (__ldg(bricks + at(bd, i0 / BRICK, j0 / BRICK, k0 / BRICK)) <= 0.0f) continue;
+      }
+      column = column + fmax_(sample_index_space(smoke, d, g), 0.0f) * step;
     }
   }
   light[at(d, i, j, k)] = exp_f(-opacity * column * cell_m);
@@ -114,10 +145,13 @@ struct MarchArgs {
   Dims d, dg, dl;
 };
 
-// raymarch_kernel (raymarch.py:86-140): one thread per pixel.
+// raymarch_kernel (raymarch.py:86-140): one thread per pixel. Terms that are exactly zero are not evaluated:
+// with no smoke at a sample (all eight corners <= 0 in the brick map, or a blend <= 0) alpha is exactly 0, so
+// the exp, the light or gradient sample and the transmittance update are skipped (they would add +0 or
+// multiply by 1); with no glow the pow is skipped (it would add +0). Every result bit is unchanged.
 __global__ void k_raymarch(MarchArgs a, const float* __restrict__ smoke, const float* __restrict__ temperature,
                            const float* __restrict__ gradient, const float* __restrict__ light, float* __restrict__ image,
-                           int height, int width) {
+                           int height, int width, const float* __restrict__ bricks) {
   const int px = blockIdx.x * blockDim.x + threadIdx.x, py = blockIdx.y * blockDim.y + threadIdx.y;
   if (px >= width || py >= height) return;
   const PlumeViewParams& view = a.view;
@@ -145,21 +179,31 @@ __global__ void k_raymarch(MarchArgs a, const float* __restrict__ smoke, const f
     float length = s1 - s0;
     int steps = (int)ceilf(length / (0.5f * info.cell_m));
     float step_m = length / (float)steps;
+    const Dims bd = brick_dims(a.d);
     for (int s = 0; s < steps; ++s) {
       F3 position = add3(origin, mul3(direction, s0 + ((float)s + 0.5f) * step_m));
       F3 g = sub3(div3(sub3(position, box_origin), info.cell_m), f3(0.5f, 0.5f, 0.5f));
-      float density = fmax_(sample_index_space(smoke, a.d, g), 0.0f);
-      float alpha = 1.0f - exp_f(-look.opacity_per_density * density * step_m);
-      float glow = fmax_(sample_index_space(temperature, a.d, g) - look.glow_start_k, 0.0f);
-      heat = heat + glow * step_m * pow_f(tr, look.smoke_hides_heat);
-      if (look.shade_layout == 1) {
-        float lit = look.shade_fill + (1.0f - look.shade_fill) * sample_index_space(light, a.dl, g);
-        shade_sum = shade_sum + tr * alpha * lit;
-      } else {
-        F3 slope = sample_vec(gradient, a.dg, g);
-        if (alpha > 0.0f && len3(slope) > 1.0e-9f) normal_sum = sub3(normal_sum, mul3(normalize3(slope), tr * alpha));
+      bool empty = false;
+      if (bricks) {
+        const int i0 = (int)fminf(fmaxf(g[0], 0.0f), (float)(a.d.n0 - 1));
+        const int j0 = (int)fminf(fmaxf(g[1], 0.0f), (float)(a.d.n1 - 1));
+        const int k0 = (int)fminf(fmaxf(g[2], 0.0f), (float)(a.d.n2 - 1));
+        empty = __ldg(bricks + at(bd, i0 / BRICK, j0 / BRICK, k0 / BRICK)) <= 0.0f;
       }
-      tr = tr * (1.0f - alpha);
+      const float density = empty ? 0.0f : fmax_(sample_index_space(smoke, a.d, g), 0.0f);
+      const float alpha = density > 0.0f ? 1.0f - exp_f(-look.opacity_per_density * density * step_m) : 0.0f;
+      const float glow = fmax_(sample_index_space(temperature, a.d, g) - look.glow_start_k, 0.0f);
+      if (glow > 0.0f) heat = heat + glow * step_m * pow_f(tr, look.smoke_hides_heat);
+      if (alpha > 0.0f) {
+        if (look.shade_layout == 1) {
+          float lit = look.shade_fill + (1.0f - look.shade_fill) * sample_index_space(light, a.dl, g);
+          shade_sum = shade_sum + tr * alpha * lit;
+        } else {
+          F3 slope = sample_vec(gradient, a.dg, g);
+          if (len3(slope) > 1.0e-9f) normal_sum = sub3(normal_sum, mul3(normalize3(slope), tr * alpha));
+        }
+        tr = tr * (1.0f - alpha);
+      }
     }
   }
   float thickness = 1.0f - tr;
@@ -194,12 +238,25 @@ static bool valid_shape(const int32_t* s) {
 
 using namespace plume;
 
+extern "C" long long plume_brick_floats(const int32_t shape[3]) {
+  if (!valid_shape(shape)) return fail(PLUME_ERR_INVALID, "brick_floats: bad shape");
+  const Dims b = brick_dims(Dims{shape[0], shape[1], shape[2]});
+  return (long long)b.n0 * b.n1 * b.n2;
+}
+
 extern "C" int plume_light_volume(const int32_t shape[3], const float* smoke, const float toward_light[3], float cell_m,
-                                  float opacity_per_density, float* light, void* stream) {
+                                  float opacity_per_density, float* light, float* bricks, void* stream) {
   if (!valid_shape(shape) || !smoke || !toward_light || !light) return fail(PLUME_ERR_INVALID, "light_volume: bad argument");
   Dims d{shape[0], shape[1], shape[2]};
-  k_light_volume<<<cell_grid(d.n0, d.n1, d.n2), cell_block(), 0, as_stream(stream)>>>(
-      d, smoke, f3(toward_light[0], toward_light[1], toward_light[2]), cell_m, opacity_per_density, light);
+  cudaStream_t st = as_stream(stream);
+  if (bricks) {
+    const Dims b = brick_dims(d);
+    k_brick_max<<<cell_grid(b.n0, b.n1, b.n2), cell_block(), 0, st>>>(d, smoke, bricks);
+    int status = launch_status("smoke brick map");
+    if (status != PLUME_OK) return status;
+  }
+  k_light_volume<<<cell_grid(d.n0, d.n1, d.n2), cell_block(), 0, st>>>(
+      d, smoke, f3(toward_light[0], toward_light[1], toward_light[2]), cell_m, opacity_per_density, light, bricks);
   return launch_status("light volume");
 }
 
@@ -225,10 +282,18 @@ extern "C" int plume_normal_field(const int32_t shape[3], const float* smoke, fl
   return launch_status("gradient");
 }
 
+extern "C" int plume_brick_max(const int32_t shape[3], const float* field, float* bricks, void* stream) {
+  if (!valid_shape(shape) || !field || !bricks) return fail(PLUME_ERR_INVALID, "brick_max: bad argument");
+  const Dims d{shape[0], shape[1], shape[2]};
+  const Dims b = brick_dims(d);
+  k_brick_max<<<cell_grid(b.n0, b.n1, b.n2), cell_block(), 0, as_stream(stream)>>>(d, field, bricks);
+  return launch_status("brick map");
+}
+
 extern "C" int plume_raymarch(const PlumeGridInfo* info, const float* smoke, const float* temperature,
                               const float* gradient, const int32_t gradient_shape[3], const float* light,
                               const int32_t light_shape[3], const PlumeViewParams* view, const PlumeLookParams* look,
-                              float* image, int32_t height, int32_t width, void* stream) {
+                              float* image, int32_t height, int32_t width, float* bricks, void* stream) {
   if (!info || !smoke || !temperature || !gradient || !light || !view || !look || !image || height < 1 || width < 1 ||
       !valid_shape(info->dims) || !valid_shape(gradient_shape) || !valid_shape(light_shape))
     return fail(PLUME_ERR_INVALID, "raymarch: bad argument");
@@ -239,7 +304,14 @@ extern "C" int plume_raymarch(const PlumeGridInfo* info, const float* smoke, con
   a.d = Dims{info->dims[0], info->dims[1], info->dims[2]};
   a.dg = Dims{gradient_shape[0], gradient_shape[1], gradient_shape[2]};
   a.dl = Dims{light_shape[0], light_shape[1], light_shape[2]};
+  cudaStream_t st = as_stream(stream);
+  if (bricks) {  // the brick map of exactly the smoke being marched
+    const Dims b = brick_dims(a.d);
+    k_brick_max<<<cell_grid(b.n0, b.n1, b.n2), cell_block(), 0, st>>>(a.d, smoke, bricks);
+    int status = launch_status("smoke brick map");
+    if (status != PLUME_OK) return status;
+  }
   dim3 block(16, 16), grid((width + 15) / 16, (height + 15) / 16);
-  k_raymarch<<<grid, block, 0, as_stream(stream)>>>(a, smoke, temperature, gradient, light, image, height, width);
+  k_raymarch<<<grid, block, 0, st>>>(a, smoke, temperature, gradient, light, image, height, width, bricks);
   return launch_status("raymarch");
 }

@@ -33,6 +33,8 @@ class FrameRenderer:
             self.gradient = self.normal_field.gradient
             self.light = torch.zeros((1, 1, 1), dtype=torch.float32, device=device)
         self.image = torch.zeros((view.height_px, view.width_px, CHANNELS), dtype=torch.float32, device=device)
+        # scratch for the marched smoke's brick map (empty-space skipping; built by every march)
+        self.bricks = torch.empty(N.lib().plume_brick_floats(N.c_int3(*cells)), dtype=torch.float32, device=device)
         self._host = torch.empty(self.image.shape, dtype=torch.float32, pin_memory=True)
 
     def render(self, grid) -> np.ndarray:
@@ -48,15 +50,18 @@ class FrameRenderer:
 
     def prepare(self, smoke, cell_m: float) -> None:
         if self.shade_layout:
-            self.light = self.light_volume.compute(smoke, cell_m)
+            self.light = self.light_volume.compute(smoke, cell_m)  # also fills the brick map
         else:
             self.gradient = self.normal_field.compute(smoke)
 
     def march(self, smoke, temperature, info, view: ViewParams, image) -> None:
+        """Marches `image` for `view` through the fields, with the volume pass of the last prepare."""
         gradient_shape = N.c_int3(*self.gradient.shape[:3])
+        bricks = N.ptr(self.bricks) if tuple(self.bricks.shape) == (N.lib().plume_brick_floats(N.shape3(smoke)),) \
+            else None
         N.call("plume_raymarch", info, N.ptr(smoke), N.ptr(temperature), N.ptr(self.gradient), gradient_shape,
                N.ptr(self.light), N.shape3(self.light), view, self.look_params, N.ptr(image), image.shape[0],
-               image.shape[1], N.stream())
+               image.shape[1], bricks, N.stream())
 
 
 def toward_light_world(camera, light_dir) -> np.ndarray:

@@ -14,8 +14,10 @@ class LightVolume:
         self.toward_light = tuple(float(x) for x in direction / np.linalg.norm(direction))
         self.opacity_per_density = opacity_per_density
         self.light = torch.zeros(tuple(cells), dtype=torch.float32, device=device)
+        # per-frame map of each 4x4x4 brick's largest smoke value: the march skips samples that add nothing
+        self.bricks = torch.empty(N.lib().plume_brick_floats(N.c_int3(*cells)), dtype=torch.float32, device=device)
 
     def compute(self, smoke: torch.Tensor, cell_m: float) -> torch.Tensor:
         N.call("plume_light_volume", N.shape3(smoke), N.ptr(smoke), N.f3(self.toward_light), cell_m,
-               self.opacity_per_density, N.ptr(self.light), N.stream())
+               self.opacity_per_density, N.ptr(self.light), N.ptr(self.bricks), N.stream())
         return self.light

@@ -37,6 +37,24 @@ def test_light_volume_matches_the_oracle(cuda_device):
     assert max_rel(host(light), expected, floor=1e-6) < LIGHT_RTOL
 
 
+def test_light_volume_empty_space_skipping_changes_no_bit(cuda_device):
+    """The brick map only skips samples that add exactly 0: the light volume is bit-identical without it."""
+    import torch
+
+    from plume_b200 import _native as N
+
+    o, c = render_pair()
+    smoke = c.smoke.data
+    toward = N.f3(np.array([0.5, 0.8, 0.3]) / np.linalg.norm([0.5, 0.8, 0.3]))
+    with_bricks, without = torch.empty_like(smoke), torch.empty_like(smoke)
+    bricks = torch.empty(N.lib().plume_brick_floats(N.shape3(smoke)), dtype=torch.float32, device="cuda:0")
+    N.call("plume_light_volume", N.shape3(smoke), N.ptr(smoke), toward, 0.05, 4.0, N.ptr(with_bricks), N.ptr(bricks),
+           N.stream())
+    N.call("plume_light_volume", N.shape3(smoke), N.ptr(smoke), toward, 0.05, 4.0, N.ptr(without), None, N.stream())
+    assert torch.equal(with_bricks, without)
+    assert float((smoke <= 0).float().mean()) > 0.5  # the case has plenty of empty space to skip
+
+
 @pytest.mark.parametrize("channels", [SHADE_LAYOUT, NORMAL_LAYOUT])
 @pytest.mark.parametrize("elevation,azimuth", [(0.0, 0.0), (20.0, 30.0), (90.0, 0.0), (-35.0, 200.0)])
 def test_frame_matches_the_oracle(cuda_device, channels, elevation, azimuth):
@@ -53,6 +71,29 @@ def test_frame_matches_the_oracle(cuda_device, channels, elevation, azimuth):
     heat_scale = max(float(np.abs(expected[..., 0]).max()), 1.0)
     assert np.abs(image[..., 0] - expected[..., 0]).max() < MARCH_ATOL * heat_scale * 10
     assert np.abs(image[..., 1:] - expected[..., 1:]).max() < MARCH_ATOL * 10
+
+
+@pytest.mark.parametrize("channels", [SHADE_LAYOUT, NORMAL_LAYOUT])
+def test_march_empty_space_skipping_changes_no_bit(cuda_device, channels):
+    import torch
+
+    from plume_b200 import _native as N
+    from plume_b200.render.frame_renderer import FrameRenderer
+
+    o, c = render_pair()
+    cells = c.cells
+    size = tuple(n * 0.05 for n in cells)
+    view = make_domain_view(make_camera(20.0, 30.0), (-size[0] / 2, 0.0, -size[2] / 2), size, 0.05, 2.0)
+    renderer = FrameRenderer(view, RenderSettings(glow_start_k=600.0, light_dir=(0.5, 0.8, 0.3)), cells, channels,
+                             "cuda:0")
+    renderer.prepare(c.smoke.data, c.info.cell_m)
+    skipped = torch.zeros_like(renderer.image)
+    full = torch.zeros_like(renderer.image)
+    renderer.march(c.smoke.data, c.temperature.data, c.info, renderer.view_params, skipped)
+    N.call("plume_raymarch", c.info, N.ptr(c.smoke.data), N.ptr(c.temperature.data), N.ptr(renderer.gradient),
+           N.c_int3(*renderer.gradient.shape[:3]), N.ptr(renderer.light), N.shape3(renderer.light),
+           renderer.view_params, renderer.look_params, N.ptr(full), full.shape[0], full.shape[1], None, N.stream())
+    assert torch.equal(skipped, full)
 
 
 def test_normal_field_matches_the_oracle(cuda_device):
