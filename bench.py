@@ -36,6 +36,9 @@ METRIC = "Mcell-substeps/s"
 PHASE_BYTES = {"forces": 32.0, "velocity advection": 24.0, "divergence": 16.0, "pressure solve": None,
                "gradient": 28.0, "scalar advection": 44.0}
 MG_BYTES_PER_CYCLE = 74.0
+# DRAM bytes (read + write) per top-level cell per V-cycle that ncu counted for the pressure-solve kernels of
+# the 128x192x128 step (1099.9 MB per substep at 4 cycles); the solve's traffic scales with the level cells.
+MG_TRAFFIC_PER_CYCLE = 1099.9e6 / (128 * 192 * 128) / 4
 
 
 def parse_args():
@@ -216,6 +219,7 @@ def main():
     for n in range(args.warmup):
         stepper.step(n * dt, dt)
     torch.cuda.synchronize()
+    resident_gb = torch.cuda.memory_allocated(local) / 1e9  # the grid and every scratch array of the step
 
     # timed region: K substeps, phase events recorded inside plume_step on the same stream
     phases = N.STEP_PHASES
@@ -315,9 +319,10 @@ def main():
                                f"velocities, masked smoke sphere), {cycles} multigrid V-cycles x 2+2 sweeps, "
                                f"confinement + drag + emitter, dt 1/96 s",
                    "cells": list(derived.cells), "parallelism": f"replicas x{world}",
-                   "l2": "inputs larger than L2 (state about 0.3 GB per grid)"},
+                   "l2": f"inputs larger than L2 ({resident_gb:.2f} GB resident per grid; L2 is 126 MB)"},
         "roofline": {"bound": "hbm", "kernel": f"{dominant} phase of plume_step", "achieved": achieved, "peak": peak,
-                     "unit": "GB/s", "frac": achieved / peak if achieved else None, "traffic": None,
+                     "unit": "GB/s", "frac": achieved / peak if achieved else None,
+                     "traffic": (MG_TRAFFIC_PER_CYCLE * cycles * ncells if dominant == "pressure solve" else None),
                      "peak_kind": peak_kind},
         "step_roofline": {"bytes_per_cell_substep": step_bytes,
                           "achieved": step_bytes * ncells * args.steps / (max_ms / 1e3) / 1e9,

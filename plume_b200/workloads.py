@@ -89,3 +89,42 @@ def smoke_puff_recipe(cells=(64, 96, 64), frames: int = 48):
         "output": {"frame_px": 128},
     }
     return resolve_table(table, "smoke_puff_c1")
+
+
+def run_plain_steps(cells=(128, 192, 128), substeps: int = 1, device: str = "cuda:0", render: bool = False):
+    """Steps the seeded operator-level state `substeps` times through Stepper.step (and renders one frame when
+    `render`), for profiling single kernels on a small case."""
+    import torch
+
+    from plume_b200.recipe.derived import derive
+    from plume_b200.render.camera import sheet_domain_view
+    from plume_b200.render.frame_renderer import FrameRenderer
+    from plume_b200.sim.grid import make_grid
+    from plume_b200.sim.stepper import Stepper
+
+    recipe = plain_step_recipe(tuple(cells))
+    derived = derive(recipe)
+    d = recipe.domain
+    grid = make_grid(derived, d.cell_m, d.faces, d.ambient_k, device)
+    for name, values in operator_fields(derived.cells, DEFAULT_SEED, d.ambient_k).items():
+        getattr(grid, name).data.copy_(torch.from_numpy(values))
+    stepper = Stepper(grid, recipe)
+    for n in range(substeps):
+        stepper.step(n * derived.dt_s, derived.dt_s)
+    if render:
+        view = sheet_domain_view(recipe, derived)
+        FrameRenderer(view, recipe.render, derived.cells, recipe.output.channels, device).render(grid)
+    torch.cuda.synchronize()
+    return grid
+
+
+if __name__ == "__main__":
+    import argparse
+
+    ap = argparse.ArgumentParser(description="run the plain step on the seeded operator-level state")
+    ap.add_argument("--cells", default="128,192,128")
+    ap.add_argument("--substeps", type=int, default=1)
+    ap.add_argument("--render", action="store_true")
+    args = ap.parse_args()
+    run_plain_steps(tuple(int(x) for x in args.cells.split(",")), args.substeps, render=args.render)
+    print("ok")
