@@ -26,6 +26,12 @@ extern "C" {
 #define PLUME_ERR_LAUNCH (-2)  /* a kernel launch or CUDA runtime call failed */
 #define PLUME_ERR_DEVICE (-3)  /* a device-side check failed (reported through a status word) */
 
+/* Storage of velocity, smoke and temperature arrays (plume_step, the render calls, plume_grid_speed); kernels
+ * always compute in float. Pressure, divergence and scratch arrays are float in every mode. */
+#define PLUME_STORAGE_F32 0
+#define PLUME_STORAGE_BF16 1 /* bfloat16, rounded to nearest even on store */
+#define PLUME_STORAGE_F16 2  /* IEEE half, rounded to nearest even on store */
+
 #define PLUME_MAX_EMITTERS 16 /* emitters applied per launch; longer lists are applied in order, in chunks */
 #define PLUME_STEP_PHASES 6   /* forces, velocity advection, divergence, pressure solve, gradient, scalars */
 
@@ -80,12 +86,12 @@ typedef struct PlumeLookParams {
   float shade_fill;
 } PlumeLookParams;
 
-/* One advected quantity's buffers (AdvectedField, sim/grid.py:36-51). `back` is not needed: the MacCormack
- * correction recomputes the backward pass on the fly. */
+/* One advected quantity's buffers (AdvectedField, sim/grid.py:36-51), elements of the step's storage type.
+ * `back` is not needed: the MacCormack correction recomputes the backward pass on the fly. */
 typedef struct PlumeField {
-  float* data;
-  float* hat;
-  float* next;
+  void* data;
+  void* hat;
+  void* next;
 } PlumeField;
 
 /* One multigrid level (multigrid.py:71-77): its geometry and pressure, right-hand side, residual arrays. */
@@ -109,12 +115,14 @@ typedef struct PlumeStepState {
   double* sums;
   float* factor;
   /* scratch (optional, may be null): plume_advect_scratch_floats() floats; with it the MacCormack forward
-   * pass stores each element's clamp range and the correction does not trace forward a second time */
+   * pass stores each element's clamp range (two values of the storage type) and the correction does not
+   * trace forward a second time */
   float* advect_scratch;
   /* pressure-solve levels: levels[0] aliases pressure/divergence and its residual array is the sweeps' second
    * pressure array (Gauss-Seidel uses levels[0] only); coarser multigrid levels are caller-allocated */
   const PlumeLevel* levels;
   int32_t level_count;
+  int32_t storage;          /* PLUME_STORAGE_*: the type of the u, v, w, smoke and temperature arrays */
 } PlumeStepState;
 
 typedef struct PlumeStepParams {
@@ -202,6 +210,8 @@ int plume_multigrid(const PlumeLevel* levels, int32_t level_count, int32_t cycle
  * bottom_kind 1 an 8-CTA thread-block cluster (levels split in x-slabs over the CTAs' shared memory), 0 one
  * 1024-thread block; at most 200 KiB of shared memory per CTA. Process-wide; defaults 2^40, 8192, 0. */
 int plume_tune_solver(long long tiled_min_cells, long long bottom_max_cells, int32_t bottom_kind);
+/* The current pressure-solve strategy (the three values plume_tune_solver sets). */
+int plume_solver_tuning(long long* tiled_min_cells, long long* bottom_max_cells, int32_t* bottom_kind);
 
 /* Pressure solves replay a CUDA graph of their launches, captured once per levels/cycles/strategy (default
  * on). 0 turns that off (every kernel launched one by one); results are the same either way. When the
@@ -241,9 +251,9 @@ int plume_triple_sum(const int32_t shape[3], const float* a, const float* b, con
 int plume_dissipate(const PlumeGridInfo* info, float* smoke, float* temperature, float smoke_keep,
                     float heat_keep, float ambient_k, void* stream);
 
-/* step_cap.py:50-55 StepCap.grid_speed: largest |u|, |v|, |w| into *speed (device float). */
-int plume_grid_speed(const PlumeGridInfo* info, const float* u, const float* v, const float* w, float* speed,
-                     void* stream);
+/* step_cap.py:50-55 StepCap.grid_speed: largest |u|, |v|, |w| (stored as `storage`) into *speed (device float). */
+int plume_grid_speed(const PlumeGridInfo* info, const void* u, const void* v, const void* w, int32_t storage,
+                     float* speed, void* stream);
 
 /* stepper.py:28-44 Stepper.step: one whole substep. On return the caller swaps data/next of u, v, w, smoke and
  * temperature, as the reference's AdvectedField.swap does. */
@@ -255,25 +265,25 @@ int plume_step(const PlumeStepState* state, const PlumeStepParams* params, void*
  * map of each 4x4x4 brick's largest smoke value; with it, samples whose eight corners are all <= 0 are
  * skipped, which leaves every result bit unchanged (they add exactly 0). */
 long long plume_brick_floats(const int32_t shape[3]);
-int plume_light_volume(const int32_t shape[3], const float* smoke, const float toward_light[3], float cell_m,
-                       float opacity_per_density, float* light, float* bricks, void* stream);
+int plume_light_volume(const int32_t shape[3], const void* smoke, int32_t storage, const float toward_light[3],
+                       float cell_m, float opacity_per_density, float* light, float* bricks, void* stream);
 
 /* normal_field.py:52-61 NormalField.compute (blur_axis_kernel x 3 + gradient_kernel); gradient is
  * (n0, n1, n2, 3). */
-int plume_normal_field(const int32_t shape[3], const float* smoke, float* blurred, float* scratch, float* gradient,
-                       const float* weights_host, int32_t radius, void* stream);
+int plume_normal_field(const int32_t shape[3], const void* smoke, int32_t storage, float* blurred, float* scratch,
+                       float* gradient, const float* weights_host, int32_t radius, void* stream);
 
 /* The brick map of a field (largest value of each 4x4x4 brick and the next cell past it on each axis). */
-int plume_brick_max(const int32_t shape[3], const float* field, float* bricks, void* stream);
+int plume_brick_max(const int32_t shape[3], const void* field, int32_t storage, float* bricks, void* stream);
 
 /* raymarch.py:86-140 raymarch_kernel; image is (height, width, 5). gradient/light are the unused pass's
  * 1-cell stand-in when not read (frame_renderer.py:29-35). `bricks` (optional, plume_brick_floats() floats)
  * is scratch for the marched smoke's brick map, built by this call; with it, samples with no smoke skip their
  * smoke sample. Terms that are exactly 0 are never evaluated, so the image is the same with or without it. */
-int plume_raymarch(const PlumeGridInfo* info, const float* smoke, const float* temperature, const float* gradient,
-                   const int32_t gradient_shape[3], const float* light, const int32_t light_shape[3],
-                   const PlumeViewParams* view, const PlumeLookParams* look, float* image, int32_t height,
-                   int32_t width, float* bricks, void* stream);
+int plume_raymarch(const PlumeGridInfo* info, const void* smoke, const void* temperature, int32_t storage,
+                   const float* gradient, const int32_t gradient_shape[3], const float* light,
+                   const int32_t light_shape[3], const PlumeViewParams* view, const PlumeLookParams* look, float* image,
+                   int32_t height, int32_t width, float* bricks, void* stream);
 
 #ifdef __cplusplus
 }

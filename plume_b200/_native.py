@@ -56,7 +56,17 @@ class PlumeStepState(ctypes.Structure):
                 ("divergence", ctypes.c_void_p), ("curl", ctypes.c_void_p * 3), ("push", ctypes.c_void_p * 3),
                 ("sums", ctypes.c_void_p), ("factor", ctypes.c_void_p), ("advect_scratch", ctypes.c_void_p),
                 ("levels", ctypes.POINTER(PlumeLevel)),
-                ("level_count", ctypes.c_int32)]
+                ("level_count", ctypes.c_int32), ("storage", ctypes.c_int32)]
+
+
+# Storage codes of the velocity, smoke and temperature arrays (PLUME_STORAGE_*): float32, bfloat16, float16.
+STORAGE = {torch.float32: 0, torch.bfloat16: 1, torch.float16: 2}
+
+
+def storage_of(tensor: torch.Tensor) -> int:
+    if tensor.dtype not in STORAGE:
+        raise TypeError(f"fields are stored as float32, bfloat16 or float16, not {tensor.dtype}")
+    return STORAGE[tensor.dtype]
 
 
 class PlumeStepParams(ctypes.Structure):
@@ -94,6 +104,8 @@ SIGNATURES = {
     "plume_multigrid": [ctypes.POINTER(PlumeLevel), _I, _I, _I, _P],
     "plume_residual": [_INFO, _P, _P, _P, _P],
     "plume_tune_solver": [ctypes.c_longlong, ctypes.c_longlong, _I],
+    "plume_solver_tuning": [ctypes.POINTER(ctypes.c_longlong), ctypes.POINTER(ctypes.c_longlong),
+                            ctypes.POINTER(ctypes.c_int32)],
     "plume_use_graphs": [_I],
     "plume_smoke_scratch_doubles": [_INFO],
     "plume_advect_scratch_floats": [_INFO],
@@ -101,13 +113,13 @@ SIGNATURES = {
     "plume_triple_sum": [_SHAPE, _P, _P, _P, _P, _P, _P],
     "plume_smoke_budget_static": [_INFO, _P, _P, _P, _P, _P],
     "plume_dissipate": [_INFO, _P, _P, _F, _F, _F, _P],
-    "plume_grid_speed": [_INFO, _P, _P, _P, _P, _P],
+    "plume_grid_speed": [_INFO, _P, _P, _P, _I, _P, _P],
     "plume_step": [ctypes.POINTER(PlumeStepState), ctypes.POINTER(PlumeStepParams), _P],
     "plume_brick_floats": [_SHAPE],
-    "plume_light_volume": [_SHAPE, _P, _F3P, _F, _F, _P, _P, _P],
-    "plume_normal_field": [_SHAPE, _P, _P, _P, _P, _F3P, _I, _P],
-    "plume_brick_max": [_SHAPE, _P, _P, _P],
-    "plume_raymarch": [_INFO, _P, _P, _P, _SHAPE, _P, _SHAPE, ctypes.POINTER(PlumeViewParams),
+    "plume_light_volume": [_SHAPE, _P, _I, _F3P, _F, _F, _P, _P, _P],
+    "plume_normal_field": [_SHAPE, _P, _I, _P, _P, _P, _F3P, _I, _P],
+    "plume_brick_max": [_SHAPE, _P, _I, _P, _P],
+    "plume_raymarch": [_INFO, _P, _P, _I, _P, _SHAPE, _P, _SHAPE, ctypes.POINTER(PlumeViewParams),
                        ctypes.POINTER(PlumeLookParams), _P, _I, _I, _P, _P],
 }
 
@@ -145,6 +157,12 @@ def call(name: str, *args) -> None:
 
 def stream() -> ctypes.c_void_p:
     return ctypes.c_void_p(torch.cuda.current_stream().cuda_stream)
+
+
+def field_ptr(tensor: torch.Tensor) -> ctypes.c_void_p:
+    """The device address of a field array stored as float32, bfloat16 or float16."""
+    storage_of(tensor)
+    return ptr(tensor, tensor.dtype)
 
 
 def ptr(tensor: torch.Tensor, dtype=torch.float32) -> ctypes.c_void_p:

@@ -7,6 +7,8 @@
 // in double and rounded once to float (within 1 ulp of the C library's expf/powf the reference calls).
 #pragma once
 
+#include <cuda_bf16.h>
+#include <cuda_fp16.h>
 #include <cuda_runtime.h>
 #include <stdint.h>
 
@@ -59,6 +61,53 @@ __host__ __device__ __forceinline__ Dims dims_of(const PlumeGridInfo& info) {
   return Dims{info.dims[0], info.dims[1], info.dims[2]};
 }
 
+// ---- field storage ----------------------------------------------------------------------------------------
+// Velocity, smoke and temperature may be stored as float, bfloat16 or half (PLUME_STORAGE_*); every kernel
+// loads them as float, computes in float and rounds once to the storage type (round to nearest even) when it
+// stores. Pressure, divergence and all scratch stay float.
+template <class T>
+__device__ __forceinline__ float to_f(T x);
+template <>
+__device__ __forceinline__ float to_f<float>(float x) { return x; }
+template <>
+__device__ __forceinline__ float to_f<__nv_bfloat16>(__nv_bfloat16 x) { return __bfloat162float(x); }
+template <>
+__device__ __forceinline__ float to_f<__half>(__half x) { return __half2float(x); }
+
+template <class T>
+__device__ __forceinline__ T from_f(float x);
+template <>
+__device__ __forceinline__ float from_f<float>(float x) { return x; }
+template <>
+__device__ __forceinline__ __nv_bfloat16 from_f<__nv_bfloat16>(float x) { return __float2bfloat16_rn(x); }
+template <>
+__device__ __forceinline__ __half from_f<__half>(float x) { return __float2half_rn(x); }
+
+// read-only (non-coherent) load of an element that no thread of the kernel writes
+template <class T>
+__device__ __forceinline__ float ldg_f(const T* p) { return to_f<T>(__ldg(p)); }
+// load / store of an element the kernel also writes
+template <class T>
+__device__ __forceinline__ float ld_f(const T* p) { return to_f<T>(*p); }
+template <class T>
+__device__ __forceinline__ void st_f(T* p, float x) { *p = from_f<T>(x); }
+
+// A pair of values of the storage type (a clamp range): float2, __nv_bfloat162 or __half2.
+template <class T> struct Pair;
+template <> struct Pair<float> { using type = float2; };
+template <> struct Pair<__nv_bfloat16> { using type = __nv_bfloat162; };
+template <> struct Pair<__half> { using type = __half2; };
+template <class T>
+using pair_t = typename Pair<T>::type;
+
+template <class T>
+__device__ __forceinline__ pair_t<T> make_pair_t(float lo, float hi) {
+  pair_t<T> r;
+  r.x = from_f<T>(lo);
+  r.y = from_f<T>(hi);
+  return r;
+}
+
 // One axis of a trilinear sample: the clamped position's lower index, the step to the upper corner (0 at the
 // far edge) and the weights, computed once per axis. The clamp uses min/max, which differs from the reference's
 // comparisons only in the sign of a zero (the same values follow).
@@ -82,27 +131,28 @@ __device__ __forceinline__ Axis1 axis_of(float g, int n, int stride) {
 __device__ __forceinline__ float lerp_w(float a, float b, const Axis1& w) { return a * w.one_minus_t + b * w.t; }
 
 // Trilinear sample at continuous index g, clamped to the array (sim/sample.py:10-29).
-__device__ __forceinline__ float sample_index_space(const float* __restrict__ f, const Dims& d, F3 g) {
+template <class T>
+__device__ __forceinline__ float sample_index_space(const T* __restrict__ f, const Dims& d, F3 g) {
   const Axis1 x = axis_of(g[0], d.n0, d.n1 * d.n2), y = axis_of(g[1], d.n1, d.n2), z = axis_of(g[2], d.n2, 1);
-  const float* p = f + (x.i0 * d.n1 + y.i0) * d.n2 + z.i0;
-  const float c00 = lerp_w(__ldg(p), __ldg(p + x.step), x);
-  const float c10 = lerp_w(__ldg(p + y.step), __ldg(p + x.step + y.step), x);
-  const float c01 = lerp_w(__ldg(p + z.step), __ldg(p + x.step + z.step), x);
-  const float c11 = lerp_w(__ldg(p + y.step + z.step), __ldg(p + x.step + y.step + z.step), x);
+  const T* p = f + (x.i0 * d.n1 + y.i0) * d.n2 + z.i0;
+  const float c00 = lerp_w(ldg_f(p), ldg_f(p + x.step), x);
+  const float c10 = lerp_w(ldg_f(p + y.step), ldg_f(p + x.step + y.step), x);
+  const float c01 = lerp_w(ldg_f(p + z.step), ldg_f(p + x.step + z.step), x);
+  const float c11 = lerp_w(ldg_f(p + y.step + z.step), ldg_f(p + x.step + y.step + z.step), x);
   return lerp_w(lerp_w(c00, c10, y), lerp_w(c01, c11, y), z);
 }
 
 // The value and the min/max of the eight values a trilinear sample blends (sample.py:10-50), from one set
 // of loads: MacCormack's forward pass and its clamp bounds read the same corners. The min/max run in the
 // reference's corner order.
-__device__ __forceinline__ float sample_with_range(const float* __restrict__ f, const Dims& d, F3 g, float& lo,
-                                                   float& hi) {
+template <class T>
+__device__ __forceinline__ float sample_with_range(const T* __restrict__ f, const Dims& d, F3 g, float& lo, float& hi) {
   const Axis1 x = axis_of(g[0], d.n0, d.n1 * d.n2), y = axis_of(g[1], d.n1, d.n2), z = axis_of(g[2], d.n2, 1);
-  const float* p = f + (x.i0 * d.n1 + y.i0) * d.n2 + z.i0;
-  const float a000 = __ldg(p), a100 = __ldg(p + x.step);
-  const float a010 = __ldg(p + y.step), a110 = __ldg(p + x.step + y.step);
-  const float a001 = __ldg(p + z.step), a101 = __ldg(p + x.step + z.step);
-  const float a011 = __ldg(p + y.step + z.step), a111 = __ldg(p + x.step + y.step + z.step);
+  const T* p = f + (x.i0 * d.n1 + y.i0) * d.n2 + z.i0;
+  const float a000 = ldg_f(p), a100 = ldg_f(p + x.step);
+  const float a010 = ldg_f(p + y.step), a110 = ldg_f(p + x.step + y.step);
+  const float a001 = ldg_f(p + z.step), a101 = ldg_f(p + x.step + z.step);
+  const float a011 = ldg_f(p + y.step + z.step), a111 = ldg_f(p + x.step + y.step + z.step);
   lo = fmin_(fmin_(fmin_(fmin_(fmin_(fmin_(fmin_(a000, a000), a001), a010), a011), a100), a101), a110);
   lo = fmin_(lo, a111);
   hi = fmax_(fmax_(fmax_(fmax_(fmax_(fmax_(fmax_(a000, a000), a001), a010), a011), a100), a101), a110);
@@ -121,15 +171,18 @@ __device__ __forceinline__ bool is_outside_open_face(F3 p, const PlumeGridInfo& 
   return false;
 }
 
-struct Vel {
-  const float* __restrict__ u;
-  const float* __restrict__ v;
-  const float* __restrict__ w;
+template <class T>
+struct VelT {
+  const T* __restrict__ u;
+  const T* __restrict__ v;
+  const T* __restrict__ w;
   Dims du, dv, dw;
 };
+using Vel = VelT<float>;
 
-__host__ __device__ __forceinline__ Vel make_vel(const float* u, const float* v, const float* w, const int* dims) {
-  Vel r;
+template <class T>
+__host__ __device__ __forceinline__ VelT<T> make_vel(const T* u, const T* v, const T* w, const int* dims) {
+  VelT<T> r;
   r.u = u;
   r.v = v;
   r.w = w;
@@ -139,14 +192,16 @@ __host__ __device__ __forceinline__ Vel make_vel(const float* u, const float* v,
   return r;
 }
 
-__device__ __forceinline__ F3 velocity_at(const Vel& vel, F3 p) {  // sample.py:74-82
+template <class T>
+__device__ __forceinline__ F3 velocity_at(const VelT<T>& vel, F3 p) {  // sample.py:74-82
   return f3(sample_index_space(vel.u, vel.du, sub3(p, f3(0.0f, 0.5f, 0.5f))),
             sample_index_space(vel.v, vel.dv, sub3(p, f3(0.5f, 0.0f, 0.5f))),
             sample_index_space(vel.w, vel.dw, sub3(p, f3(0.5f, 0.5f, 0.0f))));
 }
 
 // Midpoint backtrace (advect.py:16-21); a negative dt_over_cell traces forward.
-__device__ __forceinline__ F3 trace(const Vel& vel, F3 p, float dt_over_cell) {
+template <class T>
+__device__ __forceinline__ F3 trace(const VelT<T>& vel, F3 p, float dt_over_cell) {
   F3 mid = sub3(p, mul3(velocity_at(vel, p), 0.5f * dt_over_cell));
   return sub3(p, mul3(velocity_at(vel, mid), dt_over_cell));
 }

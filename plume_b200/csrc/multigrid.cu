@@ -797,19 +797,28 @@ struct GraphKey {
 
 struct GraphEntry {
   GraphKey key;
+  uint64_t hash;
   cudaGraphExec_t exec;
   size_t kernels;  // kernel nodes in the graph
 };
+
+static uint64_t key_hash(const GraphKey& key) {  // FNV-1a over the key's bytes
+  uint64_t h = 1469598103934665603ull;
+  const unsigned char* bytes = reinterpret_cast<const unsigned char*>(&key);
+  for (size_t i = 0; i < sizeof(GraphKey); ++i) h = (h ^ bytes[i]) * 1099511628211ull;
+  return h;
+}
 
 static std::mutex g_graph_mutex;
 static std::vector<GraphEntry> g_graphs;
 static cudaStream_t g_capture_stream[64] = {};
 static bool g_use_graphs = true;
-constexpr size_t MAX_GRAPHS = 32;
+constexpr size_t MAX_GRAPHS = 1024;  // one per live level hierarchy (batched runs hold many)
 
 static int graph_for(const GraphKey& key, const PlumeLevel* levels, cudaGraphExec_t* out, size_t* kernels) {
+  const uint64_t hash = key_hash(key);
   for (const GraphEntry& e : g_graphs)
-    if (e.key == key) {
+    if (e.hash == hash && e.key == key) {
       *out = e.exec;
       *kernels = e.kernels;
       return PLUME_OK;
@@ -847,7 +856,7 @@ static int graph_for(const GraphKey& key, const PlumeLevel* levels, cudaGraphExe
     cudaGraphExecDestroy(g_graphs.front().exec);
     g_graphs.erase(g_graphs.begin());
   }
-  g_graphs.push_back(GraphEntry{key, exec, kernel_nodes});
+  g_graphs.push_back(GraphEntry{key, hash, exec, kernel_nodes});
   *out = exec;
   *kernels = kernel_nodes;
   return PLUME_OK;
@@ -899,5 +908,14 @@ extern "C" int plume_tune_solver(long long tiled_min_cells, long long bottom_max
   plume::g_tiled_min_cells = (long)tiled_min_cells;
   plume::g_bottom_max_cells = (long)bottom_max_cells;
   plume::g_bottom_kind = bottom_kind;
+  return PLUME_OK;
+}
+
+extern "C" int plume_solver_tuning(long long* tiled_min_cells, long long* bottom_max_cells, int32_t* bottom_kind) {
+  if (!tiled_min_cells || !bottom_max_cells || !bottom_kind)
+    return plume::fail(PLUME_ERR_INVALID, "solver_tuning: null output");
+  *tiled_min_cells = plume::g_tiled_min_cells;
+  *bottom_max_cells = plume::g_bottom_max_cells;
+  *bottom_kind = plume::g_bottom_kind;
   return PLUME_OK;
 }

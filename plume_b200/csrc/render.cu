@@ -38,21 +38,23 @@ __host__ __device__ __forceinline__ Dims brick_dims(const Dims& d) {
   return Dims{(d.n0 + BRICK - 1) / BRICK, (d.n1 + BRICK - 1) / BRICK, (d.n2 + BRICK - 1) / BRICK};
 }
 
-__global__ void k_brick_max(Dims d, const float* __restrict__ f, float* __restrict__ bricks) {
+template <class T>
+__global__ void k_brick_max(Dims d, const T* __restrict__ f, float* __restrict__ bricks) {
   const Dims b = brick_dims(d);
   const int bi = blockIdx.z, bj = blockIdx.y * blockDim.y + threadIdx.y, bk = blockIdx.x * blockDim.x + threadIdx.x;
   if (bj >= b.n1 || bk >= b.n2) return;
   float best = -3.0e38f;
   for (int i = bi * BRICK; i <= imin_(bi * BRICK + BRICK, d.n0 - 1); ++i)
     for (int j = bj * BRICK; j <= imin_(bj * BRICK + BRICK, d.n1 - 1); ++j)
-      for (int k = bk * BRICK; k <= imin_(bk * BRICK + BRICK, d.n2 - 1); ++k) best = fmaxf(best, __ldg(f + at(d, i, j, k)));
+      for (int k = bk * BRICK; k <= imin_(bk * BRICK + BRICK, d.n2 - 1); ++k) best = fmaxf(best, ldg_f(f + at(d, i, j, k)));
   bricks[at(b, bi, bj, bk)] = best;
 }
 
 // light_volume_kernel (light_volume.py:18-33): one thread per cell marches toward the light in at most
 // half-cell steps to the box edge and writes exp(-opacity * column * cell_m). With `bricks`, samples whose
 // corners are all <= 0 are skipped (they add exactly 0).
-__global__ void k_light_volume(Dims d, const float* __restrict__ smoke, F3 toward, float cell_m, float opacity,
+template <class T>
+__global__ void k_light_volume(Dims d, const T* __restrict__ smoke, F3 toward, float cell_m, float opacity,
                                float* __restrict__ light, const float* __restrict__ bricks) {
   const int i = blockIdx.z, j = blockIdx.y * blockDim.y + threadIdx.y, k = blockIdx.x * blockDim.x + threadIdx.x;
   if (j >= d.n1 || k >= d.n2) return;
@@ -85,7 +87,8 @@ __global__ void k_light_volume(Dims d, const float* __restrict__ smoke, F3 towar
 constexpr int MAX_BLUR_TAPS = 129;
 __constant__ float c_weights[MAX_BLUR_TAPS];
 
-__global__ void k_blur_axis(Dims d, const float* __restrict__ src, float* __restrict__ dst, int radius, int axis) {
+template <class T>
+__global__ void k_blur_axis(Dims d, const T* __restrict__ src, float* __restrict__ dst, int radius, int axis) {
   const int i = blockIdx.z, j = blockIdx.y * blockDim.y + threadIdx.y, k = blockIdx.x * blockDim.x + threadIdx.x;
   if (j >= d.n1 || k >= d.n2) return;
   const int cell[3] = {i, j, k};
@@ -94,7 +97,7 @@ __global__ void k_blur_axis(Dims d, const float* __restrict__ src, float* __rest
   for (int o = -radius; o <= radius; ++o) {
     int c[3] = {i, j, k};
     c[axis] = imin_(imax_(cell[axis] + o, 0), n[axis] - 1);
-    total = total + c_weights[o + radius] * __ldg(src + at(d, c[0], c[1], c[2]));
+    total = total + c_weights[o + radius] * ldg_f(src + at(d, c[0], c[1], c[2]));
   }
   dst[at(d, i, j, k)] = total;
 }
@@ -149,7 +152,8 @@ struct MarchArgs {
 // with no smoke at a sample (all eight corners <= 0 in the brick map, or a blend <= 0) alpha is exactly 0, so
 // the exp, the light or gradient sample and the transmittance update are skipped (they would add +0 or
 // multiply by 1); with no glow the pow is skipped (it would add +0). Every result bit is unchanged.
-__global__ void k_raymarch(MarchArgs a, const float* __restrict__ smoke, const float* __restrict__ temperature,
+template <class T>
+__global__ void k_raymarch(MarchArgs a, const T* __restrict__ smoke, const T* __restrict__ temperature,
                            const float* __restrict__ gradient, const float* __restrict__ light, float* __restrict__ image,
                            int height, int width, const float* __restrict__ bricks) {
   const int px = blockIdx.x * blockDim.x + threadIdx.x, py = blockIdx.y * blockDim.y + threadIdx.y;
@@ -244,24 +248,83 @@ extern "C" long long plume_brick_floats(const int32_t shape[3]) {
   return (long long)b.n0 * b.n1 * b.n2;
 }
 
-extern "C" int plume_light_volume(const int32_t shape[3], const float* smoke, const float toward_light[3], float cell_m,
-                                  float opacity_per_density, float* light, float* bricks, void* stream) {
-  if (!valid_shape(shape) || !smoke || !toward_light || !light) return fail(PLUME_ERR_INVALID, "light_volume: bad argument");
-  Dims d{shape[0], shape[1], shape[2]};
-  cudaStream_t st = as_stream(stream);
+namespace plume {
+
+template <class T>
+static int light_volume(const Dims& d, const T* smoke, F3 toward, float cell_m, float opacity, float* light,
+                        float* bricks, cudaStream_t st) {
   if (bricks) {
     const Dims b = brick_dims(d);
-    k_brick_max<<<cell_grid(b.n0, b.n1, b.n2), cell_block(), 0, st>>>(d, smoke, bricks);
+    k_brick_max<T><<<cell_grid(b.n0, b.n1, b.n2), cell_block(), 0, st>>>(d, smoke, bricks);
     int status = launch_status("smoke brick map");
     if (status != PLUME_OK) return status;
   }
-  k_light_volume<<<cell_grid(d.n0, d.n1, d.n2), cell_block(), 0, st>>>(
-      d, smoke, f3(toward_light[0], toward_light[1], toward_light[2]), cell_m, opacity_per_density, light, bricks);
+  k_light_volume<T><<<cell_grid(d.n0, d.n1, d.n2), cell_block(), 0, st>>>(d, smoke, toward, cell_m, opacity, light,
+                                                                          bricks);
   return launch_status("light volume");
 }
 
-extern "C" int plume_normal_field(const int32_t shape[3], const float* smoke, float* blurred, float* scratch,
-                                  float* gradient, const float* weights_host, int32_t radius, void* stream) {
+template <class T>
+static int normal_field(const Dims& d, const T* smoke, float* blurred, float* scratch, float* gradient, int radius,
+                        cudaStream_t st) {
+  k_blur_axis<T><<<cell_grid(d.n0, d.n1, d.n2), cell_block(), 0, st>>>(d, smoke, blurred, radius, 0);
+  int status = launch_status("blur");
+  if (status != PLUME_OK) return status;
+  k_blur_axis<float><<<cell_grid(d.n0, d.n1, d.n2), cell_block(), 0, st>>>(d, blurred, scratch, radius, 1);
+  if ((status = launch_status("blur")) != PLUME_OK) return status;
+  k_blur_axis<float><<<cell_grid(d.n0, d.n1, d.n2), cell_block(), 0, st>>>(d, scratch, blurred, radius, 2);
+  if ((status = launch_status("blur")) != PLUME_OK) return status;
+  k_gradient<<<cell_grid(d.n0, d.n1, d.n2), cell_block(), 0, st>>>(d, blurred, gradient);
+  return launch_status("gradient");
+}
+
+template <class T>
+static int brick_max(const Dims& d, const T* field, float* bricks, cudaStream_t st) {
+  const Dims b = brick_dims(d);
+  k_brick_max<T><<<cell_grid(b.n0, b.n1, b.n2), cell_block(), 0, st>>>(d, field, bricks);
+  return launch_status("brick map");
+}
+
+template <class T>
+static int raymarch(const MarchArgs& a, const T* smoke, const T* temperature, const float* gradient, const float* light,
+                    float* image, int height, int width, float* bricks, cudaStream_t st) {
+  if (bricks) {  // the brick map of exactly the smoke being marched
+    int status = brick_max<T>(a.d, smoke, bricks, st);
+    if (status != PLUME_OK) return status;
+  }
+  dim3 block(16, 16), grid((width + 15) / 16, (height + 15) / 16);
+  k_raymarch<T><<<grid, block, 0, st>>>(a, smoke, temperature, gradient, light, image, height, width, bricks);
+  return launch_status("raymarch");
+}
+
+// Returns the call for the storage code (its arrays of float, bfloat16 or half).
+#define PLUME_BY_STORAGE(storage, call_f32, call_bf16, call_f16, what) \
+  switch (storage) {                                                 \
+    case PLUME_STORAGE_F32: return call_f32;                           \
+    case PLUME_STORAGE_BF16: return call_bf16;                         \
+    case PLUME_STORAGE_F16: return call_f16;                           \
+  }                                                                    \
+  return fail(PLUME_ERR_INVALID, "%s: storage %d", what, storage);
+
+}  // namespace plume
+
+extern "C" int plume_light_volume(const int32_t shape[3], const void* smoke, int32_t storage, const float toward_light[3],
+                                  float cell_m, float opacity_per_density, float* light, float* bricks, void* stream) {
+  if (!valid_shape(shape) || !smoke || !toward_light || !light) return fail(PLUME_ERR_INVALID, "light_volume: bad argument");
+  const Dims d{shape[0], shape[1], shape[2]};
+  const F3 toward = f3(toward_light[0], toward_light[1], toward_light[2]);
+  cudaStream_t st = as_stream(stream);
+  PLUME_BY_STORAGE(storage,
+                   light_volume(d, static_cast<const float*>(smoke), toward, cell_m, opacity_per_density, light, bricks, st),
+                   light_volume(d, static_cast<const __nv_bfloat16*>(smoke), toward, cell_m, opacity_per_density, light,
+                                bricks, st),
+                   light_volume(d, static_cast<const __half*>(smoke), toward, cell_m, opacity_per_density, light, bricks, st),
+                   "light_volume")
+}
+
+extern "C" int plume_normal_field(const int32_t shape[3], const void* smoke, int32_t storage, float* blurred,
+                                  float* scratch, float* gradient, const float* weights_host, int32_t radius,
+                                  void* stream) {
   if (!valid_shape(shape) || !smoke || !blurred || !scratch || !gradient || !weights_host || radius < 0 ||
       2 * radius + 1 > MAX_BLUR_TAPS)
     return fail(PLUME_ERR_INVALID, "normal_field: bad argument");
@@ -269,28 +332,23 @@ extern "C" int plume_normal_field(const int32_t shape[3], const float* smoke, fl
   int weights = runtime_status("blur weights", cudaMemcpyToSymbolAsync(c_weights, weights_host, sizeof(float) * (2 * radius + 1),
                                                                       0, cudaMemcpyHostToDevice, st));
   if (weights != PLUME_OK) return weights;
-  Dims d{shape[0], shape[1], shape[2]};
-  const float* source = smoke;
-  float* targets[3] = {blurred, scratch, blurred};
-  for (int axis = 0; axis < 3; ++axis) {
-    k_blur_axis<<<cell_grid(d.n0, d.n1, d.n2), cell_block(), 0, st>>>(d, source, targets[axis], radius, axis);
-    int status = launch_status("blur");
-    if (status != PLUME_OK) return status;
-    source = targets[axis];
-  }
-  k_gradient<<<cell_grid(d.n0, d.n1, d.n2), cell_block(), 0, st>>>(d, source, gradient);
-  return launch_status("gradient");
+  const Dims d{shape[0], shape[1], shape[2]};
+  PLUME_BY_STORAGE(storage, normal_field(d, static_cast<const float*>(smoke), blurred, scratch, gradient, radius, st),
+                   normal_field(d, static_cast<const __nv_bfloat16*>(smoke), blurred, scratch, gradient, radius, st),
+                   normal_field(d, static_cast<const __half*>(smoke), blurred, scratch, gradient, radius, st),
+                   "normal_field")
 }
 
-extern "C" int plume_brick_max(const int32_t shape[3], const float* field, float* bricks, void* stream) {
+extern "C" int plume_brick_max(const int32_t shape[3], const void* field, int32_t storage, float* bricks, void* stream) {
   if (!valid_shape(shape) || !field || !bricks) return fail(PLUME_ERR_INVALID, "brick_max: bad argument");
   const Dims d{shape[0], shape[1], shape[2]};
-  const Dims b = brick_dims(d);
-  k_brick_max<<<cell_grid(b.n0, b.n1, b.n2), cell_block(), 0, as_stream(stream)>>>(d, field, bricks);
-  return launch_status("brick map");
+  cudaStream_t st = as_stream(stream);
+  PLUME_BY_STORAGE(storage, brick_max(d, static_cast<const float*>(field), bricks, st),
+                   brick_max(d, static_cast<const __nv_bfloat16*>(field), bricks, st),
+                   brick_max(d, static_cast<const __half*>(field), bricks, st), "brick_max")
 }
 
-extern "C" int plume_raymarch(const PlumeGridInfo* info, const float* smoke, const float* temperature,
+extern "C" int plume_raymarch(const PlumeGridInfo* info, const void* smoke, const void* temperature, int32_t storage,
                               const float* gradient, const int32_t gradient_shape[3], const float* light,
                               const int32_t light_shape[3], const PlumeViewParams* view, const PlumeLookParams* look,
                               float* image, int32_t height, int32_t width, float* bricks, void* stream) {
@@ -305,13 +363,12 @@ extern "C" int plume_raymarch(const PlumeGridInfo* info, const float* smoke, con
   a.dg = Dims{gradient_shape[0], gradient_shape[1], gradient_shape[2]};
   a.dl = Dims{light_shape[0], light_shape[1], light_shape[2]};
   cudaStream_t st = as_stream(stream);
-  if (bricks) {  // the brick map of exactly the smoke being marched
-    const Dims b = brick_dims(a.d);
-    k_brick_max<<<cell_grid(b.n0, b.n1, b.n2), cell_block(), 0, st>>>(a.d, smoke, bricks);
-    int status = launch_status("smoke brick map");
-    if (status != PLUME_OK) return status;
-  }
-  dim3 block(16, 16), grid((width + 15) / 16, (height + 15) / 16);
-  k_raymarch<<<grid, block, 0, st>>>(a, smoke, temperature, gradient, light, image, height, width, bricks);
-  return launch_status("raymarch");
+  PLUME_BY_STORAGE(storage,
+                   raymarch(a, static_cast<const float*>(smoke), static_cast<const float*>(temperature), gradient, light,
+                            image, height, width, bricks, st),
+                   raymarch(a, static_cast<const __nv_bfloat16*>(smoke), static_cast<const __nv_bfloat16*>(temperature),
+                            gradient, light, image, height, width, bricks, st),
+                   raymarch(a, static_cast<const __half*>(smoke), static_cast<const __half*>(temperature), gradient,
+                            light, image, height, width, bricks, st),
+                   "raymarch")
 }

@@ -108,9 +108,10 @@ __device__ __forceinline__ F3 world_position(const PlumeGridInfo& info, F3 index
 // three face arrays, within a box of cells (`lo`, `n`) that contains every cell and face an active emitter can
 // cover (coverage is 0 outside each emitter's reach). blockIdx.z segments: n[0] cell slices, then n[0]+1 u
 // slices, n[0] v slices, n[0] w slices.
-__global__ void k_emit(PlumeGridInfo info, float* __restrict__ smoke, float* __restrict__ temperature,
-                       float* __restrict__ u, float* __restrict__ v, float* __restrict__ w, EmitterSet set, int seed,
-                       float time_s, float dt, int3 lo, int3 n) {
+template <class T>
+__global__ void k_emit(PlumeGridInfo info, T* __restrict__ smoke, T* __restrict__ temperature, T* __restrict__ u,
+                       T* __restrict__ v, T* __restrict__ w, EmitterSet set, int seed, float time_s, float dt, int3 lo,
+                       int3 n) {
   const int nx = info.dims[0], ny = info.dims[1], nz = info.dims[2];
   int slab = blockIdx.z;
   int part = 0;
@@ -129,14 +130,14 @@ __global__ void k_emit(PlumeGridInfo info, float* __restrict__ smoke, float* __r
       if (!(time_s >= e.start_s && time_s < e.end_s)) continue;
       float amount = coverage(e, x, seed);
       if (amount > 0.0f) {
-        smoke[c] = smoke[c] + e.smoke_per_s * amount * dt;
-        temperature[c] = lerpf_(temperature[c], e.temperature_k, blend_factor(amount, dt));
+        st_f(smoke + c, ld_f(smoke + c) + e.smoke_per_s * amount * dt);
+        st_f(temperature + c, lerpf_(ld_f(temperature + c), e.temperature_k, blend_factor(amount, dt)));
       }
     }
     return;
   }
   const int axis = part - 1;
-  float* comp = axis == 0 ? u : (axis == 1 ? v : w);
+  T* comp = axis == 0 ? u : (axis == 1 ? v : w);
   const int n0 = nx + (axis == 0), n1 = ny + (axis == 1), n2 = nz + (axis == 2);
   if (i >= n0 || j >= n1 || k >= n2 || j > lo.y + n.y || k > lo.z + n.z) return;
   F3 offset = axis == 0 ? f3(0.0f, 0.5f, 0.5f) : (axis == 1 ? f3(0.5f, 0.0f, 0.5f) : f3(0.5f, 0.5f, 0.0f));
@@ -152,7 +153,7 @@ __global__ void k_emit(PlumeGridInfo info, float* __restrict__ smoke, float* __r
         F3 away = sub3(x, v3(e.center_m));
         if (len3(away) > 0.0f) target = mul3(normalize3(away), len3(v3(e.velocity_mps)));
       }
-      comp[c] = lerpf_(comp[c], target[axis], blend_factor(amount, dt));
+      st_f(comp + c, lerpf_(ld_f(comp + c), target[axis], blend_factor(amount, dt)));
     }
   }
 }
@@ -180,7 +181,8 @@ static bool emitter_box(const PlumeGridInfo& info, const PlumeEmitter* e, int co
   return true;
 }
 
-static int launch_emit(const PlumeGridInfo& info, float* smoke, float* temperature, float* u, float* v, float* w,
+template <class T>
+static int launch_emit(const PlumeGridInfo& info, T* smoke, T* temperature, T* u, T* v, T* w,
                        const PlumeEmitter* emitters, int count, int seed, float time_s, float dt, cudaStream_t st) {
   // Emitters inactive at time_s change nothing; skip them on the host (the kernel re-checks).
   std::vector<PlumeEmitter> active;
@@ -202,30 +204,33 @@ static int launch_emit(const PlumeGridInfo& info, float* smoke, float* temperatu
 }
 
 // ---- buoyancy: forces.py:13-23 -----------------------------------------------------------------------------
-__global__ void k_buoyancy(PlumeGridInfo info, float* __restrict__ v, const float* __restrict__ smoke,
-                           const float* __restrict__ temperature, float gravity, float heat_buoyancy,
-                           float smoke_weight, float ambient, float dt) {
+template <class T>
+__global__ void k_buoyancy(PlumeGridInfo info, T* __restrict__ v, const T* __restrict__ smoke,
+                           const T* __restrict__ temperature, float gravity, float heat_buoyancy, float smoke_weight,
+                           float ambient, float dt) {
   const int ny = info.dims[1], nz = info.dims[2];
   const int i = blockIdx.z, j = blockIdx.y * blockDim.y + threadIdx.y, k = blockIdx.x * blockDim.x + threadIdx.x;
   if (j > ny || k >= nz) return;
   const int below = imax_(j - 1, 0), above = imin_(j, ny - 1);
   const int cb = (i * ny + below) * nz + k, ca = (i * ny + above) * nz + k;
-  float heat = 0.5f * (temperature[cb] + temperature[ca]);
-  float density = 0.5f * (smoke[cb] + smoke[ca]);
+  float heat = 0.5f * (ldg_f(temperature + cb) + ldg_f(temperature + ca));
+  float density = 0.5f * (ldg_f(smoke + cb) + ldg_f(smoke + ca));
   float lift = heat_buoyancy * (heat - ambient) / ambient - smoke_weight * density;
   const int c = (i * (ny + 1) + j) * nz + k;
-  v[c] = v[c] + gravity * lift * dt;
+  st_f(v + c, ld_f(v + c) + gravity * lift * dt);
 }
 
 // ---- vorticity confinement: vorticity.py:17-84 -------------------------------------------------------------
-__device__ __forceinline__ F3 center_velocity(const Vel& vel, int i, int j, int k) {  // vorticity.py:17-22
-  return f3(0.5f * (__ldg(vel.u + at(vel.du, i, j, k)) + __ldg(vel.u + at(vel.du, i + 1, j, k))),
-            0.5f * (__ldg(vel.v + at(vel.dv, i, j, k)) + __ldg(vel.v + at(vel.dv, i, j + 1, k))),
-            0.5f * (__ldg(vel.w + at(vel.dw, i, j, k)) + __ldg(vel.w + at(vel.dw, i, j, k + 1))));
+template <class T>
+__device__ __forceinline__ F3 center_velocity(const VelT<T>& vel, int i, int j, int k) {  // vorticity.py:17-22
+  return f3(0.5f * (ldg_f(vel.u + at(vel.du, i, j, k)) + ldg_f(vel.u + at(vel.du, i + 1, j, k))),
+            0.5f * (ldg_f(vel.v + at(vel.dv, i, j, k)) + ldg_f(vel.v + at(vel.dv, i, j + 1, k))),
+            0.5f * (ldg_f(vel.w + at(vel.dw, i, j, k)) + ldg_f(vel.w + at(vel.dw, i, j, k + 1))));
 }
 
 // curl_kernel (vorticity.py:38-45) with the centre velocities of center_velocity_kernel computed in place.
-__global__ void k_curl(PlumeGridInfo info, Vel vel, float* __restrict__ cx, float* __restrict__ cy,
+template <class T>
+__global__ void k_curl(PlumeGridInfo info, VelT<T> vel, float* __restrict__ cx, float* __restrict__ cy,
                        float* __restrict__ cz) {
   const int nx = info.dims[0], ny = info.dims[1], nz = info.dims[2];
   const int i = blockIdx.z, j = blockIdx.y * blockDim.y + threadIdx.y, k = blockIdx.x * blockDim.x + threadIdx.x;
@@ -318,12 +323,12 @@ struct FaceForces {
 
 // One pass over the three face arrays applying, per face and in the reference's order, the confinement push,
 // the turbulence push and drag. blockIdx.z segments: nx+1 u slices, nx v slices, nx w slices.
-template <int AXIS>
-__device__ __forceinline__ void face_forces_at(const PlumeGridInfo& info, float* __restrict__ f, int i, int j, int k,
+template <int AXIS, class T>
+__device__ __forceinline__ void face_forces_at(const PlumeGridInfo& info, T* __restrict__ f, int i, int j, int k,
                                                int n1, int n2, const FaceForces& ff) {
   const int nx = info.dims[0], ny = info.dims[1], nz = info.dims[2];
   const int c = (i * n1 + j) * n2 + k;
-  float value = f[c];
+  float value = ld_f(f + c);
   if (ff.confinement) {
     const int index = AXIS == 0 ? i : (AXIS == 1 ? j : k);
     const int lo = imax_(index - 1, 0), hi = imin_(index, info.dims[AXIS] - 1);
@@ -349,11 +354,12 @@ __device__ __forceinline__ void face_forces_at(const PlumeGridInfo& info, float*
     value = value + ff.strength * curl * ff.dt;
   }
   if (ff.drag) value = ff.wind[AXIS] + (value - ff.wind[AXIS]) * ff.keep;
-  f[c] = value;
+  st_f(f + c, value);
 }
 
-__global__ void k_face_forces(PlumeGridInfo info, float* __restrict__ u, float* __restrict__ v,
-                              float* __restrict__ w, FaceForces ff) {
+template <class T>
+__global__ void k_face_forces(PlumeGridInfo info, T* __restrict__ u, T* __restrict__ v, T* __restrict__ w,
+                              FaceForces ff) {
   const int nx = info.dims[0], ny = info.dims[1], nz = info.dims[2];
   int slab = blockIdx.z, axis = 0;
   if (slab >= nx + 1) { slab -= nx + 1; axis = 1; }
@@ -371,11 +377,12 @@ static dim3 face_grid(const PlumeGridInfo& info) {
   return dim3((nz + 1 + TZ - 1) / TZ, (ny + 1 + TY - 1) / TY, (nx + 1) + nx + nx);
 }
 
-static int launch_confinement_push(const PlumeGridInfo& info, const float* u, const float* v, const float* w,
+template <class T>
+static int launch_confinement_push(const PlumeGridInfo& info, const T* u, const T* v, const T* w,
                                    float* const curl[3], float* const push[3], float strength, int apply,
                                    cudaStream_t st) {
   const int nx = info.dims[0], ny = info.dims[1], nz = info.dims[2];
-  Vel vel = make_vel(u, v, w, info.dims);
+  VelT<T> vel = make_vel(u, v, w, info.dims);
   k_curl<<<cell_grid(nx, ny, nz), cell_block(), 0, st>>>(info, vel, curl[0], curl[1], curl[2]);
   CHECK_LAUNCH("curl");
   if (!apply) return PLUME_OK;
@@ -393,13 +400,15 @@ static int launch_confinement_push(const PlumeGridInfo& info, const float* u, co
 // that first sample, and fields with the same positions (smoke and temperature) share whole traces.
 
 // Up to two fields sampled at the same positions (same shape and offset, e.g. smoke and temperature).
-// `range`, when set, holds per element the (lo, hi) clamp bounds the forward pass found (2 floats), so the
-// correction does not trace forward again.
+// `range`, when set, holds per element the (lo, hi) clamp bounds the forward pass found (two values of the
+// storage type: the bounds are stored values, so they keep every bit), so the correction does not trace
+// forward a second time.
+template <class T>
 struct FieldDesc {
-  const float* data[2];
-  float* hat[2];
-  float* next[2];
-  float2* range[2];
+  const T* data[2];
+  T* hat[2];
+  T* next[2];
+  pair_t<T>* range[2];
   float outside[2];
   int fields;
   Dims d;
@@ -408,12 +417,14 @@ struct FieldDesc {
 };
 
 // Up to three groups (the three velocity components) in one launch (blockIdx.z segments).
+template <class T>
 struct FieldSet {
-  FieldDesc f[3];
+  FieldDesc<T> f[3];
   int count;
 };
 
-__device__ __forceinline__ int pick_field(const FieldSet& set, int& slab) {
+template <class T>
+__device__ __forceinline__ int pick_field(const FieldSet<T>& set, int& slab) {
   int which = 0;
   while (which + 1 < set.count && slab >= set.f[which].d.n0) {
     slab -= set.f[which].d.n0;
@@ -423,7 +434,8 @@ __device__ __forceinline__ int pick_field(const FieldSet& set, int& slab) {
 }
 
 // Trilinear sample that skips the corners whose weight is exactly 0 (sample.py:10-29 otherwise unchanged).
-__device__ __forceinline__ float sample_sparse(const float* __restrict__ f, const Dims& d, F3 g) {
+template <class T>
+__device__ __forceinline__ float sample_sparse(const T* __restrict__ f, const Dims& d, F3 g) {
   float x = clampf_(g[0], 0.0f, (float)(d.n0 - 1));
   float y = clampf_(g[1], 0.0f, (float)(d.n1 - 1));
   float z = clampf_(g[2], 0.0f, (float)(d.n2 - 1));
@@ -431,8 +443,8 @@ __device__ __forceinline__ float sample_sparse(const float* __restrict__ f, cons
   const int i1 = imin_(i0 + 1, d.n0 - 1), j1 = imin_(j0 + 1, d.n1 - 1), k1 = imin_(k0 + 1, d.n2 - 1);
   const float tx = x - (float)i0, ty = y - (float)j0, tz = z - (float)k0;
   auto along_x = [&](int j, int k) {
-    const float a = __ldg(f + at(d, i0, j, k));
-    return tx == 0.0f ? a : lerpf_(a, __ldg(f + at(d, i1, j, k)), tx);
+    const float a = ldg_f(f + at(d, i0, j, k));
+    return tx == 0.0f ? a : lerpf_(a, ldg_f(f + at(d, i1, j, k)), tx);
   };
   const float c00 = along_x(j0, k0);
   const float y0 = ty == 0.0f ? c00 : lerpf_(c00, along_x(j1, k0), ty);
@@ -442,23 +454,26 @@ __device__ __forceinline__ float sample_sparse(const float* __restrict__ f, cons
   return lerpf_(y0, y1, tz);
 }
 
-__device__ __forceinline__ F3 velocity_at_node(const Vel& vel, F3 p) {  // velocity_at (sample.py:74-82) at p
+template <class T>
+__device__ __forceinline__ F3 velocity_at_node(const VelT<T>& vel, F3 p) {  // velocity_at (sample.py:74-82) at p
   return f3(sample_sparse(vel.u, vel.du, sub3(p, f3(0.0f, 0.5f, 0.5f))),
             sample_sparse(vel.v, vel.dv, sub3(p, f3(0.5f, 0.0f, 0.5f))),
             sample_sparse(vel.w, vel.dw, sub3(p, f3(0.5f, 0.5f, 0.0f))));
 }
 
 // trace (advect.py:16-21) given the velocity at p.
-__device__ __forceinline__ F3 trace_from(const Vel& vel, F3 p, F3 vp, float dt_over_cell) {
+template <class T>
+__device__ __forceinline__ F3 trace_from(const VelT<T>& vel, F3 p, F3 vp, float dt_over_cell) {
   F3 mid = sub3(p, mul3(vp, 0.5f * dt_over_cell));
   return sub3(p, mul3(velocity_at(vel, mid), dt_over_cell));
 }
 
 // semi_lagrangian_kernel (advect.py:24-31): the forward pass into `hat` (or, for plain semi-Lagrangian
 // advection, into `next`).
-__global__ void k_advect_forward(PlumeGridInfo info, Vel vel, FieldSet set, float dt_over_cell, int write_next) {
+template <class T>
+__global__ void k_advect_forward(PlumeGridInfo info, VelT<T> vel, FieldSet<T> set, float dt_over_cell, int write_next) {
   int slab = blockIdx.z;
-  const FieldDesc& fd = set.f[pick_field(set, slab)];
+  const FieldDesc<T>& fd = set.f[pick_field(set, slab)];
   const int i = slab, j = blockIdx.y * blockDim.y + threadIdx.y, k = blockIdx.x * blockDim.x + threadIdx.x;
   if (j >= fd.d.n1 || k >= fd.d.n2) return;
   const int c = at(fd.d, i, j, k);
@@ -469,18 +484,18 @@ __global__ void k_advect_forward(PlumeGridInfo info, Vel vel, FieldSet set, floa
   for (int n = 0; n < fd.fields; ++n) {
     float value = fd.outside[n], lo = fd.outside[n], hi = fd.outside[n];
     if (!outside) value = sample_with_range(fd.data[n], fd.d, g, lo, hi);
-    (write_next ? fd.next[n] : fd.hat[n])[c] = value;
-    if (fd.range[n]) fd.range[n][c] = make_float2(lo, hi);
+    st_f((write_next ? fd.next[n] : fd.hat[n]) + c, value);
+    if (fd.range[n]) fd.range[n][c] = make_pair_t<T>(lo, hi);
   }
 }
 
 // maccormack_correct_kernel (advect.py:34-50) with the backward pass (advect.py:64) evaluated in place:
 // back = sample(hat, trace(p, -dt)), corrected = hat + (data - back) / 2, clamped to the range of the eight
 // values the forward sample blended.
-template <bool STORED_RANGE>
-__global__ void k_advect_correct(PlumeGridInfo info, Vel vel, FieldSet set, float dt_over_cell) {
+template <class T, bool STORED_RANGE>
+__global__ void k_advect_correct(PlumeGridInfo info, VelT<T> vel, FieldSet<T> set, float dt_over_cell) {
   int slab = blockIdx.z;
-  const FieldDesc& fd = set.f[pick_field(set, slab)];
+  const FieldDesc<T>& fd = set.f[pick_field(set, slab)];
   const int i = slab, j = blockIdx.y * blockDim.y + threadIdx.y, k = blockIdx.x * blockDim.x + threadIdx.x;
   if (j >= fd.d.n1 || k >= fd.d.n2) return;
   const int c = at(fd.d, i, j, k);
@@ -498,20 +513,21 @@ __global__ void k_advect_correct(PlumeGridInfo info, Vel vel, FieldSet set, floa
   }
   for (int n = 0; n < fd.fields; ++n) {
     const float back = back_outside ? fd.outside[n] : sample_index_space(fd.hat[n], fd.d, gb);
-    const float corrected = __ldg(fd.hat[n] + c) + 0.5f * (__ldg(fd.data[n] + c) - back);
+    const float corrected = ldg_f(fd.hat[n] + c) + 0.5f * (ldg_f(fd.data[n] + c) - back);
     float lo = fd.outside[n], hi = fd.outside[n];
     if (STORED_RANGE) {
-      const float2 r = __ldg(fd.range[n] + c);
-      lo = r.x;
-      hi = r.y;
+      const pair_t<T> r = fd.range[n][c];
+      lo = to_f<T>(r.x);
+      hi = to_f<T>(r.y);
     } else if (!source_outside) {
       sample_with_range(fd.data[n], fd.d, gs, lo, hi);
     }
-    fd.next[n][c] = clampf_(corrected, lo, hi);
+    st_f(fd.next[n] + c, clampf_(corrected, lo, hi));
   }
 }
 
-static int launch_advect(const PlumeGridInfo& info, const Vel& vel, const FieldSet& set, float dt_over_cell,
+template <class T>
+static int launch_advect(const PlumeGridInfo& info, const VelT<T>& vel, const FieldSet<T>& set, float dt_over_cell,
                          bool maccormack, cudaStream_t st) {
   int slabs = 0, n1 = 0, n2 = 0;
   for (int n = 0; n < set.count; ++n) {
@@ -521,21 +537,21 @@ static int launch_advect(const PlumeGridInfo& info, const Vel& vel, const FieldS
   }
   dim3 grid((n2 + TZ - 1) / TZ, (n1 + TY - 1) / TY, slabs);
   if (!maccormack) {
-    k_advect_forward<<<grid, cell_block(), 0, st>>>(info, vel, set, dt_over_cell, 1);
+    k_advect_forward<T><<<grid, cell_block(), 0, st>>>(info, vel, set, dt_over_cell, 1);
     CHECK_LAUNCH("semi-Lagrangian advection");
     return PLUME_OK;
   }
-  k_advect_forward<<<grid, cell_block(), 0, st>>>(info, vel, set, dt_over_cell, 0);
+  k_advect_forward<T><<<grid, cell_block(), 0, st>>>(info, vel, set, dt_over_cell, 0);
   CHECK_LAUNCH("MacCormack forward pass");
-  if (set.f[0].range[0]) k_advect_correct<true><<<grid, cell_block(), 0, st>>>(info, vel, set, dt_over_cell);
-  else k_advect_correct<false><<<grid, cell_block(), 0, st>>>(info, vel, set, dt_over_cell);
+  if (set.f[0].range[0]) k_advect_correct<T, true><<<grid, cell_block(), 0, st>>>(info, vel, set, dt_over_cell);
+  else k_advect_correct<T, false><<<grid, cell_block(), 0, st>>>(info, vel, set, dt_over_cell);
   CHECK_LAUNCH("MacCormack correction");
   return PLUME_OK;
 }
 
-static FieldDesc single_field(const float* data, float* hat, float* next, Dims d, F3 offset, float outside,
-                              int uses_outside) {
-  FieldDesc f{};
+template <class T>
+static FieldDesc<T> single_field(const T* data, T* hat, T* next, Dims d, F3 offset, float outside, int uses_outside) {
+  FieldDesc<T> f{};
   f.data[0] = data;
   f.hat[0] = hat;
   f.next[0] = next;
@@ -550,7 +566,8 @@ static FieldDesc single_field(const float* data, float* hat, float* next, Dims d
 // ---- pressure: pressure.py ----------------------------------------------------------------------------------
 
 // zero_closed_faces_kernel (pressure.py:21-28) on the two boundary planes of each face array.
-__global__ void k_zero_walls(PlumeGridInfo info, float* __restrict__ u, float* __restrict__ v, float* __restrict__ w) {
+template <class T>
+__global__ void k_zero_walls(PlumeGridInfo info, T* __restrict__ u, T* __restrict__ v, T* __restrict__ w) {
   const int nx = info.dims[0], ny = info.dims[1], nz = info.dims[2];
   const int axis = blockIdx.z / 2, side = blockIdx.z % 2;
   const bool closed = side == 0 ? info.open_lo[axis] == 0 : info.open_hi[axis] == 0;
@@ -558,28 +575,29 @@ __global__ void k_zero_walls(PlumeGridInfo info, float* __restrict__ u, float* _
   const int a = blockIdx.y * blockDim.y + threadIdx.y, b = blockIdx.x * blockDim.x + threadIdx.x;
   const int plane = side == 0 ? 0 : info.dims[axis];
   if (axis == 0) {
-    if (a < ny && b < nz) u[(plane * ny + a) * nz + b] = 0.0f;
+    if (a < ny && b < nz) st_f(u + (plane * ny + a) * nz + b, 0.0f);
   } else if (axis == 1) {
-    if (a < nx && b < nz) v[(a * (ny + 1) + plane) * nz + b] = 0.0f;
+    if (a < nx && b < nz) st_f(v + (a * (ny + 1) + plane) * nz + b, 0.0f);
   } else {
-    if (a < nx && b < ny) w[(a * ny + b) * (nz + 1) + plane] = 0.0f;
+    if (a < nx && b < ny) st_f(w + (a * ny + b) * (nz + 1) + plane, 0.0f);
   }
 }
 
-__global__ void k_divergence(PlumeGridInfo info, const float* __restrict__ u, const float* __restrict__ v,
-                             const float* __restrict__ w, float* __restrict__ div) {  // pressure.py:31-36
+template <class T>
+__global__ void k_divergence(PlumeGridInfo info, const T* __restrict__ u, const T* __restrict__ v,
+                             const T* __restrict__ w, float* __restrict__ div) {  // pressure.py:31-36
   const int ny = info.dims[1], nz = info.dims[2];
   const int i = blockIdx.z, j = blockIdx.y * blockDim.y + threadIdx.y, k = blockIdx.x * blockDim.x + threadIdx.x;
   if (j >= ny || k >= nz) return;
-  float flux = (__ldg(u + ((i + 1) * ny + j) * nz + k) - __ldg(u + (i * ny + j) * nz + k)) +
-               (__ldg(v + (i * (ny + 1) + j + 1) * nz + k) - __ldg(v + (i * (ny + 1) + j) * nz + k)) +
-               (__ldg(w + (i * ny + j) * (nz + 1) + k + 1) - __ldg(w + (i * ny + j) * (nz + 1) + k));
+  float flux = (ldg_f(u + ((i + 1) * ny + j) * nz + k) - ldg_f(u + (i * ny + j) * nz + k)) +
+               (ldg_f(v + (i * (ny + 1) + j + 1) * nz + k) - ldg_f(v + (i * (ny + 1) + j) * nz + k)) +
+               (ldg_f(w + (i * ny + j) * (nz + 1) + k + 1) - ldg_f(w + (i * ny + j) * (nz + 1) + k));
   div[(i * ny + j) * nz + k] = flux / info.cell_m;
 }
 
 // subtract_gradient_kernel (pressure.py:95-116) over the three face arrays (blockIdx.z segments).
-template <int AXIS>
-__device__ __forceinline__ void subtract_gradient_at(const PlumeGridInfo& info, float* __restrict__ f,
+template <int AXIS, class T>
+__device__ __forceinline__ void subtract_gradient_at(const PlumeGridInfo& info, T* __restrict__ f,
                                                      const float* __restrict__ q, int i, int j, int k, int n1, int n2) {
   const Dims d = dims_of(info);
   const int index = AXIS == 0 ? i : (AXIS == 1 ? j : k);
@@ -596,11 +614,12 @@ __device__ __forceinline__ void subtract_gradient_at(const PlumeGridInfo& info, 
     q_below = __ldg(q + below);
   }
   const int c = (i * n1 + j) * n2 + k;
-  f[c] = f[c] - (q_above - q_below) / info.cell_m;
+  st_f(f + c, ld_f(f + c) - (q_above - q_below) / info.cell_m);
 }
 
-__global__ void k_subtract_gradient(PlumeGridInfo info, float* __restrict__ u, float* __restrict__ v,
-                                    float* __restrict__ w, const float* __restrict__ q) {
+template <class T>
+__global__ void k_subtract_gradient(PlumeGridInfo info, T* __restrict__ u, T* __restrict__ v, T* __restrict__ w,
+                                    const float* __restrict__ q) {
   const int nx = info.dims[0], ny = info.dims[1], nz = info.dims[2];
   int slab = blockIdx.z, axis = 0;
   if (slab >= nx + 1) { slab -= nx + 1; axis = 1; }
@@ -631,16 +650,17 @@ __global__ void k_residual(PlumeGridInfo info, const float* __restrict__ q, cons
 // then the block partials in order on one thread. The CPU oracle adds in the same order.
 constexpr int SUM_BLOCK = 256;
 
-__global__ void k_line_partials(Dims d, const float* __restrict__ a, const float* __restrict__ b,
-                                const float* __restrict__ c, double* __restrict__ partial, int blocks) {
+template <class T>
+__global__ void k_line_partials(Dims d, const T* __restrict__ a, const T* __restrict__ b, const T* __restrict__ c,
+                                double* __restrict__ partial, int blocks) {
   __shared__ double slot[SUM_BLOCK];
-  const float* src = blockIdx.y == 0 ? a : (blockIdx.y == 1 ? b : c);
+  const T* src = blockIdx.y == 0 ? a : (blockIdx.y == 1 ? b : c);
   const long line = (long)blockIdx.x * SUM_BLOCK + threadIdx.x;
   const long lines = (long)d.n1 * d.n2;
   double value = 0.0;
   if (line < lines) {
     float total = 0.0f;
-    for (int i = 0; i < d.n0; ++i) total = total + __ldg(src + (long)i * lines + line);
+    for (int i = 0; i < d.n0; ++i) total = total + ldg_f(src + (long)i * lines + line);
     value = (double)total;
   }
   slot[threadIdx.x] = value;
@@ -673,18 +693,20 @@ __global__ void k_budget_factor(const double* __restrict__ partial, int blocks, 
   *factor = mc > 0.0 ? (float)(held / mc) : 1.0f;
 }
 
-__global__ void k_scale(float* __restrict__ f, long n, const float* __restrict__ factor) {  // conserve.py:27-30
+template <class T>
+__global__ void k_scale(T* __restrict__ f, long n, const float* __restrict__ factor) {  // conserve.py:27-30
   const float s = *factor;
   for (long idx = (long)blockIdx.x * blockDim.x + threadIdx.x; idx < n; idx += (long)gridDim.x * blockDim.x)
-    f[idx] = f[idx] * s;
+    st_f(f + idx, ld_f(f + idx) * s);
 }
 
 static int sum_blocks(const Dims& d) { return (int)(((long)d.n1 * d.n2 + SUM_BLOCK - 1) / SUM_BLOCK); }
 
-static int launch_triple_sum(const Dims& d, const float* a, const float* b, const float* c, double* sums,
-                             float* factor, double* totals_out, cudaStream_t st) {
+template <class T>
+static int launch_triple_sum(const Dims& d, const T* a, const T* b, const T* c, double* sums, float* factor,
+                             double* totals_out, cudaStream_t st) {
   const int blocks = sum_blocks(d);
-  k_line_partials<<<dim3(blocks, 3), SUM_BLOCK, 0, st>>>(d, a, b, c, sums, blocks);
+  k_line_partials<T><<<dim3(blocks, 3), SUM_BLOCK, 0, st>>>(d, a, b, c, sums, blocks);
   CHECK_LAUNCH("line sums");
   k_budget_factor<<<1, 32, 0, st>>>(sums, blocks, factor, totals_out, factor != nullptr);
   CHECK_LAUNCH("budget factor");
@@ -697,35 +719,40 @@ static int grid_stride_blocks(long n) {
 }
 
 // ---- the scalar epilogue: conserve scale + dissipation (conserve.py:50-52, dissipate.py:10-15) -------------
-__global__ void k_scalar_finish(float* __restrict__ smoke, float* __restrict__ temperature, long n,
+// With storage narrower than float, the conserve scale is rounded to storage before dissipation, as the
+// reference's separate passes do.
+template <class T>
+__global__ void k_scalar_finish(T* __restrict__ smoke, T* __restrict__ temperature, long n,
                                 const float* __restrict__ factor, int dissipate, float smoke_keep, float heat_keep,
                                 float ambient) {
   const float s = *factor;
   for (long idx = (long)blockIdx.x * blockDim.x + threadIdx.x; idx < n; idx += (long)gridDim.x * blockDim.x) {
-    float value = smoke[idx] * s;
+    float value = to_f<T>(from_f<T>(ld_f(smoke + idx) * s));
     if (dissipate) {
       value = value * smoke_keep;
-      temperature[idx] = ambient + (temperature[idx] - ambient) * heat_keep;
+      st_f(temperature + idx, ambient + (ld_f(temperature + idx) - ambient) * heat_keep);
     }
-    smoke[idx] = value;
+    st_f(smoke + idx, value);
   }
 }
 
-__global__ void k_dissipate(float* __restrict__ smoke, float* __restrict__ temperature, long n, float smoke_keep,
+template <class T>
+__global__ void k_dissipate(T* __restrict__ smoke, T* __restrict__ temperature, long n, float smoke_keep,
                             float heat_keep, float ambient) {  // dissipate.py:10-15
   for (long idx = (long)blockIdx.x * blockDim.x + threadIdx.x; idx < n; idx += (long)gridDim.x * blockDim.x) {
-    smoke[idx] = smoke[idx] * smoke_keep;
-    temperature[idx] = ambient + (temperature[idx] - ambient) * heat_keep;
+    st_f(smoke + idx, ld_f(smoke + idx) * smoke_keep);
+    st_f(temperature + idx, ambient + (ld_f(temperature + idx) - ambient) * heat_keep);
   }
 }
 
 // ---- grid speed: step_cap.py:50-55 (max is exact in any order) ----------------------------------------------
-__global__ void k_abs_max(const float* __restrict__ a, long na, const float* __restrict__ b, long nb,
-                          const float* __restrict__ c, long nc, unsigned int* __restrict__ out) {
+template <class T>
+__global__ void k_abs_max(const T* __restrict__ a, long na, const T* __restrict__ b, long nb, const T* __restrict__ c,
+                          long nc, unsigned int* __restrict__ out) {
   float best = 0.0f;
   const long total = na + nb + nc;
   for (long idx = (long)blockIdx.x * blockDim.x + threadIdx.x; idx < total; idx += (long)gridDim.x * blockDim.x) {
-    float value = idx < na ? __ldg(a + idx) : (idx < na + nb ? __ldg(b + idx - na) : __ldg(c + idx - na - nb));
+    float value = idx < na ? ldg_f(a + idx) : (idx < na + nb ? ldg_f(b + idx - na) : ldg_f(c + idx - na - nb));
     best = fmax_(best, fabsf(value));
   }
   for (int off = 16; off >= 1; off >>= 1) best = fmax_(best, __shfl_xor_sync(0xffffffffu, best, off));
@@ -748,10 +775,10 @@ extern "C" int plume_advect_semi_lagrangian(const PlumeGridInfo* info, const int
                                             int32_t uses_outside, void* stream) {
   CHECK_ARG(info && shape && src && dst && u && v && w && offset, "semi_lagrangian: null argument");
   CHECK_ARG(valid_dims(info->dims) && valid_dims(shape), "semi_lagrangian: bad dims");
-  FieldSet set{};
+  FieldSet<float> set{};
   set.count = 1;
-  set.f[0] = single_field(src, nullptr, dst, Dims{shape[0], shape[1], shape[2]}, f3(offset[0], offset[1], offset[2]),
-                          outside, uses_outside);
+  set.f[0] = single_field<float>(src, nullptr, dst, Dims{shape[0], shape[1], shape[2]},
+                                 f3(offset[0], offset[1], offset[2]), outside, uses_outside);
   return launch_advect(*info, make_vel(u, v, w, info->dims), set, dt_over_cell, false, as_stream(stream));
 }
 
@@ -761,10 +788,10 @@ extern "C" int plume_advect_maccormack(const PlumeGridInfo* info, const int32_t 
                                        void* stream) {
   CHECK_ARG(info && shape && data && hat && next && u && v && w && offset, "maccormack: null argument");
   CHECK_ARG(valid_dims(info->dims) && valid_dims(shape), "maccormack: bad dims");
-  FieldSet set{};
+  FieldSet<float> set{};
   set.count = 1;
-  set.f[0] = single_field(data, hat, next, Dims{shape[0], shape[1], shape[2]}, f3(offset[0], offset[1], offset[2]),
-                          outside, uses_outside);
+  set.f[0] = single_field<float>(data, hat, next, Dims{shape[0], shape[1], shape[2]},
+                                 f3(offset[0], offset[1], offset[2]), outside, uses_outside);
   return launch_advect(*info, make_vel(u, v, w, info->dims), set, dt_over_cell, true, as_stream(stream));
 }
 
@@ -844,15 +871,24 @@ extern "C" int plume_divergence(const PlumeGridInfo* info, const float* u, const
   return launch_status("divergence");
 }
 
+namespace plume {
+// zero_closed_faces_kernel x 3 + divergence_kernel (pressure.py:144-150).
+template <class T>
+static int project_begin(const PlumeGridInfo& info, T* u, T* v, T* w, float* divergence, cudaStream_t st) {
+  const int nx = info.dims[0], ny = info.dims[1], nz = info.dims[2];
+  const int m = std::max(nx, ny) + 1, n = std::max(ny, nz) + 1;
+  k_zero_walls<T><<<dim3((n + TZ - 1) / TZ, (m + TY - 1) / TY, 6), cell_block(), 0, st>>>(info, u, v, w);
+  CHECK_LAUNCH("zero closed faces");
+  k_divergence<T><<<cell_grid(nx, ny, nz), cell_block(), 0, st>>>(info, u, v, w, divergence);
+  return launch_status("divergence");
+}
+}  // namespace plume
+
 extern "C" int plume_project_begin(const PlumeGridInfo* info, float* u, float* v, float* w, float* divergence,
                                    void* stream) {
   CHECK_ARG(info && u && v && w && divergence, "project: null argument");
   CHECK_ARG(valid_dims(info->dims), "project: bad dims");
-  const int nx = info->dims[0], ny = info->dims[1], nz = info->dims[2];
-  const int m = std::max(nx, ny) + 1, n = std::max(ny, nz) + 1;
-  k_zero_walls<<<dim3((n + TZ - 1) / TZ, (m + TY - 1) / TY, 6), cell_block(), 0, as_stream(stream)>>>(*info, u, v, w);
-  CHECK_LAUNCH("zero closed faces");
-  return plume_divergence(info, u, v, w, divergence, stream);
+  return project_begin(*info, u, v, w, divergence, as_stream(stream));
 }
 
 extern "C" int plume_subtract_gradient(const PlumeGridInfo* info, float* u, float* v, float* w, const float* q,
@@ -930,34 +966,47 @@ extern "C" int plume_dissipate(const PlumeGridInfo* info, float* smoke, float* t
   return launch_status("dissipate");
 }
 
-extern "C" int plume_grid_speed(const PlumeGridInfo* info, const float* u, const float* v, const float* w,
+namespace plume {
+template <class T>
+static int grid_speed(const PlumeGridInfo& info, const void* u, const void* v, const void* w, float* speed,
+                      cudaStream_t st) {
+  const long nx = info.dims[0], ny = info.dims[1], nz = info.dims[2];
+  const long na = (nx + 1) * ny * nz, nb = nx * (ny + 1) * nz, nc = nx * ny * (nz + 1);
+  int status = runtime_status("grid speed reset", cudaMemsetAsync(speed, 0, sizeof(float), st));
+  if (status != PLUME_OK) return status;
+  k_abs_max<T><<<grid_stride_blocks(na + nb + nc), 256, 0, st>>>(static_cast<const T*>(u), na, static_cast<const T*>(v),
+                                                                 nb, static_cast<const T*>(w), nc,
+                                                                 reinterpret_cast<unsigned int*>(speed));
+  return launch_status("grid speed");
+}
+}  // namespace plume
+
+extern "C" int plume_grid_speed(const PlumeGridInfo* info, const void* u, const void* v, const void* w, int32_t storage,
                                 float* speed, void* stream) {
   CHECK_ARG(info && u && v && w && speed, "grid_speed: null argument");
   CHECK_ARG(valid_dims(info->dims), "grid_speed: bad dims");
   cudaStream_t st = as_stream(stream);
-  const long nx = info->dims[0], ny = info->dims[1], nz = info->dims[2];
-  const long na = (nx + 1) * ny * nz, nb = nx * (ny + 1) * nz, nc = nx * ny * (nz + 1);
-  int status = runtime_status("grid speed reset", cudaMemsetAsync(speed, 0, sizeof(float), st));
-  if (status != PLUME_OK) return status;
-  k_abs_max<<<grid_stride_blocks(na + nb + nc), 256, 0, st>>>(u, na, v, nb, w, nc, reinterpret_cast<unsigned int*>(speed));
-  return launch_status("grid speed");
+  switch (storage) {
+    case PLUME_STORAGE_F32: return grid_speed<float>(*info, u, v, w, speed, st);
+    case PLUME_STORAGE_BF16: return grid_speed<__nv_bfloat16>(*info, u, v, w, speed, st);
+    case PLUME_STORAGE_F16: return grid_speed<__half>(*info, u, v, w, speed, st);
+  }
+  return fail(PLUME_ERR_INVALID, "grid_speed: storage %d", storage);
 }
 
-extern "C" int plume_step(const PlumeStepState* s, const PlumeStepParams* p, void* stream) {
-  CHECK_ARG(s && p, "step: null argument");
-  CHECK_ARG(valid_dims(s->info.dims), "step: bad dims");
-  CHECK_ARG(s->u.data && s->u.hat && s->u.next && s->v.data && s->v.hat && s->v.next && s->w.data && s->w.hat &&
-                s->w.next && s->smoke.data && s->smoke.hat && s->smoke.next && s->temperature.data &&
-                s->temperature.hat && s->temperature.next && s->pressure && s->divergence && s->sums && s->factor,
-            "step: null buffer");
-  CHECK_ARG(s->levels && s->level_count >= 1 && s->levels[0].q == s->pressure && s->levels[0].rhs == s->divergence &&
-                s->levels[0].residual && s->levels[0].residual != s->pressure,
-            "step: levels must start at the grid's pressure and divergence, with a second pressure array");
-  CHECK_ARG(p->confinement == 0.0f || (s->curl[0] && s->curl[1] && s->curl[2] && s->push[0] && s->push[1] && s->push[2]),
-            "step: confinement scratch missing");
+namespace plume {
+
+// Stepper.step (stepper.py:28-44) with the fields stored as T.
+template <class T>
+static int step(const PlumeStepState* s, const PlumeStepParams* p, void* stream) {
   cudaStream_t st = as_stream(stream);
   const PlumeGridInfo& info = s->info;
   const int nx = info.dims[0], ny = info.dims[1], nz = info.dims[2];
+  T* const ud = static_cast<T*>(s->u.data);
+  T* const vd = static_cast<T*>(s->v.data);
+  T* const wd = static_cast<T*>(s->w.data);
+  T* const sd = static_cast<T*>(s->smoke.data);
+  T* const td = static_cast<T*>(s->temperature.data);
   int status;
   int phase = 0;
   auto mark = [&]() -> int {  // phase boundary event, when the caller asked for them
@@ -966,12 +1015,11 @@ extern "C" int plume_step(const PlumeStepState* s, const PlumeStepParams* p, voi
   };
   if ((status = mark()) != PLUME_OK) return status;
   // emit, buoyancy (stepper.py:32-34)
-  if ((status = launch_emit(info, s->smoke.data, s->temperature.data, s->u.data, s->v.data, s->w.data, p->emitters,
-                            p->emitter_count, p->seed, p->time_s, p->dt, st)) != PLUME_OK)
+  if ((status = launch_emit<T>(info, sd, td, ud, vd, wd, p->emitters, p->emitter_count, p->seed, p->time_s, p->dt,
+                               st)) != PLUME_OK)
     return status;
-  k_buoyancy<<<cell_grid(nx, ny + 1, nz), cell_block(), 0, st>>>(info, s->v.data, s->smoke.data, s->temperature.data,
-                                                                 p->gravity, p->heat_buoyancy, p->smoke_weight,
-                                                                 p->ambient_k, p->dt);
+  k_buoyancy<T><<<cell_grid(nx, ny + 1, nz), cell_block(), 0, st>>>(info, vd, sd, td, p->gravity, p->heat_buoyancy,
+                                                                    p->smoke_weight, p->ambient_k, p->dt);
   CHECK_LAUNCH("buoyancy");
   // confinement, turbulence, drag (stepper.py:35-40): one face pass after the push is known
   FaceForces ff{};
@@ -979,8 +1027,7 @@ extern "C" int plume_step(const PlumeStepState* s, const PlumeStepParams* p, voi
   if (p->confinement != 0.0f) {
     float* curl[3] = {s->curl[0], s->curl[1], s->curl[2]};
     float* push[3] = {s->push[0], s->push[1], s->push[2]};
-    if ((status = launch_confinement_push(info, s->u.data, s->v.data, s->w.data, curl, push, p->confinement, 1, st)) !=
-        PLUME_OK)
+    if ((status = launch_confinement_push<T>(info, ud, vd, wd, curl, push, p->confinement, 1, st)) != PLUME_OK)
       return status;
     ff.confinement = 1;
     ff.push[0] = s->push[0];
@@ -1002,33 +1049,36 @@ extern "C" int plume_step(const PlumeStepState* s, const PlumeStepParams* p, voi
     ff.keep = p->drag_keep;
   }
   if (ff.confinement || ff.turbulence || ff.drag) {
-    k_face_forces<<<face_grid(info), cell_block(), 0, st>>>(info, s->u.data, s->v.data, s->w.data, ff);
+    k_face_forces<T><<<face_grid(info), cell_block(), 0, st>>>(info, ud, vd, wd, ff);
     CHECK_LAUNCH("face forces");
   }
   if ((status = mark()) != PLUME_OK) return status;
   // advect velocity (stepper.py:46-52)
   {
-    FieldSet set{};
+    FieldSet<T> set{};
     set.count = 3;
-    set.f[0] = single_field(s->u.data, s->u.hat, s->u.next, Dims{nx + 1, ny, nz}, f3(0.0f, 0.5f, 0.5f), 0.0f, 0);
-    set.f[1] = single_field(s->v.data, s->v.hat, s->v.next, Dims{nx, ny + 1, nz}, f3(0.5f, 0.0f, 0.5f), 0.0f, 0);
-    set.f[2] = single_field(s->w.data, s->w.hat, s->w.next, Dims{nx, ny, nz + 1}, f3(0.5f, 0.5f, 0.0f), 0.0f, 0);
+    set.f[0] = single_field<T>(ud, static_cast<T*>(s->u.hat), static_cast<T*>(s->u.next), Dims{nx + 1, ny, nz},
+                               f3(0.0f, 0.5f, 0.5f), 0.0f, 0);
+    set.f[1] = single_field<T>(vd, static_cast<T*>(s->v.hat), static_cast<T*>(s->v.next), Dims{nx, ny + 1, nz},
+                               f3(0.5f, 0.0f, 0.5f), 0.0f, 0);
+    set.f[2] = single_field<T>(wd, static_cast<T*>(s->w.hat), static_cast<T*>(s->w.next), Dims{nx, ny, nz + 1},
+                               f3(0.5f, 0.5f, 0.0f), 0.0f, 0);
     if (s->advect_scratch) {  // clamp ranges: u's, v's, w's, back to back
-      float2* r = reinterpret_cast<float2*>(s->advect_scratch);
+      pair_t<T>* r = reinterpret_cast<pair_t<T>*>(s->advect_scratch);
       set.f[0].range[0] = r;
       set.f[1].range[0] = r + (size_t)(nx + 1) * ny * nz;
       set.f[2].range[0] = r + (size_t)(nx + 1) * ny * nz + (size_t)nx * (ny + 1) * nz;
     }
-    if ((status = launch_advect(info, make_vel(s->u.data, s->v.data, s->w.data, info.dims), set, p->dt_over_cell, true,
-                                st)) != PLUME_OK)
+    if ((status = launch_advect<T>(info, make_vel<T>(ud, vd, wd, info.dims), set, p->dt_over_cell, true, st)) !=
+        PLUME_OK)
       return status;
   }
   if ((status = mark()) != PLUME_OK) return status;
-  float* u = s->u.next;  // after the swap
-  float* v = s->v.next;
-  float* w = s->w.next;
+  T* u = static_cast<T*>(s->u.next);  // after the swap
+  T* v = static_cast<T*>(s->v.next);
+  T* w = static_cast<T*>(s->w.next);
   // project (stepper.py:42, pressure.py:144-154)
-  if ((status = plume_project_begin(&info, u, v, w, s->divergence, stream)) != PLUME_OK) return status;
+  if ((status = project_begin<T>(info, u, v, w, s->divergence, st)) != PLUME_OK) return status;
   if ((status = mark()) != PLUME_OK) return status;
   if (p->solver == 0) {
     if ((status = multigrid_cycles(s->levels, s->level_count, p->solver_iterations, p->multigrid_sweeps, st)) != PLUME_OK)
@@ -1038,36 +1088,61 @@ extern "C" int plume_step(const PlumeStepState* s, const PlumeStepParams* p, voi
     return status;
   }
   if ((status = mark()) != PLUME_OK) return status;
-  k_subtract_gradient<<<face_grid(info), cell_block(), 0, st>>>(info, u, v, w, s->pressure);
+  k_subtract_gradient<T><<<face_grid(info), cell_block(), 0, st>>>(info, u, v, w, s->pressure);
   CHECK_LAUNCH("subtract gradient");
   if ((status = mark()) != PLUME_OK) return status;
   // advect smoke and temperature (stepper.py:54-60): the smoke budget holds smoke.next before its swap
   {
-    Vel vel = make_vel(u, v, w, info.dims);
-    FieldSet set{};
+    VelT<T> vel = make_vel<T>(u, v, w, info.dims);
+    FieldSet<T> set{};
     set.count = 1;  // smoke and temperature share positions: one trace serves both
-    set.f[0] = single_field(s->smoke.data, s->smoke.hat, s->smoke.next, Dims{nx, ny, nz}, f3(0.5f, 0.5f, 0.5f), 0.0f, 1);
-    set.f[0].data[1] = s->temperature.data;
-    set.f[0].hat[1] = s->temperature.hat;
-    set.f[0].next[1] = s->temperature.next;
+    set.f[0] = single_field<T>(sd, static_cast<T*>(s->smoke.hat), static_cast<T*>(s->smoke.next), Dims{nx, ny, nz},
+                               f3(0.5f, 0.5f, 0.5f), 0.0f, 1);
+    set.f[0].data[1] = td;
+    set.f[0].hat[1] = static_cast<T*>(s->temperature.hat);
+    set.f[0].next[1] = static_cast<T*>(s->temperature.next);
     set.f[0].outside[1] = p->ambient_k;
     set.f[0].fields = 2;
     if (s->advect_scratch) {
-      float2* r = reinterpret_cast<float2*>(s->advect_scratch);
+      pair_t<T>* r = reinterpret_cast<pair_t<T>*>(s->advect_scratch);
       set.f[0].range[0] = r;
       set.f[0].range[1] = r + (size_t)nx * ny * nz;
     }
-    if ((status = launch_advect(info, vel, set, p->dt_over_cell, true, st)) != PLUME_OK) return status;
+    if ((status = launch_advect<T>(info, vel, set, p->dt_over_cell, true, st)) != PLUME_OK) return status;
   }
-  if ((status = launch_triple_sum(dims_of(info), s->smoke.data, s->smoke.hat, s->smoke.next, s->sums, s->factor,
-                                  nullptr, st)) != PLUME_OK)
+  if ((status = launch_triple_sum<T>(dims_of(info), sd, static_cast<const T*>(s->smoke.hat),
+                                     static_cast<const T*>(s->smoke.next), s->sums, s->factor, nullptr, st)) != PLUME_OK)
     return status;
   // scale + dissipate (stepper.py:44) on the advected buffers
   const long n = (long)nx * ny * nz;
-  k_scalar_finish<<<grid_stride_blocks(n), 256, 0, st>>>(s->smoke.next, s->temperature.next, n, s->factor,
-                                                         p->apply_dissipation, p->smoke_keep, p->heat_keep, p->ambient_k);
+  k_scalar_finish<T><<<grid_stride_blocks(n), 256, 0, st>>>(static_cast<T*>(s->smoke.next),
+                                                            static_cast<T*>(s->temperature.next), n, s->factor,
+                                                            p->apply_dissipation, p->smoke_keep, p->heat_keep,
+                                                            p->ambient_k);
   CHECK_LAUNCH("scale and dissipate");
   return mark();
+}
+
+}  // namespace plume
+
+extern "C" int plume_step(const PlumeStepState* s, const PlumeStepParams* p, void* stream) {
+  CHECK_ARG(s && p, "step: null argument");
+  CHECK_ARG(valid_dims(s->info.dims), "step: bad dims");
+  CHECK_ARG(s->u.data && s->u.hat && s->u.next && s->v.data && s->v.hat && s->v.next && s->w.data && s->w.hat &&
+                s->w.next && s->smoke.data && s->smoke.hat && s->smoke.next && s->temperature.data &&
+                s->temperature.hat && s->temperature.next && s->pressure && s->divergence && s->sums && s->factor,
+            "step: null buffer");
+  CHECK_ARG(s->levels && s->level_count >= 1 && s->levels[0].q == s->pressure && s->levels[0].rhs == s->divergence &&
+                s->levels[0].residual && s->levels[0].residual != s->pressure,
+            "step: levels must start at the grid's pressure and divergence, with a second pressure array");
+  CHECK_ARG(p->confinement == 0.0f || (s->curl[0] && s->curl[1] && s->curl[2] && s->push[0] && s->push[1] && s->push[2]),
+            "step: confinement scratch missing");
+  switch (s->storage) {
+    case PLUME_STORAGE_F32: return step<float>(s, p, stream);
+    case PLUME_STORAGE_BF16: return step<__nv_bfloat16>(s, p, stream);
+    case PLUME_STORAGE_F16: return step<__half>(s, p, stream);
+  }
+  return fail(PLUME_ERR_INVALID, "step: storage %d", s->storage);
 }
 
 // ---- the smoke budget without caller scratch --------------------------------------------------------------

@@ -59,7 +59,10 @@ class FrameRenderer:
         gradient_shape = N.c_int3(*self.gradient.shape[:3])
         bricks = N.ptr(self.bricks) if tuple(self.bricks.shape) == (N.lib().plume_brick_floats(N.shape3(smoke)),) \
             else None
-        N.call("plume_raymarch", info, N.ptr(smoke), N.ptr(temperature), N.ptr(self.gradient), gradient_shape,
+        if temperature.dtype != smoke.dtype:
+            raise TypeError("smoke and temperature must have the same storage type")
+        N.call("plume_raymarch", info, N.field_ptr(smoke), N.field_ptr(temperature), N.storage_of(smoke),
+               N.ptr(self.gradient), gradient_shape,
                N.ptr(self.light), N.shape3(self.light), view, self.look_params, N.ptr(image), image.shape[0],
                image.shape[1], bricks, N.stream())
 

@@ -18,6 +18,7 @@ class LightVolume:
         self.bricks = torch.empty(N.lib().plume_brick_floats(N.c_int3(*cells)), dtype=torch.float32, device=device)
 
     def compute(self, smoke: torch.Tensor, cell_m: float) -> torch.Tensor:
-        N.call("plume_light_volume", N.shape3(smoke), N.ptr(smoke), N.f3(self.toward_light), cell_m,
+        N.call("plume_light_volume", N.shape3(smoke), N.field_ptr(smoke), N.storage_of(smoke),
+               N.f3(self.toward_light), cell_m,
                self.opacity_per_density, N.ptr(self.light), N.ptr(self.bricks), N.stream())
         return self.light

@@ -23,7 +23,8 @@ class NormalField:
 
     def compute(self, smoke: torch.Tensor) -> torch.Tensor:
         weights = (ctypes.c_float * len(self.weights))(*self.weights.tolist())
-        N.call("plume_normal_field", N.shape3(smoke), N.ptr(smoke), N.ptr(self.blurred), N.ptr(self.scratch),
+        N.call("plume_normal_field", N.shape3(smoke), N.field_ptr(smoke), N.storage_of(smoke), N.ptr(self.blurred),
+               N.ptr(self.scratch),
                N.ptr(self.gradient), weights, self.radius, N.stream())
         return self.gradient
 

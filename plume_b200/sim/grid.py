@@ -1,7 +1,9 @@
 """The MAC grid state on the device (mirrors chadmv/plume src/plume/sim/grid.py:15-94).
 
-Fields are float32 torch tensors, C-contiguous, shape (nx, ny, nz) with z contiguous; face velocities are
+Fields are torch tensors, C-contiguous, shape (nx, ny, nz) with z contiguous; face velocities are
 (nx+1, ny, nz), (nx, ny+1, nz), (nx, ny, nz+1). Sample positions are `index + offset` in cell units.
+Velocity, smoke and temperature are float32 as in the reference, or, for the mixed-precision step, bfloat16
+or float16 storage (every kernel computes in float32); pressure and divergence are always float32.
 """
 
 from dataclasses import dataclass
@@ -21,13 +23,14 @@ class AdvectedField:
     buffers. The backward pass is evaluated inside the correction kernel, so `back` is only allocated if a
     caller asks for it."""
 
-    def __init__(self, shape, offset, outside: float, uses_outside: bool, device: str, initial: float = 0.0):
+    def __init__(self, shape, offset, outside: float, uses_outside: bool, device: str, initial: float = 0.0,
+                 dtype=torch.float32):
         self.offset = offset
         self.outside = outside
         self.uses_outside = 1 if uses_outside else 0
-        self.data = torch.full(shape, initial, dtype=torch.float32, device=device)
-        self.hat = torch.zeros(shape, dtype=torch.float32, device=device)
-        self.next = torch.zeros(shape, dtype=torch.float32, device=device)
+        self.data = torch.full(shape, initial, dtype=dtype, device=device)
+        self.hat = torch.zeros(shape, dtype=dtype, device=device)
+        self.next = torch.zeros(shape, dtype=dtype, device=device)
         self._back = None
 
     @property
@@ -56,6 +59,11 @@ class Grid:
     def velocity_fields(self):
         return self.u, self.v, self.w
 
+    @property
+    def storage(self) -> torch.dtype:
+        """The element type of the velocity, smoke and temperature arrays."""
+        return self.smoke.data.dtype
+
 
 def make_info(cells, cell_m, origin_m, open_lo, open_hi, fill_hi=(1.0, 1.0, 1.0), ghost_gap=0.5) -> GridInfo:
     info = GridInfo()
@@ -73,18 +81,22 @@ def _is_open(kind: str) -> int:
     return 1 if kind == "open" else 0
 
 
-def make_grid(derived, cell_m: float, faces, ambient_k: float, device: str) -> Grid:
-    """Allocates a grid at rest, filled with ambient air."""
+def make_grid(derived, cell_m: float, faces, ambient_k: float, device: str, storage=torch.float32) -> Grid:
+    """Allocates a grid at rest, filled with ambient air; `storage` is the element type of the velocity, smoke
+    and temperature arrays (float32, or bfloat16 / float16 for the mixed-precision step)."""
+    if storage not in (torch.float32, torch.bfloat16, torch.float16):
+        raise TypeError(f"storage must be float32, bfloat16 or float16, not {storage}")
     nx, ny, nz = derived.cells
     info = make_info(derived.cells, cell_m, derived.domain_min_m,
                      [_is_open(k) for k in (faces.left, faces.bottom, faces.back)],
                      [_is_open(k) for k in (faces.right, faces.top, faces.front)])
     cells = (nx, ny, nz)
     return Grid(info=info, device=device, cells=cells,
-                u=AdvectedField((nx + 1, ny, nz), U_FACE, 0.0, False, device),
-                v=AdvectedField((nx, ny + 1, nz), V_FACE, 0.0, False, device),
-                w=AdvectedField((nx, ny, nz + 1), W_FACE, 0.0, False, device),
-                smoke=AdvectedField(cells, CENTER, 0.0, True, device),
-                temperature=AdvectedField(cells, CENTER, ambient_k, True, device, initial=ambient_k),
+                u=AdvectedField((nx + 1, ny, nz), U_FACE, 0.0, False, device, dtype=storage),
+                v=AdvectedField((nx, ny + 1, nz), V_FACE, 0.0, False, device, dtype=storage),
+                w=AdvectedField((nx, ny, nz + 1), W_FACE, 0.0, False, device, dtype=storage),
+                smoke=AdvectedField(cells, CENTER, 0.0, True, device, dtype=storage),
+                temperature=AdvectedField(cells, CENTER, ambient_k, True, device, initial=ambient_k,
+                                          dtype=storage),
                 pressure=torch.zeros(cells, dtype=torch.float32, device=device),
                 divergence=torch.zeros(cells, dtype=torch.float32, device=device))

@@ -20,6 +20,28 @@ COARSEST_RELAXATION = 1.5
 SMOOTHING_RELAXATION = 1.0
 
 
+@dataclass(frozen=True)
+class SolverTuning:
+    """The library's pressure-solve strategy (results do not depend on it): levels of at least
+    `tiled_min_cells` cells sweep in shared-memory tiles, one launch per sweep; smaller ones one colour per
+    launch; the first level of at most `bottom_max_cells` cells and all coarser ones run in one launch
+    (`bottom_kind` 0 one block, 1 an 8-CTA cluster)."""
+
+    tiled_min_cells: int
+    bottom_max_cells: int
+    bottom_kind: int
+
+
+def solver_tuning() -> SolverTuning:
+    values = (N.ctypes.c_longlong(), N.ctypes.c_longlong(), N.ctypes.c_int32())
+    N.call("plume_solver_tuning", *(N.ctypes.byref(v) for v in values))
+    return SolverTuning(*(int(v.value) for v in values))
+
+
+def tune_solver(tuning: SolverTuning) -> None:
+    N.call("plume_tune_solver", tuning.tiled_min_cells, tuning.bottom_max_cells, tuning.bottom_kind)
+
+
 @dataclass
 class Level:
     info: GridInfo

@@ -43,8 +43,16 @@ def simulate(recipe, derived, device: str, capture: Capture) -> StepLog:
         capture(frame, grid)
 
 
-def simulate_frames(recipe, derived, device: str) -> Generator[tuple[int, Grid], None, StepLog]:
-    grid = make_grid(derived, recipe.domain.cell_m, recipe.domain.faces, recipe.domain.ambient_k, device)
+def simulate_frames(recipe, derived, device: str, storage=None,
+                    initial_state=None) -> Generator[tuple[int, Grid], None, StepLog]:
+    """`storage` (float32 by default; bfloat16 or float16 for the mixed-precision step) and
+    `initial_state(grid)` (fills the fields before the first step) extend the reference's signature."""
+    import torch
+
+    grid = make_grid(derived, recipe.domain.cell_m, recipe.domain.faces, recipe.domain.ambient_k, device,
+                     storage=torch.float32 if storage is None else storage)
+    if initial_state is not None:
+        initial_state(grid)
     stepper = Stepper(grid, recipe)
     cap = StepCap(recipe)
     base_done = 0

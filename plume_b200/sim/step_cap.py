@@ -30,7 +30,13 @@ class StepCap:
                          for e in recipe.emitter]
 
     def plan(self, grid, start_s: float, length_s: float, base_steps: int, label: str) -> StepPlan:
-        speed = max(self.grid_speed(grid), self.emitter_speed(start_s, start_s + length_s))
+        return self.plan_for_speed(self.grid_speed(grid), start_s, length_s, base_steps, label)
+
+    def plan_for_speed(self, grid_speed: float, start_s: float, length_s: float, base_steps: int,
+                       label: str) -> StepPlan:
+        """The plan for a block given the grid's fastest face speed (read by the caller, e.g. for many grids
+        at once)."""
+        speed = max(grid_speed, self.emitter_speed(start_s, start_s + length_s))
         needed = math.ceil(speed * length_s / (self.max_cells * self.cell_m))
         steps = max(base_steps, needed)
         if steps > max(self.max_substeps, base_steps):
@@ -44,12 +50,18 @@ class StepCap:
     def grid_speed(grid) -> float:
         """The fastest face velocity component, in m/s."""
         speed = torch.zeros(1, dtype=torch.float32, device=grid.device)
-        u, v, w = (f.data for f in grid.velocity_fields())
-        N.call("plume_grid_speed", grid.info, N.ptr(u), N.ptr(v), N.ptr(w), N.ptr(speed), N.stream())
+        enqueue_grid_speed(grid, speed)
         return float(speed.item())
 
     def emitter_speed(self, start_s: float, end_s: float) -> float:
         return max((s for b, e, s in self.emitters if b < end_s and e > start_s), default=0.0)
+
+
+def enqueue_grid_speed(grid, out: torch.Tensor) -> None:
+    """Enqueues the device max of |u|, |v|, |w| into `out` (one float32 element) on the current stream."""
+    u, v, w = (f.data for f in grid.velocity_fields())
+    N.call("plume_grid_speed", grid.info, N.field_ptr(u), N.field_ptr(v), N.field_ptr(w), N.storage_of(u),
+           N.ptr(out), N.stream())
 
 
 def _emitter_speed(velocity_mps, mode: str) -> float:

@@ -72,7 +72,8 @@ class Stepper:
         s.info = grid.info
         for name in ("u", "v", "w", "smoke", "temperature"):
             field = getattr(grid, name)
-            setattr(s, name, N.PlumeField(N.ptr(field.data).value, N.ptr(field.hat).value, N.ptr(field.next).value))
+            setattr(s, name, N.PlumeField(N.field_ptr(field.data).value, N.field_ptr(field.hat).value,
+                                          N.field_ptr(field.next).value))
         s.pressure, s.divergence = N.ptr(grid.pressure).value, N.ptr(grid.divergence).value
         if self.confinement is not None:
             s.curl = (ctypes.c_void_p * 3)(*[N.ptr(t).value for t in self.confinement._curl])
@@ -90,6 +91,7 @@ class Stepper:
         self._levels = levels
         s.levels = ctypes.cast(levels, ctypes.POINTER(N.PlumeLevel))
         s.level_count = len(levels)
+        s.storage = N.storage_of(grid.smoke.data)
         return s
 
     def step(self, time_s: float, dt: float) -> None:

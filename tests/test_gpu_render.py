@@ -48,9 +48,9 @@ def test_light_volume_empty_space_skipping_changes_no_bit(cuda_device):
     toward = N.f3(np.array([0.5, 0.8, 0.3]) / np.linalg.norm([0.5, 0.8, 0.3]))
     with_bricks, without = torch.empty_like(smoke), torch.empty_like(smoke)
     bricks = torch.empty(N.lib().plume_brick_floats(N.shape3(smoke)), dtype=torch.float32, device="cuda:0")
-    N.call("plume_light_volume", N.shape3(smoke), N.ptr(smoke), toward, 0.05, 4.0, N.ptr(with_bricks), N.ptr(bricks),
-           N.stream())
-    N.call("plume_light_volume", N.shape3(smoke), N.ptr(smoke), toward, 0.05, 4.0, N.ptr(without), None, N.stream())
+    N.call("plume_light_volume", N.shape3(smoke), N.ptr(smoke), 0, toward, 0.05, 4.0, N.ptr(with_bricks),
+           N.ptr(bricks), N.stream())
+    N.call("plume_light_volume", N.shape3(smoke), N.ptr(smoke), 0, toward, 0.05, 4.0, N.ptr(without), None, N.stream())
     assert torch.equal(with_bricks, without)
     assert float((smoke <= 0).float().mean()) > 0.5  # the case has plenty of empty space to skip
 
@@ -90,7 +90,7 @@ def test_march_empty_space_skipping_changes_no_bit(cuda_device, channels):
     skipped = torch.zeros_like(renderer.image)
     full = torch.zeros_like(renderer.image)
     renderer.march(c.smoke.data, c.temperature.data, c.info, renderer.view_params, skipped)
-    N.call("plume_raymarch", c.info, N.ptr(c.smoke.data), N.ptr(c.temperature.data), N.ptr(renderer.gradient),
+    N.call("plume_raymarch", c.info, N.ptr(c.smoke.data), N.ptr(c.temperature.data), 0, N.ptr(renderer.gradient),
            N.c_int3(*renderer.gradient.shape[:3]), N.ptr(renderer.light), N.shape3(renderer.light),
            renderer.view_params, renderer.look_params, N.ptr(full), full.shape[0], full.shape[1], None, N.stream())
     assert torch.equal(skipped, full)
