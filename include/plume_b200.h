@@ -285,6 +285,57 @@ int plume_raymarch(const PlumeGridInfo* info, const void* smoke, const void* tem
                    const int32_t light_shape[3], const PlumeViewParams* view, const PlumeLookParams* look, float* image,
                    int32_t height, int32_t width, float* bricks, void* stream);
 
+/* ---- sheet assembly and the numbers file (sheet/assemble.py:39-77, report/numbers.py:42-100) ------------- */
+/* Raw frames are one (frames, height, width, 5) float32 device array; finished frames (frames, size, size, 5)
+ * double; quantised frames (frames, size, size, 4) bytes. Scratch and outputs are caller-owned device memory. */
+
+/* crop.py:29-43 content_box: *heat_key = the order key of the largest heat; box = (left, top, right, bottom),
+ * right and bottom exclusive (right <= left when no frame shows anything). */
+int plume_sheet_content_box(const float* raw, int32_t frames, int32_t height, int32_t width, uint32_t* heat_key,
+                            int32_t* box, void* stream);
+
+/* resample.py:16-41 resample_frame: the crop square of every frame, padded by `pad` empty pixels, resampled to
+ * out x out with the bicubic two-pass filter of the per-pass tap tables (first source index, window length,
+ * ksize normalised double weights per output index; source indices are padded-image indices); the horizontal
+ * pass covers padded rows [row_first, row_first + rows). temp: frames * 5 * rows * out floats. */
+int plume_sheet_resample(const float* raw, int32_t frames, int32_t height, int32_t width, int32_t pad,
+                         const float empty[5], const int32_t* h_first, const int32_t* h_count, const double* h_weights,
+                         int32_t h_ksize, const int32_t* v_first, const int32_t* v_count, const double* v_weights,
+                         int32_t v_ksize, int32_t row_first, int32_t rows, int32_t out, int32_t shade_layout,
+                         float* temp, double* frame, void* stream);
+
+/* soften.py:21-49 blur: `channels` planes starting at `offset` of `stride` interleaved doubles per pixel,
+ * blurred along rows then columns (edges extended) with 2 * radius + 1 device weights; dst may equal src. */
+int plume_sheet_blur(const double* src, double* dst, double* scratch, int32_t frames, int32_t size, int32_t channels,
+                     int32_t stride, int32_t offset, const double* weights, int32_t radius, void* stream);
+
+/* soften.py:52-60 _renormalize (normal layout). */
+int plume_sheet_renormalize(double* frame, int32_t frames, int32_t size, void* stream);
+
+/* shade.py:22-42 ease_thin_pixels, given `blurred`: a frame-shaped array whose thickness and shade-times-
+ * thickness channels hold those planes blurred by the neighbourhood Gaussian; sums: 2 doubles per frame. */
+int plume_sheet_ease(double* frame, const double* blurred, double* sums, int32_t frames, int32_t size,
+                     double fade_thickness, void* stream);
+
+/* The largest value of `channel` over every pixel of every frame whose thickness is >= floor:
+ * out[0] = that value (0 when none), out[1] = 1 if any pixel qualified. key, any: scratch. */
+int plume_sheet_channel_max(const double* frame, int32_t frames, int32_t size, int32_t channel, double floor,
+                            unsigned long long* key, int32_t* any, double* out, void* stream);
+
+/* quantize.py:20-39 quantize, then assemble.py:70-73: *touched = 1 when a frame has a non-zero R or G byte
+ * within `gutter` pixels of its edge. */
+int plume_sheet_quantize(const double* frame, int32_t frames, int32_t size, double heat_divisor,
+                         double shade_divisor, int32_t shade_layout, int32_t gutter, uint8_t* rgba, int32_t* touched,
+                         void* stream);
+
+/* pack.py:13-20 pack: frames in rows of `columns`, unused slots zero; sheet is (rows * size, columns * size, 4). */
+int plume_sheet_pack(const uint8_t* rgba, int32_t frames, int32_t size, int32_t columns, uint8_t* sheet, void* stream);
+
+/* numbers.py:80-100 per frame (9 int64s): covered count (G >= covered_level), covered box left, top, right,
+ * bottom (right/bottom exclusive), R and G byte sums over covered pixels, G byte sum, largest R byte. */
+int plume_sheet_measure(const uint8_t* rgba, int32_t frames, int32_t size, int32_t covered_level, long long* stats,
+                        void* stream);
+
 #ifdef __cplusplus
 }
 #endif

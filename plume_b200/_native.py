@@ -87,6 +87,7 @@ STEP_PHASES = ("forces", "velocity advection", "divergence", "pressure solve", "
 _P, _I, _F = ctypes.c_void_p, ctypes.c_int32, ctypes.c_float
 _INFO, _SHAPE, _F3P = ctypes.POINTER(PlumeGridInfo), ctypes.POINTER(ctypes.c_int32), ctypes.POINTER(ctypes.c_float)
 _PP = ctypes.POINTER(ctypes.c_void_p)
+_F5P = ctypes.POINTER(ctypes.c_float)
 
 SIGNATURES = {
     "plume_abi_version": [],
@@ -121,6 +122,15 @@ SIGNATURES = {
     "plume_brick_max": [_SHAPE, _P, _I, _P, _P],
     "plume_raymarch": [_INFO, _P, _P, _I, _P, _SHAPE, _P, _SHAPE, ctypes.POINTER(PlumeViewParams),
                        ctypes.POINTER(PlumeLookParams), _P, _I, _I, _P, _P],
+    "plume_sheet_content_box": [_P, _I, _I, _I, _P, _P, _P],
+    "plume_sheet_resample": [_P, _I, _I, _I, _I, _F5P, _P, _P, _P, _I, _P, _P, _P, _I, _I, _I, _I, _I, _P, _P, _P],
+    "plume_sheet_blur": [_P, _P, _P, _I, _I, _I, _I, _I, _P, _I, _P],
+    "plume_sheet_renormalize": [_P, _I, _I, _P],
+    "plume_sheet_ease": [_P, _P, _P, _I, _I, ctypes.c_double, _P],
+    "plume_sheet_channel_max": [_P, _I, _I, _I, ctypes.c_double, _P, _P, _P, _P],
+    "plume_sheet_quantize": [_P, _I, _I, ctypes.c_double, ctypes.c_double, _I, _I, _P, _P, _P],
+    "plume_sheet_pack": [_P, _I, _I, _I, _P, _P],
+    "plume_sheet_measure": [_P, _I, _I, _I, _P, _P],
 }
 
 _lib = None

@@ -14,7 +14,8 @@ from pathlib import Path
 
 PACKAGE = Path(__file__).resolve().parent
 REPO = PACKAGE.parent
-SOURCES = [PACKAGE / "csrc" / "sim.cu", PACKAGE / "csrc" / "multigrid.cu", PACKAGE / "csrc" / "render.cu"]
+SOURCES = [PACKAGE / "csrc" / "sim.cu", PACKAGE / "csrc" / "multigrid.cu", PACKAGE / "csrc" / "render.cu",
+           PACKAGE / "csrc" / "sheet.cu"]
 HEADERS = [PACKAGE / "csrc" / "common.cuh", PACKAGE / "csrc" / "poisson.cuh", REPO / "include" / "plume_b200.h"]
 LIBRARY = PACKAGE / "libplume_b200.so"
 NVCC_FLAGS = ["-O3", "-std=c++17", "-gencode", "arch=compute_100a,code=sm_100a", "-lineinfo", "-fmad=false",

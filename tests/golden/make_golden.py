@@ -17,6 +17,7 @@ The GPU tests compare the CUDA path's raw frames with the oracle run on the same
 statistics; they never read the reference.
 """
 
+import hashlib
 import json
 import sys
 from pathlib import Path
@@ -71,6 +72,36 @@ def reference_numbers(frames) -> str:
     return numbers_text(measure(assembled.frames, derived.fps), facts)
 
 
+LAYOUTS = ("heat,thickness,shade,unused", "heat,thickness,normal_x,normal_y")
+
+
+def frames_digest(frames) -> str:
+    digest = hashlib.sha256()
+    for frame in frames:
+        digest.update(np.ascontiguousarray(frame, dtype=np.uint8).tobytes())
+    return digest.hexdigest()
+
+
+def reference_sheets(frames) -> dict:
+    """The reference's own sheet assembly (plume.sheet.assemble) of the oracle's preview frames, in both
+    channel layouts: the crop, margin, divisors and a SHA-256 of the quantised frames."""
+    sys.path.insert(0, str(REFERENCE_SRC))
+    from plume.recipe.derived import derive as ref_derive
+    from plume.recipe.load import load_recipe as ref_load
+    from plume.render.camera import sheet_domain_view as ref_view
+    from plume.sheet.assemble import assemble, seat_point
+
+    recipe = ref_load(HERE / "smoke_puff.toml", preview=True)
+    view = ref_view(recipe, ref_derive(recipe))
+    sheets = {}
+    for layout in LAYOUTS:
+        a = assemble(list(frames), view, seat_point(recipe), recipe.output.frame_px, recipe.render, layout)
+        sheets[layout] = {"crop": [a.crop.left, a.crop.top, a.crop.side], "margin": a.margin,
+                          "heat_divisor": a.heat_divisor, "shade_divisor": a.shade_divisor,
+                          "frames_sha256": frames_digest(a.frames)}
+    return sheets
+
+
 def read_numbers(text: str):
     head, _, table = text.partition("\n\n")
     summary = {}
@@ -120,6 +151,9 @@ def main() -> None:
         return
     text = reference_numbers(frames)
     (HERE / "oracle_preview.numbers.txt").write_text(text)
+    sheets = {"source": "chadmv/plume src/plume/sheet/assemble.py:39-60 (reference code, run on the oracle's "
+                        "smoke puff preview raw frames)", "layouts": reference_sheets(frames)}
+    (HERE / "preview_sheet.json").write_text(json.dumps(sheets, indent=1) + "\n")
     problems = numbers_close(text, (HERE / "smoke_puff_preview.numbers.txt").read_text())
     print("golden numbers:", "match within the reference's tolerances" if not problems else problems)
     if problems:

@@ -16,8 +16,9 @@ pytestmark = pytest.mark.gpu
 # max |gpu - fp64| / max |fp64| per field after SUBSTEPS substeps (float32 storage is ~1e-6)
 SUBSTEPS = 4
 FIELD_TOL = {"float32": 1e-4, "bfloat16": 3e-2, "float16": 4e-3}
-# max |thickness - fp64 thickness| of a rendered frame of that state
-THICKNESS_TOL = {"float32": 2e-3, "bfloat16": 5e-2, "float16": 1e-2}
+# max |thickness - fp64 thickness| of a rendered frame of that state (measured on B200: float32 7.6e-4,
+# bfloat16 2.4e-3, float16 9.7e-4; the field errors: float32 6e-5, bfloat16 1.5e-2, float16 1.9e-3)
+THICKNESS_TOL = {"float32": 2e-3, "bfloat16": 5e-3, "float16": 2e-3}
 
 
 def storage_dtype(name):
