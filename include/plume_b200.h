@@ -336,6 +336,55 @@ int plume_sheet_pack(const uint8_t* rgba, int32_t frames, int32_t size, int32_t 
 int plume_sheet_measure(const uint8_t* rgba, int32_t frames, int32_t size, int32_t covered_level, long long* stats,
                         void* stream);
 
+/* ---- live viewer compute (view/viewport.py, view/slice_plane.py, view/live_run.py, view/frame_cache.py) ---- */
+
+/* LookInputs (viewport.py:50-59): view 0 look, 1 heat, 2 thickness, 3 shade (the normal in the normal layout);
+ * toward_light in the drawn camera's space; background linear RGB. */
+typedef struct PlumeLookInputs {
+  int32_t view;
+  int32_t shade_layout;
+  float heat_divisor;
+  float shade_divisor;
+  float shade_depth;
+  float ambient;
+  float toward_light[3];
+  float background[3];
+} PlumeLookInputs;
+
+/* viewport.py:78-113 look_kernel: a raw march image (height, width, 5) to display bytes (height, width, 4);
+ * smoke_ramp/emission_ramp: ramp_n linear RGB float triples; srgb: srgb_n bytes of the sRGB curve. */
+int plume_view_look(const float* raw, int32_t height, int32_t width, const float* smoke_ramp,
+                    const float* emission_ramp, int32_t ramp_n, const uint8_t* srgb, int32_t srgb_n,
+                    const PlumeLookInputs* inputs, uint8_t* out, void* stream);
+
+/* viewport.py:116-140 center_depth_kernel: *result (device) = distance along the ray where the march's
+ * thickness first reaches threshold, -1 if never. */
+int plume_view_center_depth(const float* smoke, const PlumeGridInfo* info, const float origin[3],
+                            const float direction[3], float opacity_per_density, float threshold, float* result,
+                            void* stream);
+
+/* vorticity.py:17-22 center_velocity_kernel: centers is (nx, ny, nz, 3). */
+int plume_view_center_velocity(const PlumeGridInfo* info, const float* u, const float* v, const float* w,
+                               float* centers, void* stream);
+
+/* vorticity.py:25-45 curl_kernel on a cell-centred (nx, ny, nz, 3) field (the slice plane's swirl). */
+int plume_view_curl(const PlumeGridInfo* info, const float* centers, float* curl, void* stream);
+
+/* slice_plane.py:104-107 speed_kernel: out[c] = |vectors[c]|. */
+int plume_view_speed(const float* vectors, long long cells, float* out, void* stream);
+
+/* slice_plane.py:110-137 slice_kernel over the display bytes `image` (height, width, 4), in place. */
+int plume_view_slice(const PlumeViewParams* view, const PlumeGridInfo* info, int32_t axis, float coordinate_m,
+                     const float* values, float low, float high, const float* ramp, int32_t ramp_n, uint8_t* image,
+                     int32_t height, int32_t width, void* stream);
+
+/* live_run.py:42-57 boundary_layer_kernel: layers is (6, S, S) with S the largest dimension. */
+int plume_view_boundary_layers(const float* smoke, const int32_t shape[3], float* layers, void* stream);
+
+/* frame_cache.py:26-50 narrow/widen kernels: float32 <-> IEEE half (round to nearest even). */
+int plume_view_narrow(const float* src, void* dst, long long count, void* stream);
+int plume_view_widen(const void* src, float* dst, long long count, void* stream);
+
 #ifdef __cplusplus
 }
 #endif

@@ -41,6 +41,12 @@ class PlumeLookParams(ctypes.Structure):
                 ("shade_layout", ctypes.c_int32), ("shade_fill", ctypes.c_float)]
 
 
+class PlumeLookInputs(ctypes.Structure):
+    _fields_ = [("view", ctypes.c_int32), ("shade_layout", ctypes.c_int32), ("heat_divisor", ctypes.c_float),
+                ("shade_divisor", ctypes.c_float), ("shade_depth", ctypes.c_float), ("ambient", ctypes.c_float),
+                ("toward_light", c_float3), ("background", c_float3)]
+
+
 class PlumeField(ctypes.Structure):
     _fields_ = [("data", ctypes.c_void_p), ("hat", ctypes.c_void_p), ("next", ctypes.c_void_p)]
 
@@ -131,6 +137,15 @@ SIGNATURES = {
     "plume_sheet_quantize": [_P, _I, _I, ctypes.c_double, ctypes.c_double, _I, _I, _P, _P, _P],
     "plume_sheet_pack": [_P, _I, _I, _I, _P, _P],
     "plume_sheet_measure": [_P, _I, _I, _I, _P, _P],
+    "plume_view_look": [_P, _I, _I, _P, _P, _I, _P, _I, ctypes.POINTER(PlumeLookInputs), _P, _P],
+    "plume_view_center_depth": [_P, _INFO, _F3P, _F3P, _F, _F, _P, _P],
+    "plume_view_center_velocity": [_INFO, _P, _P, _P, _P, _P],
+    "plume_view_curl": [_INFO, _P, _P, _P],
+    "plume_view_speed": [_P, ctypes.c_longlong, _P, _P],
+    "plume_view_slice": [ctypes.POINTER(PlumeViewParams), _INFO, _I, _F, _P, _F, _F, _P, _I, _P, _I, _I, _P],
+    "plume_view_boundary_layers": [_P, _SHAPE, _P, _P],
+    "plume_view_narrow": [_P, _P, ctypes.c_longlong, _P],
+    "plume_view_widen": [_P, _P, ctypes.c_longlong, _P],
 }
 
 _lib = None

@@ -113,7 +113,8 @@ def _build(cls: type, table: dict, where: str):
     hints = typing.get_type_hints(cls)
     fields = {f.name: f for f in dataclasses.fields(cls)}
     for key in table:
-        if key not in fields and not (where == "" and key in ("resolved", "look")):
+        if key not in fields and not (where == "" and key == "resolved") and not (where == "look" and
+                                                                                key == "backgrounds"):
             raise RecipeError(f"unknown key {where + '.' if where else ''}{key}")
     values = {}
     for name, f in fields.items():

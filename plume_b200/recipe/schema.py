@@ -2,8 +2,8 @@
 
 Key names, nesting and defaults follow chadmv/plume src/plume/recipe/schema.py:60-247 so that a recipe written
 for the reference loads here unchanged (a recipe is a file format: its keys have to match). Only the tables
-the simulation, the render and the sheet geometry use are modelled; the contact-sheet colours (`look`) are
-accepted and ignored.
+the simulation, the render, the sheet geometry and the viewer's look use are modelled (the contact sheets'
+`look.backgrounds` is accepted and ignored).
 """
 
 from dataclasses import dataclass, field
@@ -138,6 +138,21 @@ class PreviewSettings:
     frame_px: int = 128
 
 
+ColorStop = tuple[float, str]
+
+
+@dataclass(frozen=True, kw_only=True)
+class LookSettings:
+    """How the contact sheets and the viewer light a sheet frame (chadmv/plume recipe/schema.py:214-225)."""
+
+    ambient: float = 0.65
+    shade_depth: float = 0.75
+    smoke_ramp: tuple[ColorStop, ...] = ((0.0, "#aea193"), (0.4, "#bc9c84"), (0.75, "#dca07a"), (1.0, "#f5b47e"))
+    emission_ramp: tuple[ColorStop, ...] = ((0.0, "#000000"), (0.2, "#3a0c04"), (0.5, "#c4441a"), (0.8, "#ff9a3a"),
+                                            (1.0, "#fff2c2"))
+    contact_px: int = 128
+
+
 @dataclass(frozen=True, kw_only=True)
 class Recipe:
     emitter: tuple[EmitterSettings, ...]
@@ -152,3 +167,4 @@ class Recipe:
     render: RenderSettings = field(default_factory=RenderSettings)
     output: OutputSettings = field(default_factory=OutputSettings)
     preview: PreviewSettings = field(default_factory=PreviewSettings)
+    look: LookSettings = field(default_factory=LookSettings)
