@@ -6,6 +6,7 @@ keeps the full run's length), then fill the "empty means derived" defaults.
 """
 
 import dataclasses
+import difflib
 import math
 import tomllib
 import typing
@@ -15,11 +16,14 @@ from plume_b200.recipe.errors import RecipeError
 from plume_b200.recipe.schema import CHANNEL_LAYOUTS, FACE_KINDS, SEED_MAX, Recipe
 
 
-def load_recipe(path: Path, preview: bool = False) -> Recipe:
+def load_recipe(path: Path, preview: bool = False, sets=()) -> Recipe:
+    """The recipe at `path`, merged over its `extends` parents, with `--set key=value` overrides applied
+    (recipe/load.py:18-28, recipe/variation.py)."""
+    from plume_b200.recipe.variation import apply_sets, read_toml, resolve_extends
+
     path = Path(path)
-    with path.open("rb") as handle:
-        table = tomllib.load(handle)
-    return resolve_table(table, path.stem, preview)
+    table, _ = resolve_extends(read_toml(path), path)
+    return resolve_table(apply_sets(table, sets), path.stem, preview)
 
 
 def resolve_table(table: dict, recipe_stem: str, preview: bool = False) -> Recipe:
@@ -115,7 +119,9 @@ def _build(cls: type, table: dict, where: str):
     for key in table:
         if key not in fields and not (where == "" and key == "resolved") and not (where == "look" and
                                                                                 key == "backgrounds"):
-            raise RecipeError(f"unknown key {where + '.' if where else ''}{key}")
+            close = difflib.get_close_matches(key, list(fields), n=1)
+            hint = f"; did you mean {close[0]}?" if close else ""
+            raise RecipeError(f"unknown key {where + '.' if where else ''}{key}{hint}")
     values = {}
     for name, f in fields.items():
         path = f"{where}.{name}" if where else name
