@@ -208,7 +208,7 @@ int plume_multigrid(const PlumeLevel* levels, int32_t level_count, int32_t cycle
  * `tiled_min_cells` cells sweep in shared-memory tiles (one launch per sweep), smaller levels one colour per
  * launch; the first level with at most `bottom_max_cells` cells and all coarser ones run in one launch:
  * bottom_kind 1 an 8-CTA thread-block cluster (levels split in x-slabs over the CTAs' shared memory), 0 one
- * 1024-thread block; at most 200 KiB of shared memory per CTA. Process-wide; defaults 2^40, 8192, 0. */
+ * 1024-thread block; at most 200 KiB of shared memory per CTA. Process-wide; defaults 2^40, 2048, 0. */
 int plume_tune_solver(long long tiled_min_cells, long long bottom_max_cells, int32_t bottom_kind);
 /* The current pressure-solve strategy (the three values plume_tune_solver sets). */
 int plume_solver_tuning(long long* tiled_min_cells, long long* bottom_max_cells, int32_t* bottom_kind);
