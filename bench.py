@@ -49,6 +49,7 @@ def parse_args():
     ap.add_argument("--impl", choices=("ours", "reference"), default="ours")
     ap.add_argument("--cells", default="128,192,128")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-variants", action="store_true", help="skip the mixed-storage and batched measurements")
     return ap.parse_args()
 
 
@@ -139,6 +140,94 @@ def cpu_baseline(recipe, derived, fields, budget_s: float = 20.0) -> dict:
     return {"value": cells * steps / elapsed / 1e6, "unit": METRIC, "cores": threads, "kind": "port",
             "sample": f"{steps} whole-grid substeps of the {'x'.join(map(str, derived.cells))} plain step after 1 "
                       f"warm-up, oracle C++ FP32 with OpenMP on {threads} threads ({elapsed:.1f} s)"}
+
+
+def storage_variants(recipe, derived, fields, steps: int, device: str) -> dict:
+    """The same workload with velocity, smoke and temperature stored as bfloat16 / float16 (float32
+    arithmetic): Mcell-substeps/s over `steps` substeps, and the error against an FP64 run of the plain method
+    on a small case of the same step (24 x 32 x 24, 4 substeps): the largest field error relative to the
+    field's range and the largest rendered-thickness error."""
+    import numpy as np
+    import torch
+
+    from oracle import oracle as O
+    from plume_b200.recipe.derived import derive
+    from plume_b200.render.camera import sheet_domain_view
+    from plume_b200.render.frame_renderer import FrameRenderer
+    from plume_b200.sim.grid import make_grid
+    from plume_b200.sim.stepper import Stepper
+    from plume_b200.workloads import operator_fields, plain_step_recipe
+
+    small = plain_step_recipe((24, 32, 24), cycles=4)
+    small_derived = derive(small)
+    sd = small.domain
+    reference = O.make_grid(small_derived, sd.cell_m, sd.faces, sd.ambient_k, "f64")
+    small_fields = operator_fields(small_derived.cells, 11, sd.ambient_k)
+    for name, values in small_fields.items():
+        getattr(reference, name).data[...] = values
+    stepper64 = O.Stepper(reference, small)
+    for n in range(4):
+        stepper64.step(n * small_derived.dt_s, small_derived.dt_s)
+    view = sheet_domain_view(small, small_derived)
+    thickness64 = O.FrameRenderer(view, small.render, small_derived.cells, small.output.channels,
+                                  "f64").render(reference)[..., 1]
+    out = {}
+    for label, storage in (("f32", torch.float32), ("bf16", torch.bfloat16), ("f16", torch.float16)):
+        d = recipe.domain
+        grid = make_grid(derived, d.cell_m, d.faces, d.ambient_k, device, storage=storage)
+        for name, values in fields.items():
+            getattr(grid, name).data.copy_(torch.from_numpy(values))
+        stepper = Stepper(grid, recipe)
+        for n in range(3):
+            stepper.step(n * derived.dt_s, derived.dt_s)
+        start, end = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        start.record()
+        for n in range(steps):
+            stepper.step((3 + n) * derived.dt_s, derived.dt_s)
+        end.record()
+        torch.cuda.synchronize()
+        value = math.prod(derived.cells) * steps / (start.elapsed_time(end) / 1e3) / 1e6
+        del grid, stepper
+        g = make_grid(small_derived, sd.cell_m, sd.faces, sd.ambient_k, device, storage=storage)
+        for name, values in small_fields.items():
+            getattr(g, name).data.copy_(torch.from_numpy(values))
+        st = Stepper(g, small)
+        for n in range(4):
+            st.step(n * small_derived.dt_s, small_derived.dt_s)
+        field_error = max(float(np.abs(getattr(g, n).data.float().cpu().numpy() - getattr(reference, n).data).max()
+                                / np.abs(getattr(reference, n).data).max())
+                          for n in ("u", "v", "w", "smoke", "temperature"))
+        frame = FrameRenderer(view, small.render, small_derived.cells, small.output.channels, device).render(g)
+        out[label] = {"value": value, "unit": METRIC, "steps": steps,
+                      "field_error_vs_fp64": field_error,
+                      "thickness_error_vs_fp64": float(np.abs(frame[..., 1] - thickness64).max())}
+    return out
+
+
+def batched_variant(device: str, count: int = 32, frames: int = 24) -> dict:
+    """Uneven recipes (grids 48^3 to 160x240x160, sweep of emitter, buoyancy, drag and confinement) run one
+    after another through simulate_frames, then all at once on per-instance streams; Mcell-substeps/s of each
+    (whole runs, timed on the host around device-synchronised runs)."""
+    import torch
+
+    from plume_b200.sim.batch import Batch, run_one_at_a_time
+    from plume_b200.workloads import batched_recipes
+
+    recipes = batched_recipes(count=count, frames=frames)
+    result = {}
+    for arm in ("one_at_a_time", "batched"):
+        torch.cuda.synchronize()
+        start = time.perf_counter()
+        logs = run_one_at_a_time(recipes, device) if arm == "one_at_a_time" else Batch(recipes, device).run()
+        torch.cuda.synchronize()
+        elapsed = time.perf_counter() - start
+        from plume_b200.recipe.derived import derive
+
+        work = sum(math.prod(derive(r).cells) * log.total_steps for r, log in zip(recipes, logs))
+        result[arm] = work / elapsed / 1e6
+        torch.cuda.empty_cache()
+    return {"instances": count, "frames": frames, "unit": METRIC, "value": result["batched"],
+            "one_at_a_time": result["one_at_a_time"], "ratio": result["batched"] / result["one_at_a_time"]}
 
 
 def run_reference(args, cells):
@@ -333,6 +422,9 @@ def main():
         "gpu_launches": launches,
         "clocks": clocks.summary(),
     }
+    if not args.no_variants:
+        line["variants"] = {"storage": storage_variants(recipe, derived, fields, args.steps, device),
+                            "batched": batched_variant(device)}
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         line["cpu_baseline"] = cpu_baseline(recipe, derived, fields)
     if rank == 0:

@@ -1,0 +1,345 @@
+// The adjoint (reverse-mode derivative) of the smoke path of the fluid step and of the thickness render, for
+// fitting a smoke source field to a target thickness image. The smoke path is: a source field added to the
+// smoke, MacCormack advection of the smoke by a given velocity (advect.py:59-68), the smoke budget's rescale
+// (conserve.py:45-52) and dissipation (dissipate.py:10-15); the render is the ray march's thickness channel
+// (raymarch.py:86-140). With the velocity independent of the smoke (no smoke weight in the buoyancy), these
+// are exactly the operators a smoke source field acts through, so the derivative is the loss's gradient.
+//
+// Each adjoint kernel recomputes its forward pass's traces and branches and then transposes it:
+//   - a trilinear sample becomes a scatter of the incoming derivative to its eight corners with the same
+//     weights (atomic adds: several samples share a corner);
+//   - MacCormack's clamp passes the derivative to the clamped value's corner (the first of equal corners in the
+//     reference's min/max order) when it clamps, else through the correction hat + (data - back) / 2;
+//   - the smoke budget's factor is a function of three totals, which adds uniform terms to the data, hat and
+//     next derivatives;
+//   - the march's thickness 1 - prod(exp(-k rho_s ds)) has d thickness / d rho_s = k ds * transmittance for every
+//     sample with rho_s > 0.
+#include <cstdint>
+
+#include "common.cuh"
+
+namespace plume {
+
+constexpr int ADJ_THREADS = 256;
+static int adj_blocks(long n) { return (int)((n + ADJ_THREADS - 1) / ADJ_THREADS); }
+
+// The eight corners and weights of sample_index_space at g (sim/sample.py:10-29), in the reference's corner
+// order (x fastest within (y, z) pairs as the lerps pair them).
+struct Corners {
+  int idx[8];
+  float w[8];
+};
+
+__device__ __forceinline__ Corners corners_of(const Dims& d, F3 g) {
+  const Axis1 x = axis_of(g[0], d.n0, d.n1 * d.n2), y = axis_of(g[1], d.n1, d.n2), z = axis_of(g[2], d.n2, 1);
+  const int base = (x.i0 * d.n1 + y.i0) * d.n2 + z.i0;
+  Corners c;
+  // c00 = lerp(a000, a100, tx), c10 = lerp(a010, a110), c01 = lerp(a001, a101), c11 = lerp(a011, a111);
+  // result = lerp(lerp(c00, c10, ty), lerp(c01, c11, ty), tz)
+  const float wx[2] = {x.one_minus_t, x.t}, wy[2] = {y.one_minus_t, y.t}, wz[2] = {z.one_minus_t, z.t};
+  const int sx[2] = {0, x.step}, sy[2] = {0, y.step}, sz[2] = {0, z.step};
+  int n = 0;
+  for (int kz = 0; kz < 2; ++kz)
+    for (int ky = 0; ky < 2; ++ky)
+      for (int kx = 0; kx < 2; ++kx) {
+        c.idx[n] = base + sx[kx] + sy[ky] + sz[kz];
+        c.w[n] = (wx[kx] * wy[ky]) * wz[kz];
+        ++n;
+      }
+  return c;
+}
+
+__device__ __forceinline__ void scatter(float* __restrict__ target, const Corners& c, float value) {
+  if (value == 0.0f) return;
+#pragma unroll
+  for (int n = 0; n < 8; ++n)
+    if (c.w[n] != 0.0f) atomicAdd(target + c.idx[n], c.w[n] * value);
+}
+
+// The clamp range of the forward sample and the corner each bound came from (sample.py:32-50: the min and max
+// run over a000, a001, a010, a011, a100, a101, a110, a111; a tie keeps the earlier corner).
+__device__ __forceinline__ void range_corners(const float* __restrict__ f, const Dims& d, F3 g, int& lo_idx,
+                                              int& hi_idx, float& lo, float& hi) {
+  const Axis1 x = axis_of(g[0], d.n0, d.n1 * d.n2), y = axis_of(g[1], d.n1, d.n2), z = axis_of(g[2], d.n2, 1);
+  const int base = (x.i0 * d.n1 + y.i0) * d.n2 + z.i0;
+  const int order[8] = {base,
+                        base + z.step,
+                        base + y.step,
+                        base + y.step + z.step,
+                        base + x.step,
+                        base + x.step + z.step,
+                        base + x.step + y.step,
+                        base + x.step + y.step + z.step};
+  lo = hi = __ldg(f + order[0]);
+  lo_idx = hi_idx = order[0];
+#pragma unroll
+  for (int n = 1; n < 8; ++n) {
+    const float v = __ldg(f + order[n]);
+    if (v < lo) {
+      lo = v;
+      lo_idx = order[n];
+    }
+    if (v > hi) {
+      hi = v;
+      hi_idx = order[n];
+    }
+  }
+}
+
+// smoke[corner + (i, j, k)] += scale * source[i, j, k] inside the grid.
+__global__ void k_add_source(float* __restrict__ smoke, Dims d, const float* __restrict__ source, Dims s, int3 corner,
+                             float scale) {
+  const long idx = (long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (idx >= (long)s.n0 * s.n1 * s.n2) return;
+  const int k = (int)(idx % s.n2), j = (int)((idx / s.n2) % s.n1), i = (int)(idx / ((long)s.n1 * s.n2));
+  const int gi = corner.x + i, gj = corner.y + j, gk = corner.z + k;
+  if (gi < 0 || gj < 0 || gk < 0 || gi >= d.n0 || gj >= d.n1 || gk >= d.n2) return;
+  const int c = at(d, gi, gj, gk);
+  smoke[c] = smoke[c] + scale * source[idx];
+}
+
+// grad[i, j, k] += scale * a_smoke[corner + (i, j, k)] (the adjoint of k_add_source for its source).
+__global__ void k_source_grad(const float* __restrict__ a_smoke, Dims d, float* __restrict__ grad, Dims s,
+                              int3 corner, float scale) {
+  const long idx = (long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (idx >= (long)s.n0 * s.n1 * s.n2) return;
+  const int k = (int)(idx % s.n2), j = (int)((idx / s.n2) % s.n1), i = (int)(idx / ((long)s.n1 * s.n2));
+  const int gi = corner.x + i, gj = corner.y + j, gk = corner.z + k;
+  if (gi < 0 || gj < 0 || gk < 0 || gi >= d.n0 || gj >= d.n1 || gk >= d.n2) return;
+  grad[idx] = grad[idx] + scale * a_smoke[at(d, gi, gj, gk)];
+}
+
+// MacCormack adjoint, part 1 (per cell of the advected cell-centred field): the clamp's branch, the correction's
+// own terms, and the backward sample's transpose into a_hat. a_data and a_hat must start as the derivatives
+// already known for them (atomically accumulated).
+__global__ void k_mac_adjoint_correct(PlumeGridInfo info, Vel vel, const float* __restrict__ data,
+                                      const float* __restrict__ hat, const float* __restrict__ a_next,
+                                      float* __restrict__ a_data, float* __restrict__ a_hat, float dt_over_cell,
+                                      float outside) {
+  const int i = blockIdx.z, j = blockIdx.y * blockDim.y + threadIdx.y, k = blockIdx.x * blockDim.x + threadIdx.x;
+  const Dims d = dims_of(info);
+  if (j >= d.n1 || k >= d.n2) return;
+  const int c = at(d, i, j, k);
+  const float g_next = a_next[c];
+  if (g_next == 0.0f) return;
+  const F3 offset = f3(0.5f, 0.5f, 0.5f);
+  const F3 p = add3(f3((float)i, (float)j, (float)k), offset);
+  const F3 vp = velocity_at_node(vel, p);
+  const F3 src = trace_from(vel, p, vp, dt_over_cell);
+  const F3 back_src = trace_from(vel, p, vp, -dt_over_cell);
+  const bool src_outside = is_outside_open_face(src, info);
+  const bool back_outside = is_outside_open_face(back_src, info);
+  const F3 gb = sub3(back_src, offset);
+  const float back = back_outside ? outside : sample_index_space(hat, d, gb);
+  const float corrected = __ldg(hat + c) + 0.5f * (__ldg(data + c) - back);
+  float lo = outside, hi = outside;
+  int lo_idx = -1, hi_idx = -1;
+  if (!src_outside) range_corners(data, d, sub3(src, offset), lo_idx, hi_idx, lo, hi);
+  if (corrected < lo) {  // clampf_: x < lo ? lo : (x > hi ? hi : x)
+    if (lo_idx >= 0) atomicAdd(a_data + lo_idx, g_next);
+    return;
+  }
+  if (corrected > hi) {
+    if (hi_idx >= 0) atomicAdd(a_data + hi_idx, g_next);
+    return;
+  }
+  atomicAdd(a_hat + c, g_next);
+  atomicAdd(a_data + c, 0.5f * g_next);
+  if (!back_outside) scatter(a_hat, corners_of(d, gb), -0.5f * g_next);
+}
+
+// MacCormack adjoint, part 2: the forward sample's transpose, a_data += sample^T(a_hat).
+__global__ void k_mac_adjoint_forward(PlumeGridInfo info, Vel vel, const float* __restrict__ a_hat,
+                                      float* __restrict__ a_data, float dt_over_cell) {
+  const int i = blockIdx.z, j = blockIdx.y * blockDim.y + threadIdx.y, k = blockIdx.x * blockDim.x + threadIdx.x;
+  const Dims d = dims_of(info);
+  if (j >= d.n1 || k >= d.n2) return;
+  const float g = a_hat[at(d, i, j, k)];
+  if (g == 0.0f) return;
+  const F3 offset = f3(0.5f, 0.5f, 0.5f);
+  const F3 p = add3(f3((float)i, (float)j, (float)k), offset);
+  const F3 src = trace_from(vel, p, velocity_at_node(vel, p), dt_over_cell);
+  if (is_outside_open_face(src, info)) return;
+  scatter(a_data, corners_of(d, sub3(src, offset)), g);
+}
+
+// sum_i a[i] * b[i] in double, per block of ADJ_THREADS, then the blocks in order on one thread.
+__global__ void k_dot_partials(const float* __restrict__ a, const float* __restrict__ b, long n, double* __restrict__ partial) {
+  __shared__ double slot[ADJ_THREADS];
+  double value = 0.0;
+  for (long i = (long)blockIdx.x * ADJ_THREADS + threadIdx.x; i < n; i += (long)gridDim.x * ADJ_THREADS)
+    value = value + (double)a[i] * (double)b[i];
+  slot[threadIdx.x] = value;
+  __syncthreads();
+  for (int h = ADJ_THREADS / 2; h >= 1; h >>= 1) {
+    if ((int)threadIdx.x < h) slot[threadIdx.x] = slot[threadIdx.x] + slot[threadIdx.x + h];
+    __syncthreads();
+  }
+  if (threadIdx.x == 0) partial[blockIdx.x] = slot[0];
+}
+
+// The smoke budget's adjoint coefficients from its three totals (before, semi-Lagrangian, MacCormack) and
+// G = sum a_out * next (next before scaling): factor = held / mc with held = max(sl, min(mc, before)); the
+// derivatives of the scaled output add uniform terms c_data to a_data, c_hat to a_hat and c_next to a_next.
+// coeffs = {factor, c_data, c_hat, c_next}.
+__global__ void k_budget_adjoint_coeffs(const double* __restrict__ totals, const double* __restrict__ partial, int blocks,
+                                        double* __restrict__ coeffs) {
+  if (threadIdx.x != 0 || blockIdx.x != 0) return;
+  double g = 0.0;
+  for (int b = 0; b < blocks; ++b) g = g + partial[b];
+  const double before = totals[0], sl = totals[1], mc = totals[2];
+  double factor = 1.0, c_data = 0.0, c_hat = 0.0, c_next = 0.0;
+  if (mc > 0.0) {
+    const double inner = mc < before ? mc : before;
+    const double held = sl > inner ? sl : inner;
+    factor = (double)(float)(held / mc);
+    if (sl > inner) {  // held = sl
+      c_hat = g / mc;
+      c_next = -g * sl / (mc * mc);
+    } else if (!(mc < before)) {  // held = before
+      c_data = g / mc;
+      c_next = -g * before / (mc * mc);
+    }  // held = mc: factor is 1 around here
+  }
+  coeffs[0] = factor;
+  coeffs[1] = c_data;
+  coeffs[2] = c_hat;
+  coeffs[3] = c_next;
+}
+
+// a_next_pre = keep * factor * a_out + keep * c_next (a_out: derivative of the dissipated, scaled smoke);
+// a_data += c_data; a_hat = c_hat (a_hat starts here). Dissipation's keep enters as a_out * keep.
+__global__ void k_budget_adjoint_apply(const float* __restrict__ a_out, long n, const double* __restrict__ coeffs,
+                                       float keep, float* __restrict__ a_next, float* __restrict__ a_data,
+                                       float* __restrict__ a_hat) {
+  const double factor = coeffs[0], c_data = coeffs[1], c_hat = coeffs[2], c_next = coeffs[3];
+  for (long i = (long)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (long)gridDim.x * blockDim.x) {
+    const double a = (double)a_out[i] * (double)keep;
+    a_next[i] = (float)(a * factor + c_next * (double)keep);
+    a_data[i] = (float)c_data * keep;
+    a_hat[i] = (float)c_hat * keep;
+  }
+}
+
+// The ortho thickness march (raymarch.py:86-140, thickness channel only) and its adjoint for
+// loss = sum over pixels (thickness - target)^2: writes thickness, adds the pixel's squared error to *loss and
+// scatters d loss / d smoke into a_smoke.
+__global__ void k_thickness_adjoint(PlumeGridInfo info, PlumeViewParams view, float opacity,
+                                    const float* __restrict__ smoke, const float* __restrict__ target, int height,
+                                    int width, float* __restrict__ thickness_out, double* __restrict__ loss,
+                                    float* __restrict__ a_smoke) {
+  const int px = blockIdx.x * blockDim.x + threadIdx.x, py = blockIdx.y * blockDim.y + threadIdx.y;
+  if (px >= width || py >= height) return;
+  const Dims d = dims_of(info);
+  const F3 right = f3(view.right[0], view.right[1], view.right[2]);
+  const F3 up = f3(view.up[0], view.up[1], view.up[2]);
+  const F3 toward = f3(view.toward[0], view.toward[1], view.toward[2]);
+  const float plane_x = view.left_m + ((float)px + 0.5f) * view.pixel_m;
+  const float plane_y = view.top_m - ((float)py + 0.5f) * view.pixel_m;
+  const F3 origin = add3(add3(mul3(right, plane_x), mul3(up, plane_y)), mul3(toward, 1.0e4f));
+  const F3 direction = f3(-toward[0], -toward[1], -toward[2]);
+  const F3 box_origin = f3(info.origin_m[0], info.origin_m[1], info.origin_m[2]);
+  const F3 box_max = add3(box_origin, mul3(f3((float)d.n0, (float)d.n1, (float)d.n2), info.cell_m));
+  float t_enter = -1.0e30f, t_exit = 1.0e30f;
+  bool miss = false;
+  for (int a = 0; a < 3; ++a) {  // slab_range (raymarch.py:55-69)
+    if (fabsf(direction[a]) < 1.0e-12f) {
+      if (origin[a] < box_origin[a] || origin[a] > box_max[a]) miss = true;
+    } else {
+      const float t0 = (box_origin[a] - origin[a]) / direction[a], t1 = (box_max[a] - origin[a]) / direction[a];
+      t_enter = fmax_(t_enter, fmin_(t0, t1));
+      t_exit = fmin_(t_exit, fmax_(t0, t1));
+    }
+  }
+  float tr = 1.0f;
+  int steps = 0;
+  float step_m = 0.0f;
+  if (!miss && t_exit > t_enter) {
+    const float length = t_exit - t_enter;
+    steps = (int)ceilf(length / (0.5f * info.cell_m));
+    step_m = length / (float)steps;
+    for (int s = 0; s < steps; ++s) {
+      const F3 position = add3(origin, mul3(direction, t_enter + ((float)s + 0.5f) * step_m));
+      const F3 g = sub3(div3(sub3(position, box_origin), info.cell_m), f3(0.5f, 0.5f, 0.5f));
+      const float density = fmax_(sample_index_space(smoke, d, g), 0.0f);
+      if (density > 0.0f) tr = tr * (1.0f - (1.0f - exp_f(-opacity * density * step_m)));
+    }
+  }
+  const float thickness = 1.0f - tr;
+  const long pixel = (long)py * width + px;
+  thickness_out[pixel] = thickness;
+  const float error = thickness - target[pixel];
+  atomicAdd(loss, (double)error * (double)error);
+  const float a_rho = 2.0f * error * opacity * step_m * tr;
+  if (a_rho == 0.0f) return;
+  for (int s = 0; s < steps; ++s) {
+    const F3 position = add3(origin, mul3(direction, t_enter + ((float)s + 0.5f) * step_m));
+    const F3 g = sub3(div3(sub3(position, box_origin), info.cell_m), f3(0.5f, 0.5f, 0.5f));
+    if (sample_index_space(smoke, d, g) > 0.0f) scatter(a_smoke, corners_of(d, g), a_rho);
+  }
+}
+
+}  // namespace plume
+
+using namespace plume;
+
+#define ADJ_CHECK(cond, what) \
+  do {                        \
+    if (!(cond)) return fail(PLUME_ERR_INVALID, "%s", what); \
+  } while (0)
+
+extern "C" int plume_add_source(float* smoke, const int32_t shape[3], const float* source, const int32_t source_shape[3],
+                                const int32_t corner[3], float scale, void* stream) {
+  ADJ_CHECK(smoke && shape && source && source_shape && corner, "add_source: null argument");
+  const Dims s{source_shape[0], source_shape[1], source_shape[2]};
+  k_add_source<<<adj_blocks((long)s.n0 * s.n1 * s.n2), ADJ_THREADS, 0, as_stream(stream)>>>(
+      smoke, Dims{shape[0], shape[1], shape[2]}, source, s, make_int3(corner[0], corner[1], corner[2]), scale);
+  return launch_status("add source");
+}
+
+extern "C" int plume_source_grad(const float* a_smoke, const int32_t shape[3], float* grad, const int32_t source_shape[3],
+                                 const int32_t corner[3], float scale, void* stream) {
+  ADJ_CHECK(a_smoke && shape && grad && source_shape && corner, "source_grad: null argument");
+  const Dims s{source_shape[0], source_shape[1], source_shape[2]};
+  k_source_grad<<<adj_blocks((long)s.n0 * s.n1 * s.n2), ADJ_THREADS, 0, as_stream(stream)>>>(
+      a_smoke, Dims{shape[0], shape[1], shape[2]}, grad, s, make_int3(corner[0], corner[1], corner[2]), scale);
+  return launch_status("source gradient");
+}
+
+extern "C" int plume_smoke_adjoint(const PlumeGridInfo* info, const float* u, const float* v, const float* w,
+                                   const float* data, const float* hat, const float* next_pre, const double* totals,
+                                   float dt_over_cell, float keep, const float* a_out, float* a_next, float* a_hat,
+                                   float* a_data, double* partial, double* coeffs, void* stream) {
+  ADJ_CHECK(info && u && v && w && data && hat && next_pre && totals && a_out && a_next && a_hat && a_data && partial &&
+                coeffs && a_data != a_out,
+            "smoke_adjoint: bad argument");
+  cudaStream_t st = as_stream(stream);
+  const Dims d = dims_of(*info);
+  const long n = (long)d.n0 * d.n1 * d.n2;
+  const int blocks = (int)std::min<long>(adj_blocks(n), 1024);
+  k_dot_partials<<<blocks, ADJ_THREADS, 0, st>>>(a_out, next_pre, n, partial);
+  int status = launch_status("adjoint dot");
+  if (status != PLUME_OK) return status;
+  k_budget_adjoint_coeffs<<<1, 32, 0, st>>>(totals, partial, blocks, coeffs);
+  if ((status = launch_status("budget adjoint coefficients")) != PLUME_OK) return status;
+  k_budget_adjoint_apply<<<blocks, ADJ_THREADS, 0, st>>>(a_out, n, coeffs, keep, a_next, a_data, a_hat);
+  if ((status = launch_status("budget adjoint")) != PLUME_OK) return status;
+  const Vel vel = make_vel(u, v, w, info->dims);
+  k_mac_adjoint_correct<<<cell_grid(d.n0, d.n1, d.n2), cell_block(), 0, st>>>(*info, vel, data, hat, a_next, a_data, a_hat,
+                                                                              dt_over_cell, 0.0f);
+  if ((status = launch_status("MacCormack adjoint (correction)")) != PLUME_OK) return status;
+  k_mac_adjoint_forward<<<cell_grid(d.n0, d.n1, d.n2), cell_block(), 0, st>>>(*info, vel, a_hat, a_data, dt_over_cell);
+  return launch_status("MacCormack adjoint (forward sample)");
+}
+
+extern "C" int plume_thickness_adjoint(const PlumeGridInfo* info, const PlumeViewParams* view, float opacity,
+                                       const float* smoke, const float* target, int32_t height, int32_t width,
+                                       float* thickness, double* loss, float* a_smoke, void* stream) {
+  ADJ_CHECK(info && view && smoke && target && thickness && loss && a_smoke && height >= 1 && width >= 1 &&
+                view->perspective == 0,
+            "thickness_adjoint: bad argument (orthographic views only)");
+  dim3 block(16, 16), grid((width + 15) / 16, (height + 15) / 16);
+  k_thickness_adjoint<<<grid, block, 0, as_stream(stream)>>>(*info, *view, opacity, smoke, target, height, width,
+                                                             thickness, loss, a_smoke);
+  return launch_status("thickness adjoint");
+}

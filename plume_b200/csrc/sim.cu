@@ -433,41 +433,6 @@ __device__ __forceinline__ int pick_field(const FieldSet<T>& set, int& slab) {
   return which;
 }
 
-// Trilinear sample that skips the corners whose weight is exactly 0 (sample.py:10-29 otherwise unchanged).
-template <class T>
-__device__ __forceinline__ float sample_sparse(const T* __restrict__ f, const Dims& d, F3 g) {
-  float x = clampf_(g[0], 0.0f, (float)(d.n0 - 1));
-  float y = clampf_(g[1], 0.0f, (float)(d.n1 - 1));
-  float z = clampf_(g[2], 0.0f, (float)(d.n2 - 1));
-  const int i0 = (int)x, j0 = (int)y, k0 = (int)z;
-  const int i1 = imin_(i0 + 1, d.n0 - 1), j1 = imin_(j0 + 1, d.n1 - 1), k1 = imin_(k0 + 1, d.n2 - 1);
-  const float tx = x - (float)i0, ty = y - (float)j0, tz = z - (float)k0;
-  auto along_x = [&](int j, int k) {
-    const float a = ldg_f(f + at(d, i0, j, k));
-    return tx == 0.0f ? a : lerpf_(a, ldg_f(f + at(d, i1, j, k)), tx);
-  };
-  const float c00 = along_x(j0, k0);
-  const float y0 = ty == 0.0f ? c00 : lerpf_(c00, along_x(j1, k0), ty);
-  if (tz == 0.0f) return y0;
-  const float c01 = along_x(j0, k1);
-  const float y1 = ty == 0.0f ? c01 : lerpf_(c01, along_x(j1, k1), ty);
-  return lerpf_(y0, y1, tz);
-}
-
-template <class T>
-__device__ __forceinline__ F3 velocity_at_node(const VelT<T>& vel, F3 p) {  // velocity_at (sample.py:74-82) at p
-  return f3(sample_sparse(vel.u, vel.du, sub3(p, f3(0.0f, 0.5f, 0.5f))),
-            sample_sparse(vel.v, vel.dv, sub3(p, f3(0.5f, 0.0f, 0.5f))),
-            sample_sparse(vel.w, vel.dw, sub3(p, f3(0.5f, 0.5f, 0.0f))));
-}
-
-// trace (advect.py:16-21) given the velocity at p.
-template <class T>
-__device__ __forceinline__ F3 trace_from(const VelT<T>& vel, F3 p, F3 vp, float dt_over_cell) {
-  F3 mid = sub3(p, mul3(vp, 0.5f * dt_over_cell));
-  return sub3(p, mul3(velocity_at(vel, mid), dt_over_cell));
-}
-
 // semi_lagrangian_kernel (advect.py:24-31): the forward pass into `hat` (or, for plain semi-Lagrangian
 // advection, into `next`).
 template <class T>
