@@ -37,8 +37,8 @@ PHASE_BYTES = {"forces": 32.0, "velocity advection": 24.0, "divergence": 16.0, "
                "gradient": 28.0, "scalar advection": 44.0}
 MG_BYTES_PER_CYCLE = 74.0
 # DRAM bytes (read + write) per top-level cell per V-cycle that ncu counted for the pressure-solve kernels of
-# the 128x192x128 step (1099.9 MB per substep at 4 cycles); the solve's traffic scales with the level cells.
-MG_TRAFFIC_PER_CYCLE = 1099.9e6 / (128 * 192 * 128) / 4
+# the 128x192x128 step (965.7 MB per substep at 4 cycles); the solve's traffic scales with the level cells.
+MG_TRAFFIC_PER_CYCLE = 965.7e6 / (128 * 192 * 128) / 4
 
 
 def parse_args():
@@ -228,6 +228,41 @@ def batched_variant(device: str, count: int = 32, frames: int = 24) -> dict:
         torch.cuda.empty_cache()
     return {"instances": count, "frames": frames, "unit": METRIC, "value": result["batched"],
             "one_at_a_time": result["one_at_a_time"], "ratio": result["batched"] / result["one_at_a_time"]}
+
+
+def adjoint_variant(device: str) -> dict:
+    """The differentiable step's cost: a 96 x 144 x 96 smoke puff (forces.smoke_weight 0), a 16^3 source field
+    with its corner at cell (40, 0, 40) (centred on (48, 8, 48)), 64 substeps with a checkpoint every 8; the
+    forward run (recording the tape) against the backward pass (recomputing each segment's smoke path, then
+    the adjoint), per substep, timed on the host around device-synchronised runs."""
+    import dataclasses
+
+    import numpy as np
+    import torch
+
+    from plume_b200.adjoint import SourceFit
+    from plume_b200.workloads import plain_step_recipe
+
+    recipe = plain_step_recipe((96, 144, 96), cycles=4, frames=32, substeps=2)
+    recipe = dataclasses.replace(recipe, forces=dataclasses.replace(recipe.forces, smoke_weight=0.0))
+    substeps = 64
+    fit = SourceFit(recipe, (16, 16, 16), (40, 0, 40), substeps, device, checkpoint_every=8)
+    source = torch.from_numpy(np.random.default_rng(3).uniform(0.0, 1.0, (16, 16, 16)).astype(np.float32)).to(device)
+    target = torch.zeros((fit.view.height_px, fit.view.width_px), dtype=torch.float32, device=device)
+    fit.loss_and_grad(source, target)  # warm-up: graph captures, allocations
+    torch.cuda.synchronize()
+    start = time.perf_counter()
+    fit.forward(source)
+    torch.cuda.synchronize()
+    forward = time.perf_counter() - start
+    start = time.perf_counter()
+    fit.loss_and_grad(source, target)
+    torch.cuda.synchronize()
+    total = time.perf_counter() - start
+    backward = total - forward
+    return {"cells": [96, 144, 96], "substeps": substeps, "checkpoint_every": 8,
+            "forward_ms_per_substep": forward * 1e3 / substeps, "adjoint_ms_per_substep": backward * 1e3 / substeps,
+            "adjoint_over_forward": backward / forward}
 
 
 def run_reference(args, cells):
@@ -424,7 +459,7 @@ def main():
     }
     if not args.no_variants:
         line["variants"] = {"storage": storage_variants(recipe, derived, fields, args.steps, device),
-                            "batched": batched_variant(device)}
+                            "batched": batched_variant(device), "adjoint": adjoint_variant(device)}
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         line["cpu_baseline"] = cpu_baseline(recipe, derived, fields)
     if rank == 0:

@@ -385,6 +385,35 @@ int plume_view_boundary_layers(const float* smoke, const int32_t shape[3], float
 int plume_view_narrow(const float* src, void* dst, long long count, void* stream);
 int plume_view_widen(const void* src, float* dst, long long count, void* stream);
 
+/* ---- the smoke path's adjoint (no counterpart in the reference, which has no derivatives) ------------------ */
+/* For fitting a smoke source field to a target thickness image: the derivative of a thickness loss through the
+ * smoke path of the step (source add, MacCormack advection by a given velocity, smoke budget, dissipation) and
+ * the thickness march. Exact when the velocity does not depend on the smoke (forces.smoke_weight = 0). */
+
+/* smoke[corner + idx] += scale * source[idx] over the source box's cells inside the grid (a source field). */
+int plume_add_source(float* smoke, const int32_t shape[3], const float* source, const int32_t source_shape[3],
+                     const int32_t corner[3], float scale, void* stream);
+
+/* grad[idx] += scale * a_smoke[corner + idx]: the source field's share of a smoke derivative. */
+int plume_source_grad(const float* a_smoke, const int32_t shape[3], float* grad, const int32_t source_shape[3],
+                      const int32_t corner[3], float scale, void* stream);
+
+/* One substep of the smoke path backwards. Inputs: the velocity the smoke was advected by, the advected smoke
+ * `data`, its forward pass `hat` and correction `next_pre` (before the budget's scale), the budget's totals
+ * (before, semi-Lagrangian, MacCormack; 3 device doubles), dissipation's keep factor, and a_out = the derivative
+ * with respect to the substep's output smoke. Writes a_data = the derivative with respect to `data`; a_next,
+ * a_hat are scratch of the field's size, partial >= 1024 doubles, coeffs 4 doubles. */
+int plume_smoke_adjoint(const PlumeGridInfo* info, const float* u, const float* v, const float* w, const float* data,
+                        const float* hat, const float* next_pre, const double* totals, float dt_over_cell, float keep,
+                        const float* a_out, float* a_next, float* a_hat, float* a_data, double* partial,
+                        double* coeffs, void* stream);
+
+/* The orthographic march's thickness (raymarch.py:86-140) of `smoke` for `view`, written to thickness
+ * (height, width); *loss += sum (thickness - target)^2; a_smoke += d loss / d smoke. */
+int plume_thickness_adjoint(const PlumeGridInfo* info, const PlumeViewParams* view, float opacity, const float* smoke,
+                            const float* target, int32_t height, int32_t width, float* thickness, double* loss,
+                            float* a_smoke, void* stream);
+
 #ifdef __cplusplus
 }
 #endif

@@ -389,8 +389,11 @@ def dissipate(grid: Grid, smoke_per_s, cooling_per_s, ambient_k, dt) -> None:
 
 
 class Stepper:
-    def __init__(self, grid: Grid, recipe):
+    def __init__(self, grid: Grid, recipe, before_step=None):
+        """`before_step(grid, time_s, dt)`, when given, runs at the start of every substep (a test's source
+        field, added before the emitters)."""
         self.grid, self.recipe = grid, recipe
+        self.before_step = before_step
         self.emitters = emitter_params(recipe.emitter)
         self.pressure_solve = make_pressure_solve(grid, recipe.solver)
         self.smoke_budget = SmokeBudget(grid)
@@ -399,6 +402,8 @@ class Stepper:
     def step(self, time_s: float, dt: float) -> None:
         grid, recipe = self.grid, self.recipe
         ambient = recipe.domain.ambient_k
+        if self.before_step is not None:
+            self.before_step(grid, time_s, dt)
         emit(grid, self.emitters, recipe.seed, time_s, dt)
         f = recipe.forces
         apply_buoyancy(grid, f.gravity_mps2, f.heat_buoyancy, f.smoke_weight, ambient, dt)

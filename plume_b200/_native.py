@@ -146,6 +146,10 @@ SIGNATURES = {
     "plume_view_boundary_layers": [_P, _SHAPE, _P, _P],
     "plume_view_narrow": [_P, _P, ctypes.c_longlong, _P],
     "plume_view_widen": [_P, _P, ctypes.c_longlong, _P],
+    "plume_add_source": [_P, _SHAPE, _P, _SHAPE, _SHAPE, _F, _P],
+    "plume_source_grad": [_P, _SHAPE, _P, _SHAPE, _SHAPE, _F, _P],
+    "plume_smoke_adjoint": [_INFO, _P, _P, _P, _P, _P, _P, _P, _F, _F, _P, _P, _P, _P, _P, _P, _P],
+    "plume_thickness_adjoint": [_INFO, ctypes.POINTER(PlumeViewParams), _F, _P, _P, _I, _I, _P, _P, _P, _P],
 }
 
 _lib = None

@@ -15,7 +15,7 @@ from pathlib import Path
 PACKAGE = Path(__file__).resolve().parent
 REPO = PACKAGE.parent
 SOURCES = [PACKAGE / "csrc" / "sim.cu", PACKAGE / "csrc" / "multigrid.cu", PACKAGE / "csrc" / "render.cu",
-           PACKAGE / "csrc" / "sheet.cu", PACKAGE / "csrc" / "view.cu"]
+           PACKAGE / "csrc" / "sheet.cu", PACKAGE / "csrc" / "view.cu", PACKAGE / "csrc" / "adjoint.cu"]
 HEADERS = [PACKAGE / "csrc" / "common.cuh", PACKAGE / "csrc" / "poisson.cuh", REPO / "include" / "plume_b200.h"]
 LIBRARY = PACKAGE / "libplume_b200.so"
 NVCC_FLAGS = ["-O3", "-std=c++17", "-gencode", "arch=compute_100a,code=sm_100a", "-lineinfo", "-fmad=false",

@@ -14,6 +14,7 @@
 //     next derivatives;
 //   - the march's thickness 1 - prod(exp(-k rho_s ds)) has d thickness / d rho_s = k ds * transmittance for every
 //     sample with rho_s > 0.
+#include <algorithm>
 #include <cstdint>
 
 #include "common.cuh"

@@ -1,0 +1,108 @@
+"""The source-field adjoint: its loss is the FP64 oracle's for the same model (within 1e-4 relative), its
+thickness is the renderer's, and its gradient agrees with central finite differences of the FP64 oracle's loss
+(h = 1e-3) to 1e-3 of the gradient's scale, on voxels across the source box."""
+
+import dataclasses
+
+import numpy as np
+import pytest
+
+from oracle import oracle as O
+from plume_b200.recipe.derived import derive
+from plume_b200.workloads import plain_step_recipe
+
+pytestmark = pytest.mark.gpu
+
+CELLS = (24, 32, 24)
+SOURCE = (6, 6, 6)
+CORNER = (9, 3, 9)
+SUBSTEPS = 12
+FD_H = 1e-3
+GRAD_RTOL = 1e-3
+
+
+def adjoint_recipe():
+    recipe = plain_step_recipe(CELLS, cycles=4, frames=4, substeps=3)
+    forces = dataclasses.replace(recipe.forces, smoke_weight=0.0)
+    return dataclasses.replace(recipe, forces=forces,
+                               dissipation=dataclasses.replace(recipe.dissipation, smoke_per_s=0.4, cooling_per_s=0.2))
+
+
+def oracle_loss(recipe, source, target) -> float:
+    derived = derive(recipe)
+    d = recipe.domain
+
+    def add(grid, time_s, dt):
+        box = grid.smoke.data[CORNER[0]:CORNER[0] + SOURCE[0], CORNER[1]:CORNER[1] + SOURCE[1],
+                              CORNER[2]:CORNER[2] + SOURCE[2]]
+        box += source * dt
+
+    grid = O.make_grid(derived, d.cell_m, d.faces, d.ambient_k, "f64")
+    stepper = O.Stepper(grid, recipe, before_step=add)
+    for n in range(SUBSTEPS):
+        stepper.step(n * derived.dt_s, derived.dt_s)
+    from plume_b200.render.camera import sheet_domain_view
+
+    view = sheet_domain_view(recipe, derived)
+    thickness = O.FrameRenderer(view, recipe.render, derived.cells, recipe.output.channels, "f64").render(grid)[..., 1]
+    return float(((thickness - target) ** 2).sum()), thickness
+
+
+@pytest.fixture(scope="module")
+def case():
+    import torch
+
+    from plume_b200.adjoint import SourceFit
+
+    recipe = adjoint_recipe()
+    rng = np.random.default_rng(8)
+    source = rng.uniform(0.0, 1.0, SOURCE) * 20.0
+    target_source = np.clip(source + rng.normal(0.0, 4.0, SOURCE), 0.0, None)
+    _, target = oracle_loss(recipe, target_source, 0.0)
+    fit = SourceFit(recipe, SOURCE, CORNER, SUBSTEPS, "cuda:0", checkpoint_every=5)
+    loss, grad, thickness = fit.loss_and_grad(torch.from_numpy(source.astype(np.float32)),
+                                              torch.from_numpy(target.astype(np.float32)))
+    return recipe, source, target, fit, loss, grad.cpu().numpy().astype(np.float64), thickness.cpu().numpy()
+
+
+def test_loss_and_thickness_match_the_oracle(cuda_device, case):
+    import torch
+
+    from plume_b200.render.frame_renderer import FrameRenderer
+
+    recipe, source, target, fit, loss, _, thickness = case
+    want, want_thickness = oracle_loss(recipe, source, target)
+    assert abs(loss - want) <= 1e-4 * want
+    assert np.abs(thickness - want_thickness).max() < 1e-4
+    grid, _ = fit.forward(torch.from_numpy(source.astype(np.float32)).cuda())
+    frame = FrameRenderer(fit.view, recipe.render, grid.cells, recipe.output.channels, "cuda:0").render(grid)
+    assert np.array_equal(frame[..., 1], thickness)  # the adjoint's march is the renderer's
+
+
+def test_gradient_matches_central_differences(cuda_device, case):
+    recipe, source, target, _, _, grad, _ = case
+    scale = np.abs(grad).max()
+    assert scale > 0.0
+    rng = np.random.default_rng(2)
+    flat = np.argsort(-np.abs(grad).ravel())
+    picks = list(flat[:6]) + list(rng.choice(flat[6:], 6, replace=False))
+    for index in picks:
+        voxel = np.unravel_index(index, SOURCE)
+        up, down = source.copy(), source.copy()
+        up[voxel] += FD_H
+        down[voxel] -= FD_H
+        fd = (oracle_loss(recipe, up, target)[0] - oracle_loss(recipe, down, target)[0]) / (2 * FD_H)
+        assert abs(grad[voxel] - fd) <= GRAD_RTOL * scale, (voxel, grad[voxel], fd)
+
+
+def test_autograd_function_gives_the_same_gradient(cuda_device, case):
+    import torch
+
+    from plume_b200.adjoint import ThicknessLoss
+
+    _, source, target, fit, loss, grad, _ = case
+    s = torch.from_numpy(source.astype(np.float32)).cuda().requires_grad_(True)
+    value = ThicknessLoss.apply(s, fit, torch.from_numpy(target.astype(np.float32)))
+    value.backward()
+    assert abs(float(value) - loss) <= 1e-6 * loss
+    assert np.allclose(s.grad.cpu().numpy(), grad, rtol=1e-4, atol=1e-6 * np.abs(grad).max())
