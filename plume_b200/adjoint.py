@@ -66,6 +66,20 @@ class SourceFit:
             velocities.append(tuple(f.data.clone() for f in grid.velocity_fields()))
         return grid, (checkpoints, velocities)
 
+    def loss(self, source: torch.Tensor, target: torch.Tensor) -> float:
+        """The loss alone (a forward run and the march)."""
+        source = source.to(self.device, torch.float32).contiguous()
+        target = target.to(self.device, torch.float32).contiguous()
+        grid, _ = self.forward(source)
+        height, width = self.view.height_px, self.view.width_px
+        thickness = torch.empty((height, width), dtype=torch.float32, device=self.device)
+        loss = torch.zeros(1, dtype=torch.float64, device=self.device)
+        scratch = torch.zeros_like(grid.smoke.data)
+        N.call("plume_thickness_adjoint", grid.info, self.view_params, self.recipe.render.opacity_per_density,
+               N.ptr(grid.smoke.data), N.ptr(target), height, width, N.ptr(thickness), N.ptr(loss, torch.float64),
+               N.ptr(scratch), N.stream())
+        return float(loss.item())
+
     def _smoke_substep(self, smoke, n, source, scratch):
         """Recomputes substep n's smoke path from `smoke` (its start state); returns (data, hat, next_pre,
         totals, out)."""
