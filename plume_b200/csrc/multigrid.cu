@@ -15,6 +15,7 @@
 #include <cooperative_groups.h>
 
 #include <algorithm>
+#include <cstdlib>
 #include <cstring>
 #include <mutex>
 #include <vector>
@@ -44,6 +45,13 @@ static long g_bottom_max_cells = 2048;
 static int g_bottom_kind = 0;  // 0: the one-block solve, 1: the cluster solve
 constexpr size_t BOTTOM_MAX_SMEM = 200 * 1024;
 
+// The solve's kernels are launched with programmatic dependent launch: each may be scheduled while the
+// previous one drains and waits here, before touching memory, until that one has finished and its writes are
+// visible (a no-op when launched without it). Measured on B200: 4% off the 4-cycle solve at 128x192x128
+// (0.868 -> 0.833 ms). Triggering the successor early (griddepcontrol.launch_dependents) measured slower: the
+// waiting blocks take SM slots from the running kernel.
+__device__ __forceinline__ void wait_for_previous_grid() { asm volatile("griddepcontrol.wait;" ::: "memory"); }
+
 
 // One full red-black sweep of a tile; with PROLONG the tile first adds the coarse correction
 // (prolong_add_kernel, multigrid.py:63-68) to every pressure it loads.
@@ -53,6 +61,7 @@ template <bool PROLONG, bool UNIFORM>
 __global__ void __launch_bounds__(SWEEP_THREADS)
     k_rb_sweep(PlumeGridInfo info, const float* __restrict__ q_in, float* __restrict__ q_out,
                const float* __restrict__ rhs, float relaxation, const float* __restrict__ coarse_q, Dims coarse) {
+  wait_for_previous_grid();
   __shared__ float sq[QI * QJ * QK];
   __shared__ float sr[RI * RJ * RK];
   const int n0 = info.dims[0], n1 = info.dims[1], n2 = info.dims[2];
@@ -116,6 +125,7 @@ __global__ void __launch_bounds__(SWEEP_THREADS)
 template <bool UNIFORM>
 __global__ void k_rb_colour(PlumeGridInfo info, float* q, const float* __restrict__ rhs, int color, float relaxation,
                             const float* __restrict__ coarse_q, Dims coarse) {
+  wait_for_previous_grid();
   const int ny = info.dims[1], nz = info.dims[2];
   const int i = blockIdx.z, j = blockIdx.y * blockDim.y + threadIdx.y;
   const int k = 2 * (blockIdx.x * blockDim.x + threadIdx.x) + ((i + j + color) & 1);
@@ -130,6 +140,7 @@ __global__ void k_rb_colour(PlumeGridInfo info, float* q, const float* __restric
 
 // prolong_add_kernel (multigrid.py:63-68), used when a level has no post-smoothing sweep to fold it into.
 __global__ void k_prolong_add(Dims coarse, Dims fine, const float* __restrict__ cq, float* __restrict__ q) {
+  wait_for_previous_grid();
   const int i = blockIdx.z, j = blockIdx.y * blockDim.y + threadIdx.y, k = blockIdx.x * blockDim.x + threadIdx.x;
   if (j >= fine.n1 || k >= fine.n2) return;
   const int idx = at(fine, i, j, k);
@@ -140,6 +151,7 @@ __global__ void k_prolong_add(Dims coarse, Dims fine, const float* __restrict__ 
 // the residuals of its (up to 8) children, summed in the reference's child order.
 __global__ void k_residual_restrict(PlumeGridInfo fine, const float* __restrict__ q, const float* __restrict__ rhs,
                                     Dims coarse, float* __restrict__ coarse_rhs, float* __restrict__ coarse_q) {
+  wait_for_previous_grid();
   const int i = blockIdx.z, j = blockIdx.y * blockDim.y + threadIdx.y, k = blockIdx.x * blockDim.x + threadIdx.x;
   if (j >= coarse.n1 || k >= coarse.n2) return;
   const Dims fd = dims_of(fine);
@@ -517,6 +529,7 @@ __device__ void block_smooth(const PlumeGridInfo& info, float* q, const float* r
 }
 
 __global__ void __launch_bounds__(BOTTOM_THREADS) k_block_solve(BlockArgs b) {
+  wait_for_previous_grid();
   extern __shared__ float smem[];
   const int t = threadIdx.x;
   {
@@ -599,6 +612,30 @@ static dim3 tile_grid(const PlumeGridInfo& info) {
               (info.dims[0] + TILE_I - 1) / TILE_I);
 }
 
+static bool pdl_enabled() {
+  static const bool enabled = std::getenv("PLUME_B200_NO_PDL") == nullptr;
+  return enabled;
+}
+
+// Launches a solve kernel, with programmatic dependent launch unless PLUME_B200_NO_PDL is set.
+template <class... Params, class... Args>
+static int launch_solve_kernel(void (*kernel)(Params...), dim3 grid, dim3 block, size_t smem, cudaStream_t st,
+                               const char* what, Args... args) {
+  cudaLaunchConfig_t config = {};
+  config.gridDim = grid;
+  config.blockDim = block;
+  config.dynamicSmemBytes = smem;
+  config.stream = st;
+  cudaLaunchAttribute attribute[1];
+  attribute[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+  attribute[0].val.programmaticStreamSerializationAllowed = 1;
+  config.attrs = attribute;
+  config.numAttrs = pdl_enabled() ? 1 : 0;
+  int status = runtime_status(what, cudaLaunchKernelEx(&config, kernel, static_cast<Params>(args)...));
+  if (status != PLUME_OK) return status;
+  return launch_status(what);
+}
+
 // A level's pressure lives in two arrays: sweeps alternate between them. `cur` holds the current values.
 struct Pressure {
   float* cur;
@@ -623,11 +660,12 @@ static int colour_sweep(const PlumeGridInfo& info, float* q, const float* rhs, f
   const Dims d = dims_of(info);
   const dim3 grid(((d.n2 + 1) / 2 + TZ - 1) / TZ, (d.n1 + TY - 1) / TY, d.n0);
   for (int color = 0; color < 2; ++color) {
-    if (uniform_level(info))
-      k_rb_colour<true><<<grid, cell_block(), 0, st>>>(info, q, rhs, color, relaxation, nullptr, Dims{1, 1, 1});
-    else
-      k_rb_colour<false><<<grid, cell_block(), 0, st>>>(info, q, rhs, color, relaxation, nullptr, Dims{1, 1, 1});
-    int status = launch_status("red-black colour");
+    const float* none = nullptr;
+    int status = uniform_level(info)
+                     ? launch_solve_kernel(k_rb_colour<true>, grid, cell_block(), 0, st, "red-black colour", info, q, rhs,
+                                           color, relaxation, none, Dims{1, 1, 1})
+                     : launch_solve_kernel(k_rb_colour<false>, grid, cell_block(), 0, st, "red-black colour", info, q,
+                                           rhs, color, relaxation, none, Dims{1, 1, 1});
     if (status != PLUME_OK) return status;
   }
   return PLUME_OK;
@@ -643,8 +681,8 @@ static int sweeps_with_prolong(const PlumeGridInfo& info, Pressure& q, const flo
     const Dims cd = dims_of(*coarse);
     if (sweeps == 0 || !tiled) {
       const Dims fd = dims_of(info);
-      k_prolong_add<<<cell_grid(fd.n0, fd.n1, fd.n2), cell_block(), 0, st>>>(cd, fd, coarse_q, q.cur);
-      int status = launch_status("prolong");
+      int status = launch_solve_kernel(k_prolong_add, cell_grid(fd.n0, fd.n1, fd.n2), cell_block(), 0, st, "prolong",
+                                       cd, fd, coarse_q, q.cur);
       if (status != PLUME_OK) return status;
     } else {
       launch_tiled<true>(info, q, rhs, relaxation, coarse_q, cd, st);
@@ -732,8 +770,7 @@ static int launch_bottom(const PlumeLevel* levels, int count, int sweeps, size_t
       b.offset[l] = offset;
       offset += 2 * (int)cells_of(levels[l].info);
     }
-    k_block_solve<<<1, BOTTOM_THREADS, smem, st>>>(b);
-    return launch_status("coarse-level block solve");
+    return launch_solve_kernel(k_block_solve, dim3(1), dim3(BOTTOM_THREADS), smem, st, "coarse-level block solve", b);
   }
   ClusterArgs b{};
   b.count = count;
@@ -786,9 +823,10 @@ static int v_cycle(const PlumeLevel* levels, int count, int index, Pressure& q, 
   if (status != PLUME_OK) return status;
   const PlumeLevel& coarse = levels[index + 1];
   const Dims cd = dims_of(coarse.info);
-  k_residual_restrict<<<cell_grid(cd.n0, cd.n1, cd.n2), cell_block(), 0, st>>>(lv.info, q.cur, lv.rhs, cd, coarse.rhs,
-                                                                             coarse.q);
-  if ((status = launch_status("residual and restriction")) != PLUME_OK) return status;
+  if ((status = launch_solve_kernel(k_residual_restrict, cell_grid(cd.n0, cd.n1, cd.n2), cell_block(), 0, st,
+                                    "residual and restriction", lv.info, q.cur, lv.rhs, cd, coarse.rhs, coarse.q)) !=
+      PLUME_OK)
+    return status;
   Pressure coarse_q{coarse.q, coarse.residual};
   if ((status = v_cycle(levels, count, index + 1, coarse_q, bottom, smem, sweeps, st)) != PLUME_OK) return status;
   if (coarse_q.cur != coarse.q) {  // an odd number of coarsest sweeps left the result in the second array
