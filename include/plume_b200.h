@@ -262,11 +262,19 @@ int plume_step(const PlumeStepState* state, const PlumeStepParams* params, void*
 /* ---- render ------------------------------------------------------------------------------------------ */
 
 /* light_volume.py:18-51 light_volume_kernel. `bricks` (optional, plume_brick_floats() floats) is scratch for a
- * map of each 4x4x4 brick's largest smoke value; with it, samples whose eight corners are all <= 0 are
- * skipped, which leaves every result bit unchanged (they add exactly 0). */
+ * map of each 4x4x4 brick's largest smoke value; with it, runs of samples whose eight corners are all <= 0 are
+ * stepped over, which leaves every result bit unchanged (they add exactly 0). */
 long long plume_brick_floats(const int32_t shape[3]);
 int plume_light_volume(const int32_t shape[3], const void* smoke, int32_t storage, const float toward_light[3],
                        float cell_m, float opacity_per_density, float* light, float* bricks, void* stream);
+
+/* plume_light_volume for a camera march of the same smoke (frame_renderer.py:53-63 prepare then march): only
+ * the cells such a march reads get their light_volume_kernel value, bit for bit; every other cell gets 1.
+ * A march reads the light at the corners of samples with smoke > 0, so a cell is read only when a brick holding
+ * one of the lower corners around it has smoke > 0. `bricks` is required and is left holding the smoke's brick
+ * map. */
+int plume_march_light_volume(const int32_t shape[3], const void* smoke, int32_t storage, const float toward_light[3],
+                             float cell_m, float opacity_per_density, float* light, float* bricks, void* stream);
 
 /* normal_field.py:52-61 NormalField.compute (blur_axis_kernel x 3 + gradient_kernel); gradient is
  * (n0, n1, n2, 3). */
@@ -278,8 +286,9 @@ int plume_brick_max(const int32_t shape[3], const void* field, int32_t storage, 
 
 /* raymarch.py:86-140 raymarch_kernel; image is (height, width, 5). gradient/light are the unused pass's
  * 1-cell stand-in when not read (frame_renderer.py:29-35). `bricks` (optional, plume_brick_floats() floats)
- * is scratch for the marched smoke's brick map, built by this call; with it, samples with no smoke skip their
- * smoke sample. Terms that are exactly 0 are never evaluated, so the image is the same with or without it. */
+ * is scratch for the march's brick map of the smoke and temperature, built by this call; with it, samples with
+ * no smoke skip their smoke sample and runs of samples with neither smoke nor glow are stepped over. Terms
+ * that are exactly 0 are never evaluated, so the image is the same with or without it. */
 int plume_raymarch(const PlumeGridInfo* info, const void* smoke, const void* temperature, int32_t storage,
                    const float* gradient, const int32_t gradient_shape[3], const float* light,
                    const int32_t light_shape[3], const PlumeViewParams* view, const PlumeLookParams* look, float* image,

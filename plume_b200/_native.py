@@ -124,6 +124,7 @@ SIGNATURES = {
     "plume_step": [ctypes.POINTER(PlumeStepState), ctypes.POINTER(PlumeStepParams), _P],
     "plume_brick_floats": [_SHAPE],
     "plume_light_volume": [_SHAPE, _P, _I, _F3P, _F, _F, _P, _P, _P],
+    "plume_march_light_volume": [_SHAPE, _P, _I, _F3P, _F, _F, _P, _P, _P],
     "plume_normal_field": [_SHAPE, _P, _I, _P, _P, _P, _F3P, _I, _P],
     "plume_brick_max": [_SHAPE, _P, _I, _P, _P],
     "plume_raymarch": [_INFO, _P, _P, _I, _P, _SHAPE, _P, _SHAPE, ctypes.POINTER(PlumeViewParams),

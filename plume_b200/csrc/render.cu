@@ -38,6 +38,38 @@ __host__ __device__ __forceinline__ Dims brick_dims(const Dims& d) {
   return Dims{(d.n0 + BRICK - 1) / BRICK, (d.n1 + BRICK - 1) / BRICK, (d.n2 + BRICK - 1) / BRICK};
 }
 
+// How many samples after the one at index-space point g stay in g's brick, for a march that advances `delta`
+// cells per sample on each axis (returned as a float, possibly negative or huge; the caller floors and caps it).
+// A sample's brick is that of its clamped lower corner, so on each axis the first brick reaches to -inf and the
+// last to +inf. Samples nearer than `margin` cells to a brick face are not counted: the margin bounds twice the
+// float error of a computed sample point against the exact line through the march, so every counted sample,
+// as computed, lies in the brick.
+__device__ __forceinline__ float samples_in_brick(const Dims& d, F3 g, F3 delta, float margin) {
+  const int n[3] = {d.n0, d.n1, d.n2};
+  float count = 3.0e38f;
+#pragma unroll
+  for (int a = 0; a < 3; ++a) {
+    if (delta[a] == 0.0f) continue;
+    const int b = (int)fminf(fmaxf(g[a], 0.0f), (float)(n[a] - 1)) / BRICK;
+    float room;
+    if (delta[a] > 0.0f) {
+      if (b == (n[a] - 1) / BRICK) continue;
+      room = (float)((b + 1) * BRICK) - g[a];
+    } else {
+      if (b == 0) continue;
+      room = g[a] - (float)(b * BRICK);
+    }
+    count = fminf(count, (room - margin) / fabsf(delta[a]));
+  }
+  return count;
+}
+
+// Index of the sample a march continues from after the sample `s` in an empty brick: past every later sample
+// that `samples_in_brick` places in the same brick, and at most `end`.
+__device__ __forceinline__ int past_brick(int s, int end, float count) {
+  return count >= 1.0f ? s + (int)fminf(count, (float)(end - s)) : s;
+}
+
 template <class T>
 __global__ void k_brick_max(Dims d, const T* __restrict__ f, float* __restrict__ bricks) {
   const Dims b = brick_dims(d);
@@ -52,12 +84,27 @@ __global__ void k_brick_max(Dims d, const T* __restrict__ f, float* __restrict__
 
 // light_volume_kernel (light_volume.py:18-33): one thread per cell marches toward the light in at most
 // half-cell steps to the box edge and writes exp(-opacity * column * cell_m). With `bricks`, samples whose
-// corners are all <= 0 are skipped (they add exactly 0).
+// corners are all <= 0 add exactly 0: the march steps over the whole run of them that lies in one brick.
+//
+// With `march_cells`, only the cells a camera march of the same smoke with this brick map can read get their
+// value: a march sample reads the eight corners of its lower corner cell c0 only when c0's brick is not empty,
+// so a cell c is read only if the brick of some c0 in {c-1, c}^3 is not empty. Every other cell gets 1.
 template <class T>
 __global__ void k_light_volume(Dims d, const T* __restrict__ smoke, F3 toward, float cell_m, float opacity,
-                               float* __restrict__ light, const float* __restrict__ bricks) {
+                               float* __restrict__ light, const float* __restrict__ bricks, int march_cells) {
   const int i = blockIdx.z, j = blockIdx.y * blockDim.y + threadIdx.y, k = blockIdx.x * blockDim.x + threadIdx.x;
   if (j >= d.n1 || k >= d.n2) return;
+  const Dims bd = brick_dims(d);
+  if (march_cells) {
+    bool read = false;
+    for (int a = imax_(i - 1, 0); a <= i; ++a)
+      for (int b = imax_(j - 1, 0); b <= j; ++b)
+        for (int c = imax_(k - 1, 0); c <= k; ++c) read |= __ldg(bricks + at(bd, a / BRICK, b / BRICK, c / BRICK)) > 0.0f;
+    if (!read) {
+      light[at(d, i, j, k)] = 1.0f;
+      return;
+    }
+  }
   const F3 half = f3(0.5f, 0.5f, 0.5f);
   F3 start = add3(f3((float)i, (float)j, (float)k), half);
   F3 box_max = f3((float)d.n0, (float)d.n1, (float)d.n2);
@@ -67,7 +114,11 @@ __global__ void k_light_volume(Dims d, const T* __restrict__ smoke, F3 toward, f
   float column = 0.0f;
   if (steps > 0) {
     float step = length / (float)steps;
-    const Dims bd = brick_dims(d);
+    // the computed points are start + toward * ((s + 0.5) * step) - 0.5: within (2 * length + 2 * extent) * 2^-24
+    // cells of the exact line
+    const float extent = (float)(imax_(imax_(d.n0, d.n1), d.n2) + 1);
+    const float margin = (4.0f * length + 4.0f * extent) * 5.9604645e-8f + 1.0e-3f;
+    const F3 delta = mul3(toward, step);
     for (int s = 0; s < steps; ++s) {
       F3 position = add3(start, mul3(toward, ((float)s + 0.5f) * step));
       const F3 g = sub3(position, half);
@@ -75,7 +126,10 @@ __global__ void k_light_volume(Dims d, const T* __restrict__ smoke, F3 toward, f
         const int i0 = (int)fminf(fmaxf(g[0], 0.0f), (float)(d.n0 - 1));
         const int j0 = (int)fminf(fmaxf(g[1], 0.0f), (float)(d.n1 - 1));
         const int k0 = (int)fminf(fmaxf(g[2], 0.0f), (float)(d.n2 - 1));
-        if (__ldg(bricks + at(bd, i0 / BRICK, j0 / BRICK, k0 / BRICK)) <= 0.0f) continue;
+        if (__ldg(bricks + at(bd, i0 / BRICK, j0 / BRICK, k0 / BRICK)) <= 0.0f) {
+          s = past_brick(s, steps - 1, samples_in_brick(d, g, delta, margin));
+          continue;
+        }
       }
       column = column + fmax_(sample_index_space(smoke, d, g), 0.0f) * step;
     }
@@ -141,6 +195,32 @@ __device__ __forceinline__ F3 sample_vec(const float* __restrict__ f, const Dims
   return lerp3(lerp3(c00, c10, ty), lerp3(c01, c11, ty), tz);
 }
 
+// The camera march's brick map: over each brick and the next cell past it on each axis (every corner a sample
+// with lower corner in the brick can blend), 0 when the smoke is <= 0 and the temperature cannot glow, 1 when
+// the smoke is <= 0 but the temperature may glow, 2 otherwise. The temperature cannot glow when its largest
+// value is below glow_start by more than the rounding of three lerps (16 ulps), or when it is one value
+// <= glow_start: a blend of equal corners is exactly that value. A sample in a class-0 brick has alpha 0 and
+// glow 0 (adds exactly nothing); one in a class-1 brick has alpha 0.
+template <class T>
+__global__ void k_march_bricks(Dims d, const T* __restrict__ smoke, const T* __restrict__ temperature,
+                               float glow_start, float* __restrict__ bricks) {
+  const Dims b = brick_dims(d);
+  const int bi = blockIdx.z, bj = blockIdx.y * blockDim.y + threadIdx.y, bk = blockIdx.x * blockDim.x + threadIdx.x;
+  if (bj >= b.n1 || bk >= b.n2) return;
+  float most = -3.0e38f, hot = -3.0e38f, cold = 3.0e38f;
+  for (int i = bi * BRICK; i <= imin_(bi * BRICK + BRICK, d.n0 - 1); ++i)
+    for (int j = bj * BRICK; j <= imin_(bj * BRICK + BRICK, d.n1 - 1); ++j)
+      for (int k = bk * BRICK; k <= imin_(bk * BRICK + BRICK, d.n2 - 1); ++k) {
+        const size_t c = at(d, i, j, k);
+        most = fmaxf(most, ldg_f(smoke + c));
+        const float t = ldg_f(temperature + c);
+        hot = fmaxf(hot, t);
+        cold = fminf(cold, t);
+      }
+  const bool dark = (hot + fabsf(hot) * 9.5367432e-7f < glow_start) || (cold == hot && hot <= glow_start);
+  bricks[at(b, bi, bj, bk)] = most > 0.0f ? 2.0f : (dark ? 0.0f : 1.0f);
+}
+
 struct MarchArgs {
   PlumeGridInfo info;
   PlumeViewParams view;
@@ -148,16 +228,19 @@ struct MarchArgs {
   Dims d, dg, dl;
 };
 
-// raymarch_kernel (raymarch.py:86-140): one thread per pixel. Terms that are exactly zero are not evaluated:
-// with no smoke at a sample (all eight corners <= 0 in the brick map, or a blend <= 0) alpha is exactly 0, so
-// the exp, the light or gradient sample and the transmittance update are skipped (they would add +0 or
-// multiply by 1); with no glow the pow is skipped (it would add +0). Every result bit is unchanged.
+// raymarch_kernel (raymarch.py:86-140): one thread per pixel, 256 consecutive pixels of the image per block.
+// Terms that are exactly zero are not evaluated: with no smoke at a sample (all eight corners <= 0 in the
+// brick map, or a blend <= 0) alpha is exactly 0, so the exp, the light or gradient sample and the
+// transmittance update are skipped (they would add +0 or multiply by 1); with no glow the pow is skipped (it
+// would add +0); a run of samples in a brick with neither smoke nor glow is stepped over whole. Every result
+// bit is unchanged.
 template <class T>
-__global__ void k_raymarch(MarchArgs a, const T* __restrict__ smoke, const T* __restrict__ temperature,
+__global__ void __launch_bounds__(256, 4) k_raymarch(MarchArgs a, const T* __restrict__ smoke, const T* __restrict__ temperature,
                            const float* __restrict__ gradient, const float* __restrict__ light, float* __restrict__ image,
                            int height, int width, const float* __restrict__ bricks) {
-  const int px = blockIdx.x * blockDim.x + threadIdx.x, py = blockIdx.y * blockDim.y + threadIdx.y;
-  if (px >= width || py >= height) return;
+  const int pixel = blockIdx.x * blockDim.x + threadIdx.x;
+  if (pixel >= height * width) return;
+  const int px = pixel % width, py = pixel / width;
   const PlumeViewParams& view = a.view;
   const PlumeLookParams& look = a.look;
   const PlumeGridInfo& info = a.info;
@@ -184,6 +267,16 @@ __global__ void k_raymarch(MarchArgs a, const T* __restrict__ smoke, const T* __
     int steps = (int)ceilf(length / (0.5f * info.cell_m));
     float step_m = length / (float)steps;
     const Dims bd = brick_dims(a.d);
+    // The computed points origin + direction * (s0 + (s + 0.5) * step_m) lie within
+    // (3 |t| + 2 |box coordinate| + |box origin|) * 2^-24 / cell_m + 2 |g| * 2^-24 cells of the exact line; the
+    // margin is over twice that.
+    float box_far = 0.0f;
+#pragma unroll
+    for (int c = 0; c < 3; ++c) box_far = fmaxf(box_far, fmaxf(fabsf(box_origin[c]), fabsf(box_max[c])));
+    const float cells_far = (float)imax_(imax_(a.d.n0, a.d.n1), a.d.n2);
+    const float margin = (8.0f * fmaxf(fabsf(s0), fabsf(s1)) + 6.0f * box_far) * 5.9604645e-8f / info.cell_m +
+                         cells_far * 9.5367432e-7f + 1.0e-3f;
+    const F3 delta = mul3(direction, step_m / info.cell_m);
     for (int s = 0; s < steps; ++s) {
       F3 position = add3(origin, mul3(direction, s0 + ((float)s + 0.5f) * step_m));
       F3 g = sub3(div3(sub3(position, box_origin), info.cell_m), f3(0.5f, 0.5f, 0.5f));
@@ -192,7 +285,12 @@ __global__ void k_raymarch(MarchArgs a, const T* __restrict__ smoke, const T* __
         const int i0 = (int)fminf(fmaxf(g[0], 0.0f), (float)(a.d.n0 - 1));
         const int j0 = (int)fminf(fmaxf(g[1], 0.0f), (float)(a.d.n1 - 1));
         const int k0 = (int)fminf(fmaxf(g[2], 0.0f), (float)(a.d.n2 - 1));
-        empty = __ldg(bricks + at(bd, i0 / BRICK, j0 / BRICK, k0 / BRICK)) <= 0.0f;
+        const float kind = __ldg(bricks + at(bd, i0 / BRICK, j0 / BRICK, k0 / BRICK));
+        if (kind == 0.0f) {
+          s = past_brick(s, steps - 1, samples_in_brick(a.d, g, delta, margin));
+          continue;
+        }
+        empty = kind == 1.0f;
       }
       const float density = empty ? 0.0f : fmax_(sample_index_space(smoke, a.d, g), 0.0f);
       const float alpha = density > 0.0f ? 1.0f - exp_f(-look.opacity_per_density * density * step_m) : 0.0f;
@@ -252,7 +350,7 @@ namespace plume {
 
 template <class T>
 static int light_volume(const Dims& d, const T* smoke, F3 toward, float cell_m, float opacity, float* light,
-                        float* bricks, cudaStream_t st) {
+                        float* bricks, int march_cells, cudaStream_t st) {
   if (bricks) {
     const Dims b = brick_dims(d);
     k_brick_max<T><<<cell_grid(b.n0, b.n1, b.n2), cell_block(), 0, st>>>(d, smoke, bricks);
@@ -260,7 +358,7 @@ static int light_volume(const Dims& d, const T* smoke, F3 toward, float cell_m, 
     if (status != PLUME_OK) return status;
   }
   k_light_volume<T><<<cell_grid(d.n0, d.n1, d.n2), cell_block(), 0, st>>>(d, smoke, toward, cell_m, opacity, light,
-                                                                          bricks);
+                                                                          bricks, march_cells);
   return launch_status("light volume");
 }
 
@@ -288,12 +386,16 @@ static int brick_max(const Dims& d, const T* field, float* bricks, cudaStream_t 
 template <class T>
 static int raymarch(const MarchArgs& a, const T* smoke, const T* temperature, const float* gradient, const float* light,
                     float* image, int height, int width, float* bricks, cudaStream_t st) {
-  if (bricks) {  // the brick map of exactly the smoke being marched
-    int status = brick_max<T>(a.d, smoke, bricks, st);
+  if (bricks) {  // the brick map of exactly the smoke and temperature being marched
+    const Dims b = brick_dims(a.d);
+    k_march_bricks<T><<<cell_grid(b.n0, b.n1, b.n2), cell_block(), 0, st>>>(a.d, smoke, temperature,
+                                                                             a.look.glow_start_k, bricks);
+    int status = launch_status("march brick map");
     if (status != PLUME_OK) return status;
   }
-  dim3 block(16, 16), grid((width + 15) / 16, (height + 15) / 16);
-  k_raymarch<T><<<grid, block, 0, st>>>(a, smoke, temperature, gradient, light, image, height, width, bricks);
+  const long pixels = (long)height * width;
+  k_raymarch<T><<<(int)((pixels + 255) / 256), 256, 0, st>>>(a, smoke, temperature, gradient, light, image, height,
+                                                              width, bricks);
   return launch_status("raymarch");
 }
 
@@ -308,18 +410,34 @@ static int raymarch(const MarchArgs& a, const T* smoke, const T* temperature, co
 
 }  // namespace plume
 
-extern "C" int plume_light_volume(const int32_t shape[3], const void* smoke, int32_t storage, const float toward_light[3],
-                                  float cell_m, float opacity_per_density, float* light, float* bricks, void* stream) {
-  if (!valid_shape(shape) || !smoke || !toward_light || !light) return fail(PLUME_ERR_INVALID, "light_volume: bad argument");
+static int light_volume_call(const int32_t shape[3], const void* smoke, int32_t storage, const float toward_light[3],
+                             float cell_m, float opacity_per_density, float* light, float* bricks, int march_cells,
+                             void* stream) {
   const Dims d{shape[0], shape[1], shape[2]};
   const F3 toward = f3(toward_light[0], toward_light[1], toward_light[2]);
   cudaStream_t st = as_stream(stream);
   PLUME_BY_STORAGE(storage,
-                   light_volume(d, static_cast<const float*>(smoke), toward, cell_m, opacity_per_density, light, bricks, st),
+                   light_volume(d, static_cast<const float*>(smoke), toward, cell_m, opacity_per_density, light, bricks,
+                                march_cells, st),
                    light_volume(d, static_cast<const __nv_bfloat16*>(smoke), toward, cell_m, opacity_per_density, light,
-                                bricks, st),
-                   light_volume(d, static_cast<const __half*>(smoke), toward, cell_m, opacity_per_density, light, bricks, st),
+                                bricks, march_cells, st),
+                   light_volume(d, static_cast<const __half*>(smoke), toward, cell_m, opacity_per_density, light, bricks,
+                                march_cells, st),
                    "light_volume")
+}
+
+extern "C" int plume_light_volume(const int32_t shape[3], const void* smoke, int32_t storage, const float toward_light[3],
+                                  float cell_m, float opacity_per_density, float* light, float* bricks, void* stream) {
+  if (!valid_shape(shape) || !smoke || !toward_light || !light) return fail(PLUME_ERR_INVALID, "light_volume: bad argument");
+  return light_volume_call(shape, smoke, storage, toward_light, cell_m, opacity_per_density, light, bricks, 0, stream);
+}
+
+extern "C" int plume_march_light_volume(const int32_t shape[3], const void* smoke, int32_t storage,
+                                        const float toward_light[3], float cell_m, float opacity_per_density,
+                                        float* light, float* bricks, void* stream) {
+  if (!valid_shape(shape) || !smoke || !toward_light || !light || !bricks)
+    return fail(PLUME_ERR_INVALID, "march_light_volume: bad argument");
+  return light_volume_call(shape, smoke, storage, toward_light, cell_m, opacity_per_density, light, bricks, 1, stream);
 }
 
 extern "C" int plume_normal_field(const int32_t shape[3], const void* smoke, int32_t storage, float* blurred,
@@ -353,7 +471,7 @@ extern "C" int plume_raymarch(const PlumeGridInfo* info, const void* smoke, cons
                               const int32_t light_shape[3], const PlumeViewParams* view, const PlumeLookParams* look,
                               float* image, int32_t height, int32_t width, float* bricks, void* stream) {
   if (!info || !smoke || !temperature || !gradient || !light || !view || !look || !image || height < 1 || width < 1 ||
-      !valid_shape(info->dims) || !valid_shape(gradient_shape) || !valid_shape(light_shape))
+      (long long)height * width >= (1LL << 31) || !valid_shape(info->dims) || !valid_shape(gradient_shape) || !valid_shape(light_shape))
     return fail(PLUME_ERR_INVALID, "raymarch: bad argument");
   MarchArgs a;
   a.info = *info;

@@ -49,8 +49,10 @@ class FrameRenderer:
         return self._host.numpy().copy()
 
     def prepare(self, smoke, cell_m: float) -> None:
+        """The volume pass for marches of this same smoke. In the shade layout only the light at the cells such
+        a march reads is computed (the rest hold 1); those cells match LightVolume.compute bit for bit."""
         if self.shade_layout:
-            self.light = self.light_volume.compute(smoke, cell_m)  # also fills the brick map
+            self.light = self.light_volume.compute(smoke, cell_m, march_cells=True)
         else:
             self.gradient = self.normal_field.compute(smoke)
 

@@ -17,8 +17,10 @@ class LightVolume:
         # per-frame map of each 4x4x4 brick's largest smoke value: the march skips samples that add nothing
         self.bricks = torch.empty(N.lib().plume_brick_floats(N.c_int3(*cells)), dtype=torch.float32, device=device)
 
-    def compute(self, smoke: torch.Tensor, cell_m: float) -> torch.Tensor:
-        N.call("plume_light_volume", N.shape3(smoke), N.field_ptr(smoke), N.storage_of(smoke),
-               N.f3(self.toward_light), cell_m,
+    def compute(self, smoke: torch.Tensor, cell_m: float, march_cells: bool = False) -> torch.Tensor:
+        """The light volume of `smoke`. With `march_cells`, only the cells a camera march of this same smoke
+        reads get their value (bit for bit) and the rest hold 1: what FrameRenderer.prepare needs."""
+        N.call("plume_march_light_volume" if march_cells else "plume_light_volume", N.shape3(smoke),
+               N.field_ptr(smoke), N.storage_of(smoke), N.f3(self.toward_light), cell_m,
                self.opacity_per_density, N.ptr(self.light), N.ptr(self.bricks), N.stream())
         return self.light

@@ -37,13 +37,14 @@ def test_light_volume_matches_the_oracle(cuda_device):
     assert max_rel(host(light), expected, floor=1e-6) < LIGHT_RTOL
 
 
-def test_light_volume_empty_space_skipping_changes_no_bit(cuda_device):
-    """The brick map only skips samples that add exactly 0: the light volume is bit-identical without it."""
+@pytest.mark.parametrize("cells", [(24, 32, 20), (64, 96, 64)])
+def test_light_volume_empty_space_skipping_changes_no_bit(cuda_device, cells):
+    """The brick map only steps over samples that add exactly 0: the light volume is bit-identical without it."""
     import torch
 
     from plume_b200 import _native as N
 
-    o, c = render_pair()
+    o, c = render_pair(cells)
     smoke = c.smoke.data
     toward = N.f3(np.array([0.5, 0.8, 0.3]) / np.linalg.norm([0.5, 0.8, 0.3]))
     with_bricks, without = torch.empty_like(smoke), torch.empty_like(smoke)
@@ -74,26 +75,90 @@ def test_frame_matches_the_oracle(cuda_device, channels, elevation, azimuth):
 
 
 @pytest.mark.parametrize("channels", [SHADE_LAYOUT, NORMAL_LAYOUT])
-def test_march_empty_space_skipping_changes_no_bit(cuda_device, channels):
+@pytest.mark.parametrize("glow_start", [600.0, 293.0])  # 293 K is the ambient: one-valued bricks cannot glow
+@pytest.mark.parametrize("cells,perspective", [((24, 32, 20), False), ((64, 96, 64), False), ((64, 96, 64), True)])
+def test_march_empty_space_skipping_changes_no_bit(cuda_device, channels, glow_start, cells, perspective):
+    """The march's brick map only skips samples and runs of samples that add exactly 0: the image is
+    bit-identical without it, orthographic (origin 1e4 m out, the largest rounding of the sample points) and
+    perspective."""
     import torch
 
     from plume_b200 import _native as N
     from plume_b200.render.frame_renderer import FrameRenderer
 
-    o, c = render_pair()
-    cells = c.cells
+    o, c = render_pair(cells)
     size = tuple(n * 0.05 for n in cells)
     view = make_domain_view(make_camera(20.0, 30.0), (-size[0] / 2, 0.0, -size[2] / 2), size, 0.05, 2.0)
-    renderer = FrameRenderer(view, RenderSettings(glow_start_k=600.0, light_dir=(0.5, 0.8, 0.3)), cells, channels,
-                             "cuda:0")
+    renderer = FrameRenderer(view, RenderSettings(glow_start_k=glow_start, light_dir=(0.5, 0.8, 0.3)), cells,
+                             channels, "cuda:0")
+    params = renderer.view_params
+    if perspective:  # an eye 3 m out along the view axis from the box centre
+        centre = np.array([c.info.origin_m[a] + 0.5 * cells[a] * 0.05 for a in range(3)])
+        params.perspective = 1
+        params.eye = type(params.eye)(*(centre + 3.0 * view.camera.toward))
+        params.left_m, params.top_m = -0.5 * renderer.image.shape[1] / 256, 0.5 * renderer.image.shape[0] / 256
+        params.pixel_m = 1.0 / 256
     renderer.prepare(c.smoke.data, c.info.cell_m)
     skipped = torch.zeros_like(renderer.image)
     full = torch.zeros_like(renderer.image)
-    renderer.march(c.smoke.data, c.temperature.data, c.info, renderer.view_params, skipped)
+    renderer.march(c.smoke.data, c.temperature.data, c.info, params, skipped)
     N.call("plume_raymarch", c.info, N.ptr(c.smoke.data), N.ptr(c.temperature.data), 0, N.ptr(renderer.gradient),
            N.c_int3(*renderer.gradient.shape[:3]), N.ptr(renderer.light), N.shape3(renderer.light),
-           renderer.view_params, renderer.look_params, N.ptr(full), full.shape[0], full.shape[1], None, N.stream())
+           params, renderer.look_params, N.ptr(full), full.shape[0], full.shape[1], None, N.stream())
     assert torch.equal(skipped, full)
+    assert float(full[..., 1].max()) > 0.1  # the rays cross smoke
+    if glow_start < 300.0:
+        assert float(full[..., 0].max()) > 0.0  # and glow
+
+
+def read_by_march(smoke: np.ndarray) -> np.ndarray:
+    """Cells whose light a march of `smoke` can read: a neighbour c0 in {c-1, c}^3 lies in a brick (4 cells and
+    the next past it on each axis) holding smoke > 0."""
+    n = smoke.shape
+    nb = tuple((x + 3) // 4 for x in n)
+    brick = np.zeros(nb, dtype=bool)
+    for b in np.ndindex(*nb):
+        lo = [4 * b[a] for a in range(3)]
+        hi = [min(4 * b[a] + 5, n[a]) for a in range(3)]
+        brick[b] = smoke[lo[0]:hi[0], lo[1]:hi[1], lo[2]:hi[2]].max() > 0
+    lit = brick[np.ix_(*[np.arange(x) // 4 for x in n])]
+    read = lit.copy()
+    for da in (0, 1):
+        for db in (0, 1):
+            for dc in (0, 1):
+                shifted = np.zeros_like(lit)
+                shifted[da:, db:, dc:] = lit[:n[0] - da, :n[1] - db, :n[2] - dc]
+                read |= shifted
+    return read
+
+
+@pytest.mark.parametrize("cells", [(24, 32, 20), (64, 96, 64)])
+def test_march_light_volume_is_the_light_volume_where_the_march_reads(cuda_device, cells):
+    """plume_march_light_volume: the read cells bit for bit as plume_light_volume, 1 elsewhere; and the frame a
+    renderer marches with it is bit-identical to one marched with the whole light volume."""
+    import torch
+
+    from plume_b200 import _native as N
+    from plume_b200.render.frame_renderer import FrameRenderer
+    from plume_b200.render.light_volume import LightVolume
+
+    o, c = render_pair(cells)
+    direction = np.array([0.5, 0.8, 0.3])
+    whole = LightVolume(c.cells, direction, 4.0, "cuda:0").compute(c.smoke.data, c.info.cell_m).clone()
+    marched = LightVolume(c.cells, direction, 4.0, "cuda:0").compute(c.smoke.data, c.info.cell_m, march_cells=True)
+    read = read_by_march(host(c.smoke.data))
+    assert 0.05 < read.mean() < 0.9
+    assert np.array_equal(host(marched)[read], host(whole)[read])
+    assert np.all(host(marched)[~read] == 1.0)
+
+    size = tuple(n * 0.05 for n in cells)
+    view = make_domain_view(make_camera(20.0, 30.0), (-size[0] / 2, 0.0, -size[2] / 2), size, 0.05, 2.0)
+    renderer = FrameRenderer(view, RenderSettings(glow_start_k=600.0, light_dir=tuple(direction)), cells,
+                             SHADE_LAYOUT, "cuda:0")
+    image = renderer.render(c)
+    renderer.light = renderer.light_volume.compute(c.smoke.data, c.info.cell_m).clone()  # the whole light volume
+    renderer.march(c.smoke.data, c.temperature.data, c.info, renderer.view_params, renderer.image)
+    assert np.array_equal(image, host(renderer.image))
 
 
 def test_normal_field_matches_the_oracle(cuda_device):
