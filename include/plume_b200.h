@@ -270,8 +270,8 @@ int plume_light_volume(const int32_t shape[3], const void* smoke, int32_t storag
 
 /* plume_light_volume for a camera march of the same smoke (frame_renderer.py:53-63 prepare then march): only
  * the cells such a march reads get their light_volume_kernel value, bit for bit; every other cell gets 1.
- * A march reads the light at the corners of samples with smoke > 0, so a cell is read only when a brick holding
- * one of the lower corners around it has smoke > 0. `bricks` is required and is left holding the smoke's brick
+ * A march reads the light at the corners of samples with smoke > 0, so a cell is read only when one of the 27
+ * cells around it (itself included) holds smoke > 0. `bricks` is required and is left holding the smoke's brick
  * map. */
 int plume_march_light_volume(const int32_t shape[3], const void* smoke, int32_t storage, const float toward_light[3],
                              float cell_m, float opacity_per_density, float* light, float* bricks, void* stream);

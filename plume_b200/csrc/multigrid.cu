@@ -500,7 +500,111 @@ struct Walk {
   }
 };
 
-__device__ void block_smooth(const PlumeGridInfo& info, float* q, const float* rhs, int sweeps, float relaxation) {
+// The cells of one colour that a thread updates in the one-block solve, with everything about them that stays
+// fixed through a smoothing call held in registers: the cell's and its six neighbours' shared-memory indices
+// (16 bits each, 0xffff for a neighbour outside the level), and the coupling total sc and the source term
+// (cell_m * cell_m) * rhs of relaxed_uniform. A sweep pass is then seven shared loads, the sums and the update: the same float operations as relaxed_uniform, with
+// an interior cell's sum (((((a + b) + c) + d) + e) + f) taken as ((((((0 + a) + b) + c) + d) + e) + f), equal
+// in value (0 + a == a up to the sign of a zero).
+constexpr int STENCIL_SLOTS = 2;
+constexpr unsigned NO_CELL = 0xffffu;
+
+struct StencilSlot {
+  unsigned own_and_x0, x1_y0, y1_z0, z1;  // pairs of 16-bit indices
+  float sc, source;
+};
+
+__device__ __forceinline__ unsigned pack16(unsigned lo, unsigned hi) { return (lo & 0xffffu) | (hi << 16); }
+
+__device__ __forceinline__ StencilSlot stencil_slot(const PlumeGridInfo& info, const Dims& d, float ghost, const float* q,
+                                                    const float* rhs, int p, int pairs_k, int color) {
+  StencilSlot slot;
+  slot.own_and_x0 = NO_CELL;
+  const int i = p / (d.n1 * pairs_k), r = p - i * (d.n1 * pairs_k);
+  const int j = r / pairs_k, k = 2 * (r - j * pairs_k) + ((i + j + color) & 1);
+  if (k >= d.n2) return slot;
+  const int c[3] = {i, j, k};
+  const int stride[3] = {d.n1 * d.n2, d.n2, 1};
+  const int own = at(d, i, j, k);
+  unsigned nb[6];
+  float sc = 0.0f;
+#pragma unroll
+  for (int axis = 0; axis < 3; ++axis) {  // neighbor_sum_uniform's couplings, in its order
+    float tc0 = 0.0f, tc1 = 0.0f;
+    nb[2 * axis] = nb[2 * axis + 1] = NO_CELL;
+    if (c[axis] > 0) {
+      nb[2 * axis] = own - stride[axis];
+      tc0 = 1.0f;
+    } else if (info.open_lo[axis] == 1) {
+      tc0 = ghost;
+    }
+    if (c[axis] < info.dims[axis] - 1) {
+      nb[2 * axis + 1] = own + stride[axis];
+      tc1 = 1.0f;
+    } else if (info.open_hi[axis] == 1) {
+      tc1 = ghost;
+    }
+    sc = (sc + tc0) + tc1;
+  }
+  if (sc == 0.0f) return slot;  // no coupling at all: relaxed_uniform leaves the cell alone
+  slot.own_and_x0 = pack16(own, nb[0]);
+  slot.x1_y0 = pack16(nb[1], nb[2]);
+  slot.y1_z0 = pack16(nb[3], nb[4]);
+  slot.z1 = nb[5];
+  slot.sc = sc;
+  slot.source = info.cell_m * info.cell_m * rhs[own];
+  return slot;
+}
+
+__device__ __forceinline__ float neighbour16(const float* q, unsigned index) { return index == NO_CELL ? 0.0f : q[index]; }
+
+__device__ __forceinline__ void relax_slot(float* q, const StencilSlot& slot, float relaxation) {
+  if ((slot.own_and_x0 & 0xffffu) == NO_CELL) return;
+  const float a = neighbour16(q, slot.own_and_x0 >> 16), b = neighbour16(q, slot.x1_y0 & 0xffffu);
+  const float c = neighbour16(q, slot.x1_y0 >> 16), e = neighbour16(q, slot.y1_z0 & 0xffffu);
+  const float f = neighbour16(q, slot.y1_z0 >> 16), g = neighbour16(q, slot.z1);
+  const float sq = (((((0.0f + a) + b) + c) + e) + f) + g;
+  const float target = (sq - slot.source) / slot.sc;
+  float* own = q + (slot.own_and_x0 & 0xffffu);
+  *own = *own + relaxation * (target - *own);
+}
+
+// `sweeps` red-black sweeps of a uniform level from register-held stencils: `lanes` threads (one warp or the
+// whole block) with at most STENCIL_SLOTS cells of each colour each. Returns false, having done nothing, when
+// the level does not fit that.
+__device__ __forceinline__ bool stencil_smooth(const PlumeGridInfo& info, float* q, const float* rhs, int sweeps, float relaxation) {
+  const Dims d = dims_of(info);
+  const int pairs_k = (d.n2 + 1) / 2;
+  const int pairs = d.n0 * d.n1 * pairs_k;
+  const bool one_warp = pairs <= 32 * STENCIL_SLOTS;
+  const int lanes = one_warp ? 32 : BOTTOM_THREADS;
+  if (!is_uniform(info) || pairs > lanes * STENCIL_SLOTS || d.n0 * d.n1 * d.n2 >= (int)NO_CELL) return false;
+  if (!one_warp || threadIdx.x < 32) {
+    const float ghost = ghost_coupling(info);
+    StencilSlot slot[2][STENCIL_SLOTS];
+#pragma unroll
+    for (int color = 0; color < 2; ++color)
+#pragma unroll
+      for (int n = 0; n < STENCIL_SLOTS; ++n) {
+        const int p = threadIdx.x + n * lanes;
+        if (p < pairs) slot[color][n] = stencil_slot(info, d, ghost, q, rhs, p, pairs_k, color);
+        else slot[color][n].own_and_x0 = NO_CELL;
+      }
+    for (int s = 0; s < sweeps; ++s)
+#pragma unroll
+      for (int color = 0; color < 2; ++color) {
+#pragma unroll
+        for (int n = 0; n < STENCIL_SLOTS; ++n) relax_slot(q, slot[color][n], relaxation);
+        if (one_warp) __syncwarp();
+        else __syncthreads();
+      }
+  }
+  __syncthreads();
+  return true;
+}
+
+__device__ __forceinline__ void block_smooth(const PlumeGridInfo& info, float* q, const float* rhs, int sweeps, float relaxation) {
+  if (stencil_smooth(info, q, rhs, sweeps, relaxation)) return;
   const Dims d = dims_of(info);
   const int pairs_k = (d.n2 + 1) / 2;
   const int pairs = d.n0 * d.n1 * pairs_k;

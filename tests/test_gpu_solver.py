@@ -13,8 +13,8 @@ pytestmark = pytest.mark.gpu
 
 # odd sizes: several tiles, coarse levels with overhanging cells (non-uniform stencil)
 CASES = [((19, 24, 17), OPEN), ((40, 36, 70), ALL_CLOSED), ((38, 48, 38), OPEN), ((5, 33, 66), OPEN),
-         ((70, 9, 7), ALL_CLOSED)]
-IDS = ["19x24x17-open", "40x36x70-closed", "38x48x38-open", "5x33x66-open", "70x9x7-closed"]
+         ((70, 9, 7), ALL_CLOSED), ((32, 48, 32), OPEN)]
+IDS = ["19x24x17-open", "40x36x70-closed", "38x48x38-open", "5x33x66-open", "70x9x7-closed", "32x48x32-open"]
 
 
 @pytest.fixture
@@ -39,7 +39,7 @@ def seeded_pair(cells, faces):
 
 @pytest.mark.parametrize("cells,faces", CASES, ids=IDS)
 @pytest.mark.parametrize("tiled_min", [1, 1 << 40])
-@pytest.mark.parametrize("bottom_max", [0, 8192])
+@pytest.mark.parametrize("bottom_max", [0, 2048, 8192])  # uniform levels of <= 2048 cells use register stencils
 def test_multigrid_strategies_match_the_oracle(tuning, cells, faces, tiled_min, bottom_max):
     from plume_b200.sim.multigrid import Multigrid, tune_solver
     from plume_b200.sim.pressure import project
