@@ -86,9 +86,11 @@ __global__ void k_brick_max(Dims d, const T* __restrict__ f, float* __restrict__
 // half-cell steps to the box edge and writes exp(-opacity * column * cell_m). With `bricks`, samples whose
 // corners are all <= 0 add exactly 0: the march steps over the whole run of them that lies in one brick.
 //
-// With `march_cells`, only the cells a camera march of the same smoke with this brick map can read get their
-// value: a march sample reads the eight corners of its lower corner cell c0 only when c0's brick is not empty,
-// so a cell c is read only if the brick of some c0 in {c-1, c}^3 is not empty. Every other cell gets 1.
+// With `march_cells`, only the cells a camera march of the same smoke can read get their value: a march sample
+// reads the light at its eight corners only when its alpha is > 0, so when one of those corners holds smoke
+// > 0; the corners of every sample that reads cell c lie in {c-1, c, c+1}^3. So c is read only if one of those
+// 27 cells holds smoke > 0 (tested first through the bricks of the lower corners {c-1, c}^3, which hold the
+// largest smoke of every such corner). Every other cell gets 1.
 template <class T>
 __global__ void k_light_volume(Dims d, const T* __restrict__ smoke, F3 toward, float cell_m, float opacity,
                                float* __restrict__ light, const float* __restrict__ bricks, int march_cells) {
@@ -100,6 +102,12 @@ __global__ void k_light_volume(Dims d, const T* __restrict__ smoke, F3 toward, f
     for (int a = imax_(i - 1, 0); a <= i; ++a)
       for (int b = imax_(j - 1, 0); b <= j; ++b)
         for (int c = imax_(k - 1, 0); c <= k; ++c) read |= __ldg(bricks + at(bd, a / BRICK, b / BRICK, c / BRICK)) > 0.0f;
+    if (read) {
+      read = false;
+      for (int a = imax_(i - 1, 0); a <= imin_(i + 1, d.n0 - 1); ++a)
+        for (int b = imax_(j - 1, 0); b <= imin_(j + 1, d.n1 - 1); ++b)
+          for (int c = imax_(k - 1, 0); c <= imin_(k + 1, d.n2 - 1); ++c) read |= ldg_f(smoke + at(d, a, b, c)) > 0.0f;
+    }
     if (!read) {
       light[at(d, i, j, k)] = 1.0f;
       return;

@@ -112,23 +112,15 @@ def test_march_empty_space_skipping_changes_no_bit(cuda_device, channels, glow_s
 
 
 def read_by_march(smoke: np.ndarray) -> np.ndarray:
-    """Cells whose light a march of `smoke` can read: a neighbour c0 in {c-1, c}^3 lies in a brick (4 cells and
-    the next past it on each axis) holding smoke > 0."""
+    """Cells whose light a march of `smoke` can read: one of the 27 cells around it holds smoke > 0 (a sample
+    reads the light at its corners only when one of them holds smoke > 0)."""
     n = smoke.shape
-    nb = tuple((x + 3) // 4 for x in n)
-    brick = np.zeros(nb, dtype=bool)
-    for b in np.ndindex(*nb):
-        lo = [4 * b[a] for a in range(3)]
-        hi = [min(4 * b[a] + 5, n[a]) for a in range(3)]
-        brick[b] = smoke[lo[0]:hi[0], lo[1]:hi[1], lo[2]:hi[2]].max() > 0
-    lit = brick[np.ix_(*[np.arange(x) // 4 for x in n])]
-    read = lit.copy()
-    for da in (0, 1):
-        for db in (0, 1):
-            for dc in (0, 1):
-                shifted = np.zeros_like(lit)
-                shifted[da:, db:, dc:] = lit[:n[0] - da, :n[1] - db, :n[2] - dc]
-                read |= shifted
+    padded = np.pad(smoke > 0, 1)
+    read = np.zeros(n, dtype=bool)
+    for a in range(3):
+        for b in range(3):
+            for c in range(3):
+                read |= padded[a:a + n[0], b:b + n[1], c:c + n[2]]
     return read
 
 
