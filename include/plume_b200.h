@@ -221,6 +221,23 @@ int plume_use_graphs(int32_t enable);
 /* multigrid.py:36-43 residual_kernel. */
 int plume_residual(const PlumeGridInfo* info, const float* q, const float* rhs, float* residual, void* stream);
 
+/* ---- solving to a residual (no reference counterpart: the reference runs a fixed number of cycles) --------
+ * Defect correction: the residual r = rhs - A q of the float pressure is evaluated in double, the correction
+ * e solves A e = r by one float V-cycle from e = 0 whose coarsest level is swept in double, and q += e.
+ *
+ * The pressure may be carried as the unevaluated sum of two floats, q + q_lo (q_lo null for q alone), so that
+ * the iterate can go below the float rounding of q: the correction is added as a two-sum and renormalised.
+ *
+ * plume_residual_f64 stores r (as float) in `residual` and writes norms[0] = sum r^2, norms[1] = sum rhs^2
+ * (device doubles, summed in a fixed order); `scratch` holds plume_norm_scratch_doubles(info) doubles.
+ * plume_multigrid_correct runs one correction: levels[0] is {info, q = e, rhs = r, residual = a scratch
+ * array}, the coarser levels as for plume_multigrid; `pressure` (+ `pressure_lo`) gets e added. */
+long long plume_norm_scratch_doubles(const PlumeGridInfo* info);
+int plume_residual_f64(const PlumeGridInfo* info, const float* q, const float* q_lo, const float* rhs,
+                       float* residual, double* scratch, double* norms, void* stream);
+int plume_multigrid_correct(const PlumeLevel* levels, int32_t level_count, int32_t sweeps, float* pressure,
+                            float* pressure_lo, void* stream);
+
 /* conserve.py:45-52 SmokeBudget.hold + reduce.py:28-38 TripleSum, on the device: totals of data, hat and next
  * (each line summed along x in float, the lines added in double in a fixed order), the held factor
  * max(sl, min(mc, before)) / mc (1 when mc <= 0) stored as float in *factor, and next *= factor.

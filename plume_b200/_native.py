@@ -110,6 +110,9 @@ SIGNATURES = {
     "plume_red_black_sweeps": [_INFO, _P, _P, _P, _I, _F, _P],
     "plume_multigrid": [ctypes.POINTER(PlumeLevel), _I, _I, _I, _P],
     "plume_residual": [_INFO, _P, _P, _P, _P],
+    "plume_norm_scratch_doubles": [_INFO],
+    "plume_residual_f64": [_INFO, _P, _P, _P, _P, _P, _P, _P],
+    "plume_multigrid_correct": [ctypes.POINTER(PlumeLevel), _I, _I, _P, _P, _P],
     "plume_tune_solver": [ctypes.c_longlong, ctypes.c_longlong, _I],
     "plume_solver_tuning": [ctypes.POINTER(ctypes.c_longlong), ctypes.POINTER(ctypes.c_longlong),
                             ctypes.POINTER(ctypes.c_int32)],
@@ -170,7 +173,7 @@ def lib() -> ctypes.CDLL:
         for name, argtypes in SIGNATURES.items():
             fn = getattr(loaded, name)
             fn.argtypes = argtypes
-            wide = name in ("plume_advect_scratch_floats", "plume_brick_floats")
+            wide = name in ("plume_advect_scratch_floats", "plume_brick_floats", "plume_norm_scratch_doubles")
             fn.restype = ctypes.c_longlong if wide else ctypes.c_int
         _lib = loaded
     return _lib

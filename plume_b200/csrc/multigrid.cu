@@ -468,7 +468,44 @@ struct BlockArgs {
   int sweeps;
   PlumeLevel lv[BOTTOM_MAX_LEVELS];
   int offset[BOTTOM_MAX_LEVELS];
+  int f64_offset;  // k_block_solve<true>: the coarsest level's double copy, from this float offset
 };
+
+// The coarsest level's sweeps in double (the defect-correction solve's correction cycles; no reference
+// counterpart): q and rhs widened into `dq`/`drhs`, the red-black sweeps of relaxed_f64 over the whole block,
+// q rounded back to float.
+__device__ __forceinline__ void coarsest_f64(const PlumeGridInfo& info, float* q, const float* rhs, int sweeps,
+                                             double relaxation, double* dq, double* drhs) {
+  const Dims d = dims_of(info);
+  const int n = d.n0 * d.n1 * d.n2;
+  for (int idx = threadIdx.x; idx < n; idx += blockDim.x) {
+    dq[idx] = q[idx];
+    drhs[idx] = rhs[idx];
+  }
+  __syncthreads();
+  auto load = [&](int a, int b, int c) { return dq[at(d, a, b, c)]; };
+  for (int s = 0; s < sweeps; ++s)
+    for (int color = 0; color < 2; ++color) {
+      for (int idx = threadIdx.x; idx < n; idx += blockDim.x) {
+        const int i = idx / (d.n1 * d.n2), r = idx - i * d.n1 * d.n2, j = r / d.n2, k = r - j * d.n2;
+        if (((i + j + k) & 1) != color) continue;
+        double out;
+        if (relaxed_f64(info, i, j, k, dq[idx], drhs[idx], relaxation, load, out)) dq[idx] = out;
+      }
+      __syncthreads();
+    }
+  for (int idx = threadIdx.x; idx < n; idx += blockDim.x) q[idx] = (float)dq[idx];
+  __syncthreads();
+}
+
+// The coarsest level in double when it is not inside the one-block solve: one block, arrays in global memory.
+__global__ void __launch_bounds__(BOTTOM_THREADS) k_coarsest_f64(PlumeGridInfo info, float* q, const float* rhs,
+                                                                 int sweeps) {
+  wait_for_previous_grid();
+  extern __shared__ double staged[];
+  const int n = info.dims[0] * info.dims[1] * info.dims[2];
+  coarsest_f64(info, q, rhs, sweeps, 1.5, staged, staged + n);
+}
 
 // Visits the index triples (i, j, c) of p = start, start + stride, ... in an (n0, n1, nc) box without a
 // division per step: one division at the start, then the stride's own (di, dj, dc) added with carries.
@@ -632,6 +669,7 @@ __device__ __forceinline__ void block_smooth(const PlumeGridInfo& info, float* q
   __syncthreads();
 }
 
+template <bool COARSE_F64>
 __global__ void __launch_bounds__(BOTTOM_THREADS) k_block_solve(BlockArgs b) {
   wait_for_previous_grid();
   extern __shared__ float smem[];
@@ -682,7 +720,14 @@ __global__ void __launch_bounds__(BOTTOM_THREADS) k_block_solve(BlockArgs b) {
     const Dims d = dims_of(info);
     float* q = smem + b.offset[b.count - 1];
     const int longest = imax_(d.n0, imax_(d.n1, d.n2));
-    block_smooth(info, q, q + d.n0 * d.n1 * d.n2, imax_(COARSEST_SWEEPS, COARSEST_SWEEPS_PER_CELL * longest), 1.5f);
+    const int n = d.n0 * d.n1 * d.n2;
+    const int sweeps = imax_(COARSEST_SWEEPS, COARSEST_SWEEPS_PER_CELL * longest);
+    if constexpr (COARSE_F64) {
+      double* staged = reinterpret_cast<double*>(smem + b.f64_offset);
+      coarsest_f64(info, q, q + n, sweeps, 1.5, staged, staged + n);
+    } else {
+      block_smooth(info, q, q + n, sweeps, 1.5f);
+    }
   }
   for (int l = b.count - 2; l >= 0; --l) {
     const PlumeGridInfo& info = b.lv[l].info;
@@ -822,16 +867,23 @@ int red_black_sweeps(const PlumeGridInfo& info, float* q, float* scratch, const 
 
 // The first level from which the rest of the hierarchy runs in one cluster launch (count when none fits),
 // and that launch's per-CTA shared memory.
-static int bottom_start(const PlumeLevel* levels, int count, size_t* smem_bytes) {
+// With coarse_f64 the one-block solve is used (it holds the double copy of the coarsest level after the
+// float arrays, 8-byte aligned).
+static int bottom_kind(int coarse_f64) { return coarse_f64 ? 0 : g_bottom_kind; }
+
+static size_t f64_staging_offset(size_t float_bytes) { return (float_bytes + 7) / 8 * 8; }
+
+static int bottom_start(const PlumeLevel* levels, int count, size_t* smem_bytes, int coarse_f64) {
   for (int first = 0; first < count; ++first) {
     if (count - first > BOTTOM_MAX_LEVELS || cells_of(levels[first].info) > g_bottom_max_cells) continue;
     size_t bytes = 0;
     for (int l = first; l < count; ++l) {
       const PlumeGridInfo& info = levels[l].info;
-      const bool single = g_bottom_kind == 0 || cells_of(info) <= SINGLE_MAX_CELLS;
+      const bool single = bottom_kind(coarse_f64) == 0 || cells_of(info) <= SINGLE_MAX_CELLS;
       const long planes = single ? info.dims[0] : (info.dims[0] + CLUSTER - 1) / CLUSTER;
       bytes += 2 * sizeof(float) * (size_t)planes * info.dims[1] * info.dims[2];
     }
+    if (coarse_f64) bytes = f64_staging_offset(bytes) + 2 * sizeof(double) * (size_t)cells_of(levels[count - 1].info);
     if (bytes > BOTTOM_MAX_SMEM) continue;
     *smem_bytes = bytes;
     return first;
@@ -853,7 +905,15 @@ static int prepare_bottom() {
                                                  (int)BOTTOM_MAX_SMEM));
     if (status == PLUME_OK)
       status = runtime_status("coarse solve shared memory",
-                              cudaFuncSetAttribute(k_block_solve, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                              cudaFuncSetAttribute(k_block_solve<false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                                   (int)BOTTOM_MAX_SMEM));
+    if (status == PLUME_OK)
+      status = runtime_status("coarse solve shared memory",
+                              cudaFuncSetAttribute(k_block_solve<true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                                   (int)BOTTOM_MAX_SMEM));
+    if (status == PLUME_OK)
+      status = runtime_status("coarse solve shared memory",
+                              cudaFuncSetAttribute(k_coarsest_f64, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                                    (int)BOTTOM_MAX_SMEM));
     if (status != PLUME_OK) return status;
     configured[device] = true;
@@ -861,10 +921,11 @@ static int prepare_bottom() {
   return PLUME_OK;
 }
 
-static int launch_bottom(const PlumeLevel* levels, int count, int sweeps, size_t smem, cudaStream_t st) {
+static int launch_bottom(const PlumeLevel* levels, int count, int sweeps, size_t smem, cudaStream_t st,
+                         int coarse_f64) {
   int status = prepare_bottom();
   if (status != PLUME_OK) return status;
-  if (g_bottom_kind == 0) {
+  if (bottom_kind(coarse_f64) == 0) {
     BlockArgs b{};
     b.count = count;
     b.sweeps = sweeps;
@@ -874,7 +935,9 @@ static int launch_bottom(const PlumeLevel* levels, int count, int sweeps, size_t
       b.offset[l] = offset;
       offset += 2 * (int)cells_of(levels[l].info);
     }
-    return launch_solve_kernel(k_block_solve, dim3(1), dim3(BOTTOM_THREADS), smem, st, "coarse-level block solve", b);
+    b.f64_offset = (int)(f64_staging_offset(sizeof(float) * (size_t)offset) / sizeof(float));
+    return launch_solve_kernel(coarse_f64 ? k_block_solve<true> : k_block_solve<false>, dim3(1), dim3(BOTTOM_THREADS),
+                               smem, st, "coarse-level block solve", b);
   }
   ClusterArgs b{};
   b.count = count;
@@ -910,16 +973,24 @@ static int launch_bottom(const PlumeLevel* levels, int count, int sweeps, size_t
 // One V-cycle below `index` (multigrid.py:130-147). Every level keeps its pressure in q and uses its residual
 // array as the sweeps' second array; the residual itself is never stored (k_residual_restrict).
 static int v_cycle(const PlumeLevel* levels, int count, int index, Pressure& q, int bottom, size_t smem, int sweeps,
-                   cudaStream_t st) {
+                   cudaStream_t st, int coarse_f64) {
   const PlumeLevel& lv = levels[index];
   if (index == bottom) {
     PlumeLevel first[BOTTOM_MAX_LEVELS];
     for (int l = bottom; l < count && l - bottom < BOTTOM_MAX_LEVELS; ++l) first[l - bottom] = levels[l];
     first[0].q = q.cur;
-    return launch_bottom(first, count - bottom, sweeps, smem, st);
+    return launch_bottom(first, count - bottom, sweeps, smem, st, coarse_f64);
   }
   if (index == count - 1) {
     const int longest = std::max(lv.info.dims[0], std::max(lv.info.dims[1], lv.info.dims[2]));
+    if (coarse_f64) {
+      const size_t bytes = 2 * sizeof(double) * (size_t)cells_of(lv.info);
+      if (bytes > BOTTOM_MAX_SMEM) return fail(PLUME_ERR_INVALID, "coarsest level too large for the double solve");
+      int status = prepare_bottom();
+      if (status != PLUME_OK) return status;
+      return launch_solve_kernel(k_coarsest_f64, dim3(1), dim3(BOTTOM_THREADS), bytes, st, "coarsest double solve",
+                                 lv.info, q.cur, lv.rhs, std::max(COARSEST_SWEEPS, COARSEST_SWEEPS_PER_CELL * longest));
+    }
     return sweeps_with_prolong(lv.info, q, lv.rhs, std::max(COARSEST_SWEEPS, COARSEST_SWEEPS_PER_CELL * longest), 1.5f,
                                nullptr, nullptr, st);
   }
@@ -932,7 +1003,8 @@ static int v_cycle(const PlumeLevel* levels, int count, int index, Pressure& q, 
       PLUME_OK)
     return status;
   Pressure coarse_q{coarse.q, coarse.residual};
-  if ((status = v_cycle(levels, count, index + 1, coarse_q, bottom, smem, sweeps, st)) != PLUME_OK) return status;
+  if ((status = v_cycle(levels, count, index + 1, coarse_q, bottom, smem, sweeps, st, coarse_f64)) != PLUME_OK)
+    return status;
   if (coarse_q.cur != coarse.q) {  // an odd number of coarsest sweeps left the result in the second array
     status = runtime_status("coarse pressure copy", cudaMemcpyAsync(coarse.q, coarse_q.cur, sizeof(float) * cd.n0 * cd.n1 * cd.n2,
                                                                     cudaMemcpyDeviceToDevice, st));
@@ -941,12 +1013,13 @@ static int v_cycle(const PlumeLevel* levels, int count, int index, Pressure& q, 
   return sweeps_with_prolong(lv.info, q, lv.rhs, sweeps, 1.0f, coarse.q, &coarse.info, st);
 }
 
-static int multigrid_direct(const PlumeLevel* levels, int count, int cycles, int sweeps, cudaStream_t st) {
+static int multigrid_direct(const PlumeLevel* levels, int count, int cycles, int sweeps, cudaStream_t st,
+                            int coarse_f64) {
   size_t smem = 0;
-  const int bottom = bottom_start(levels, count, &smem);
+  const int bottom = bottom_start(levels, count, &smem, coarse_f64);
   Pressure q{levels[0].q, levels[0].residual};
   for (int c = 0; c < cycles; ++c) {
-    int status = v_cycle(levels, count, 0, q, bottom, smem, sweeps, st);
+    int status = v_cycle(levels, count, 0, q, bottom, smem, sweeps, st, coarse_f64);
     if (status != PLUME_OK) return status;
   }
   if (q.cur == levels[0].q) return PLUME_OK;
@@ -965,7 +1038,7 @@ namespace plume {
 // V-cycle, most of them short.
 struct GraphKey {
   int device;
-  int count, cycles, sweeps, kind;
+  int count, cycles, sweeps, kind, coarse_f64;
   long tiled, bottom;
   PlumeLevel levels[16];
   bool operator==(const GraphKey& o) const { return std::memcmp(this, &o, sizeof(GraphKey)) == 0; }
@@ -1007,7 +1080,7 @@ static int graph_for(const GraphKey& key, const PlumeLevel* levels, cudaGraphExe
   status = runtime_status("begin capture", cudaStreamBeginCapture(cap, cudaStreamCaptureModeThreadLocal));
   if (status != PLUME_OK) return status;
   set_launch_counting(false);
-  const int run = multigrid_direct(levels, key.count, key.cycles, key.sweeps, cap);
+  const int run = multigrid_direct(levels, key.count, key.cycles, key.sweeps, cap, key.coarse_f64);
   set_launch_counting(true);
   cudaGraph_t graph = nullptr;
   status = runtime_status("end capture", cudaStreamEndCapture(cap, &graph));
@@ -1038,12 +1111,12 @@ static int graph_for(const GraphKey& key, const PlumeLevel* levels, cudaGraphExe
   return PLUME_OK;
 }
 
-int multigrid_cycles(const PlumeLevel* levels, int count, int cycles, int sweeps, cudaStream_t st) {
+int multigrid_cycles(const PlumeLevel* levels, int count, int cycles, int sweeps, cudaStream_t st, int coarse_f64) {
   cudaStreamCaptureStatus capturing = cudaStreamCaptureStatusNone;
   int device = 0;
   if (!g_use_graphs || count > 16 || cudaStreamIsCapturing(st, &capturing) != cudaSuccess ||
       capturing != cudaStreamCaptureStatusNone || cudaGetDevice(&device) != cudaSuccess || device < 0 || device >= 64)
-    return multigrid_direct(levels, count, cycles, sweeps, st);
+    return multigrid_direct(levels, count, cycles, sweeps, st, coarse_f64);
   GraphKey key;
   std::memset(&key, 0, sizeof(key));
   key.device = device;
@@ -1051,13 +1124,14 @@ int multigrid_cycles(const PlumeLevel* levels, int count, int cycles, int sweeps
   key.cycles = cycles;
   key.sweeps = sweeps;
   key.kind = g_bottom_kind;
+  key.coarse_f64 = coarse_f64;
   key.tiled = g_tiled_min_cells;
   key.bottom = g_bottom_max_cells;
   std::memcpy(key.levels, levels, sizeof(PlumeLevel) * count);
   std::lock_guard<std::mutex> lock(g_graph_mutex);
   {  // the coarse solve's shared-memory attribute must be set before its first capture
     size_t smem = 0;
-    if (bottom_start(levels, count, &smem) < count) {
+    if (bottom_start(levels, count, &smem, coarse_f64) < count || coarse_f64) {
       int prepared = prepare_bottom();
       if (prepared != PLUME_OK) return prepared;
     }

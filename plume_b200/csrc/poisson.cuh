@@ -172,6 +172,64 @@ __device__ __forceinline__ float sample_plain(const float* f, const Dims& d, F3 
   return lerpf_(lerpf_(c00, c10, ty), lerpf_(c01, c11, ty), tz);
 }
 
+// ---- the same stencil in double (no reference counterpart) -------------------------------------------------
+// The defect-correction solve evaluates the residual, and sweeps the coarsest level, in double: the couplings
+// and sums of neighbor_sum / relaxed / residual_at with the level's float geometry widened to double.
+template <class Load>
+__device__ __forceinline__ void neighbor_sum_f64(const PlumeGridInfo& info, int i, int j, int k, Load load, double& sq,
+                                                 double& sc) {
+  const int c[3] = {i, j, k};
+  sq = 0.0;
+  sc = 0.0;
+#pragma unroll
+  for (int axis = 0; axis < 3; ++axis) {
+    double area = 1.0;
+#pragma unroll
+    for (int other = 0; other < 3; ++other)
+      if (other != axis) area = area * (double)cell_fill(info, other, c[other]);
+    const double own = cell_fill(info, axis, c[axis]);
+#pragma unroll
+    for (int side = 0; side < 2; ++side) {
+      const int step = side == 0 ? -1 : 1;
+      const int n = c[axis] + step;
+      if (n >= 0 && n < info.dims[axis]) {
+        const double coupling = area / (0.5 * (own + (double)cell_fill(info, axis, n)));
+        const double neighbour = axis == 0 ? load(n, j, k) : (axis == 1 ? load(i, n, k) : load(i, j, n));
+        sq = sq + coupling * neighbour;
+        sc = sc + coupling;
+      } else if ((step < 0 && info.open_lo[axis] == 1) || (step > 0 && info.open_hi[axis] == 1)) {
+        sc = sc + area / (0.5 * own + (double)info.ghost_gap);
+      }
+    }
+  }
+}
+
+__device__ __forceinline__ double cell_scale_f64(const PlumeGridInfo& info, int i, int j, int k) {
+  const double cell_m = info.cell_m;
+  return (double)cell_fill(info, 0, i) * (double)cell_fill(info, 1, j) * (double)cell_fill(info, 2, k) * cell_m * cell_m;
+}
+
+// rhs - A q in double.
+template <class Load>
+__device__ __forceinline__ double residual_f64(const PlumeGridInfo& info, int i, int j, int k, double q, double rhs,
+                                               Load load) {
+  double sq, sc;
+  neighbor_sum_f64(info, i, j, k, load, sq, sc);
+  return rhs - (sq - sc * q) / cell_scale_f64(info, i, j, k);
+}
+
+// One red-black update in double; false for a cell with no coupling.
+template <class Load>
+__device__ __forceinline__ bool relaxed_f64(const PlumeGridInfo& info, int i, int j, int k, double q, double rhs,
+                                            double relaxation, Load load, double& out) {
+  double sq, sc;
+  neighbor_sum_f64(info, i, j, k, load, sq, sc);
+  if (sc == 0.0) return false;
+  const double target = (sq - cell_scale_f64(info, i, j, k) * rhs) / sc;
+  out = q + relaxation * (target - q);
+  return true;
+}
+
 // Where a fine cell centre sits in its coarse level's index space (multigrid.py:66-67).
 __device__ __forceinline__ F3 prolong_point(int i, int j, int k) {
   return sub3(mul3(f3((float)i, (float)j, (float)k), 0.5f), f3(0.25f, 0.25f, 0.25f));
@@ -180,6 +238,7 @@ __device__ __forceinline__ F3 prolong_point(int i, int j, int k) {
 // Host side of the pressure solve (multigrid.cu).
 int red_black_sweeps(const PlumeGridInfo& info, float* q, float* scratch, const float* rhs, int sweeps,
                      float relaxation, cudaStream_t st);
-int multigrid_cycles(const PlumeLevel* levels, int count, int cycles, int sweeps, cudaStream_t st);
+// coarse_f64: sweep the coarsest level in double (the defect-correction solve's correction cycles)
+int multigrid_cycles(const PlumeLevel* levels, int count, int cycles, int sweeps, cudaStream_t st, int coarse_f64 = 0);
 
 }  // namespace plume

@@ -609,6 +609,93 @@ __global__ void k_residual(PlumeGridInfo info, const float* __restrict__ q, cons
   res[idx] = residual_at(info, i, j, k, __ldg(q + idx), __ldg(rhs + idx), load);
 }
 
+// ---- the defect-correction solve's residual (no reference counterpart) --------------------------------------
+// r = rhs - A q evaluated in double (residual_f64), stored as float for the correction cycle, with the block
+// sums of r^2 and rhs^2 (double, a halving tree over the block's 256 threads); k_norm_finish adds the block
+// partials in a fixed order, so the norms are the same on every run. With `q_lo`, the pressure is the
+// unevaluated sum q + q_lo of two floats (the refinement's compensated iterate).
+constexpr int NORM_THREADS = TZ * TY;
+
+__global__ void k_residual_f64(PlumeGridInfo info, const float* __restrict__ q, const float* __restrict__ q_lo,
+                               const float* __restrict__ rhs, float* __restrict__ res, double* __restrict__ partial) {
+  __shared__ double rr[NORM_THREADS], bb[NORM_THREADS];
+  const int ny = info.dims[1], nz = info.dims[2];
+  const int i = blockIdx.z, j = blockIdx.y * blockDim.y + threadIdx.y, k = blockIdx.x * blockDim.x + threadIdx.x;
+  const int t = threadIdx.y * blockDim.x + threadIdx.x;
+  double r = 0.0, b = 0.0;
+  if (j < ny && k < nz) {
+    const Dims d{info.dims[0], ny, nz};
+    auto value = [&](int c) { return (double)__ldg(q + c) + (q_lo ? (double)__ldg(q_lo + c) : 0.0); };
+    auto load = [&](int a, int bb_, int c) { return value(at(d, a, bb_, c)); };
+    const int idx = (i * ny + j) * nz + k;
+    b = __ldg(rhs + idx);
+    r = residual_f64(info, i, j, k, value(idx), b, load);
+    res[idx] = (float)r;
+  }
+  rr[t] = r * r;
+  bb[t] = b * b;
+  __syncthreads();
+  for (int half = NORM_THREADS / 2; half > 0; half /= 2) {
+    if (t < half) {
+      rr[t] = rr[t] + rr[t + half];
+      bb[t] = bb[t] + bb[t + half];
+    }
+    __syncthreads();
+  }
+  if (t == 0) {
+    const long block = blockIdx.x + (long)gridDim.x * (blockIdx.y + (long)gridDim.y * blockIdx.z);
+    partial[2 * block] = rr[0];
+    partial[2 * block + 1] = bb[0];
+  }
+}
+
+__global__ void k_norm_finish(const double* __restrict__ partial, long blocks, double* __restrict__ norms) {
+  __shared__ double rr[NORM_THREADS], bb[NORM_THREADS];
+  const int t = threadIdx.x;
+  double r = 0.0, b = 0.0;
+  for (long n = t; n < blocks; n += NORM_THREADS) {
+    r = r + partial[2 * n];
+    b = b + partial[2 * n + 1];
+  }
+  rr[t] = r;
+  bb[t] = b;
+  __syncthreads();
+  for (int half = NORM_THREADS / 2; half > 0; half /= 2) {
+    if (t < half) {
+      rr[t] = rr[t] + rr[t + half];
+      bb[t] = bb[t] + bb[t + half];
+    }
+    __syncthreads();
+  }
+  if (t == 0) {
+    norms[0] = rr[0];
+    norms[1] = bb[0];
+  }
+}
+
+// q += e; with q_lo, (q, q_lo) += e as a float pair: the rounding error of q + e (Knuth's two-sum) joins
+// q_lo, then the pair is renormalised so that q is the float nearest q + q_lo.
+__global__ void k_add_into(float* __restrict__ q, float* __restrict__ q_lo, const float* __restrict__ e, long n) {
+  const long idx = blockIdx.x * (long)blockDim.x + threadIdx.x;
+  if (idx >= n) return;
+  const float a = q[idx], b = e[idx];
+  const float s = a + b;
+  if (!q_lo) {
+    q[idx] = s;
+    return;
+  }
+  const float bv = s - a;
+  const float err = (a - (s - bv)) + (b - bv);
+  const float lo = q_lo[idx] + err;
+  const float hi = s + lo;
+  q[idx] = hi;
+  q_lo[idx] = lo - (hi - s);
+}
+
+static long norm_blocks(const PlumeGridInfo& info) {
+  const dim3 g = cell_grid(info.dims[0], info.dims[1], info.dims[2]);
+  return (long)g.x * g.y * g.z;
+}
 
 // ---- smoke budget: conserve.py:33-52 + reduce.py:12-38 ------------------------------------------------------
 // Line totals along x in float (reduce.py:12-25); lines added in double in blocks of 256 by a halving tree,
@@ -888,6 +975,41 @@ extern "C" int plume_residual(const PlumeGridInfo* info, const float* q, const f
   const int nx = info->dims[0], ny = info->dims[1], nz = info->dims[2];
   k_residual<<<cell_grid(nx, ny, nz), cell_block(), 0, as_stream(stream)>>>(*info, q, rhs, residual);
   return launch_status("residual");
+}
+
+extern "C" long long plume_norm_scratch_doubles(const PlumeGridInfo* info) {
+  if (!info || !valid_dims(info->dims)) return fail(PLUME_ERR_INVALID, "norm_scratch_doubles: bad dims");
+  return 2 * (long long)norm_blocks(*info);
+}
+
+extern "C" int plume_residual_f64(const PlumeGridInfo* info, const float* q, const float* q_lo, const float* rhs,
+                                  float* residual, double* scratch, double* norms, void* stream) {
+  CHECK_ARG(info && q && rhs && residual && scratch && norms, "residual_f64: null argument");
+  CHECK_ARG(valid_dims(info->dims), "residual_f64: bad dims");
+  cudaStream_t st = as_stream(stream);
+  const int nx = info->dims[0], ny = info->dims[1], nz = info->dims[2];
+  k_residual_f64<<<cell_grid(nx, ny, nz), cell_block(), 0, st>>>(*info, q, q_lo, rhs, residual, scratch);
+  int status = launch_status("residual (double)");
+  if (status != PLUME_OK) return status;
+  k_norm_finish<<<1, NORM_THREADS, 0, st>>>(scratch, norm_blocks(*info), norms);
+  return launch_status("residual norms");
+}
+
+extern "C" int plume_multigrid_correct(const PlumeLevel* levels, int32_t level_count, int32_t sweeps, float* pressure,
+                                       float* pressure_lo, void* stream) {
+  CHECK_ARG(levels && level_count >= 1 && sweeps >= 0 && pressure && pressure_lo != pressure,
+            "multigrid_correct: bad argument");
+  for (int l = 0; l < level_count; ++l)
+    CHECK_ARG(levels[l].q && levels[l].rhs && levels[l].residual && levels[l].residual != levels[l].q &&
+                  levels[l].q != pressure && levels[l].q != pressure_lo && valid_dims(levels[l].info.dims),
+              "multigrid_correct: bad level %d", l);
+  cudaStream_t st = as_stream(stream);
+  const long n = (long)levels[0].info.dims[0] * levels[0].info.dims[1] * levels[0].info.dims[2];
+  int status = runtime_status("correction clear", cudaMemsetAsync(levels[0].q, 0, sizeof(float) * n, st));
+  if (status != PLUME_OK) return status;
+  if ((status = multigrid_cycles(levels, level_count, 1, sweeps, st, 1)) != PLUME_OK) return status;
+  k_add_into<<<(unsigned)((n + 255) / 256), 256, 0, st>>>(pressure, pressure_lo, levels[0].q, n);
+  return launch_status("correction add");
 }
 
 extern "C" long long plume_advect_scratch_floats(const PlumeGridInfo* info) {

@@ -5,6 +5,7 @@ Cell-centred V-cycles with averaging restriction and trilinear prolongation. Lev
 last cell is weighted by the share inside the domain (`fill_hi`). The whole V-cycle runs in one library call.
 """
 
+import math
 from dataclasses import dataclass
 
 import torch
@@ -51,6 +52,21 @@ class Level:
     residual: torch.Tensor
 
 
+@dataclass(frozen=True)
+class Refinement:
+    """What Multigrid.refine did: the correction cycles run; ||rhs - A q|| / ||rhs|| (double precision, 2-norms)
+    of the iterate before the first correction and after each one; and that ratio for the float pressure
+    left in grid.pressure (the iterate rounded to float)."""
+
+    corrections: int
+    ratios: tuple
+    float_ratio: float
+
+    @property
+    def ratio(self) -> float:
+        return self.ratios[-1]
+
+
 def coarse_cells(cells):
     return tuple((n + 1) // 2 for n in cells)
 
@@ -71,6 +87,7 @@ class Multigrid:
         self.device = grid.device
         self.levels = self._build_levels(grid)
         self._native_levels = None
+        self._refine = None
 
     def _build_levels(self, grid):
         levels = [Level(grid.info, grid.cells, grid.pressure, grid.divergence,
@@ -101,6 +118,54 @@ class Multigrid:
     def __call__(self, grid) -> None:
         levels = self.native_levels(grid)
         N.call("plume_multigrid", levels, len(self.levels), self.cycles, self.sweeps, N.stream())
+
+    def refine(self, grid, rel_tol: float = 1e-7, max_corrections: int = 40, compensated: bool = True) -> Refinement:
+        """Solves to a relative residual by defect correction (no reference counterpart; the reference runs a
+        fixed number of V-cycles). Each correction evaluates r = divergence - A pressure in double, solves
+        A e = r with one float V-cycle from e = 0 whose coarsest level is swept in double, and adds e to the
+        pressure. With `compensated` the iterate is grid.pressure + a second float array of its rounding error
+        (two-sum), so it can go below the float pressure's own rounding floor (about 4e-7 on the seeded
+        operator fields); grid.pressure always holds the iterate rounded to float. Stops at
+        ||r|| / ||divergence|| <= rel_tol, after max_corrections, or when a correction improves the ratio by
+        less than 5%."""
+        self.native_levels(grid)
+        top = self.levels[0]
+        if self._refine is None or self._refine["e"].shape != grid.pressure.shape:
+            cells = grid.cells
+            blocks = N.lib().plume_norm_scratch_doubles(N.ctypes.byref(top.info))
+            self._refine = {name: torch.zeros(cells, dtype=torch.float32, device=self.device) for name in ("e", "r", "ping")}
+            self._refine["scratch"] = torch.empty(blocks, dtype=torch.float64, device=self.device)
+            self._refine["norms"] = torch.zeros(2, dtype=torch.float64, device=self.device)
+            self._refine["lo"] = torch.zeros(cells, dtype=torch.float32, device=self.device)
+        arrays = self._refine
+        arrays["lo"].zero_()
+        lo = N.ptr(arrays["lo"]) if compensated else None
+        levels = (N.PlumeLevel * len(self.levels))()
+        for index, (slot, level) in enumerate(zip(levels, self.levels)):
+            slot.info = level.info
+            if index == 0:
+                slot.q, slot.rhs, slot.residual = (N.ptr(arrays[name]).value for name in ("e", "r", "ping"))
+            else:
+                slot.q, slot.rhs, slot.residual = (N.ptr(t).value for t in (level.q, level.rhs, level.residual))
+
+        def measure(low) -> float:
+            N.call("plume_residual_f64", top.info, N.ptr(grid.pressure), low, N.ptr(grid.divergence),
+                   N.ptr(arrays["r"]), N.ptr(arrays["scratch"], torch.float64), N.ptr(arrays["norms"], torch.float64),
+                   N.stream())
+            rr, bb = (float(x) for x in arrays["norms"].cpu())
+            return 0.0 if bb == 0.0 else math.sqrt(rr / bb)
+
+        ratios = [measure(lo)]
+        corrections = 0
+        while ratios[-1] > rel_tol and corrections < max_corrections:
+            N.call("plume_multigrid_correct", levels, len(self.levels), self.sweeps, N.ptr(grid.pressure), lo,
+                   N.stream())
+            corrections += 1
+            ratios.append(measure(lo))
+            if ratios[-1] > 0.95 * ratios[-2]:
+                break
+        float_ratio = measure(None) if compensated else ratios[-1]
+        return Refinement(corrections, tuple(ratios), float_ratio)
 
     def residual(self, level_index: int = 0) -> torch.Tensor:
         """Fills and returns one level's residual rhs - A q (multigrid.py:36-43)."""

@@ -51,6 +51,16 @@ def project(grid, solve) -> None:
     N.call("plume_subtract_gradient", grid.info, N.ptr(u), N.ptr(v), N.ptr(w), N.ptr(grid.pressure), N.stream())
 
 
+def project_refined(grid, multigrid, rel_tol: float = 1e-6, max_corrections: int = 40):
+    """project() with the pressure solved to a relative residual by multigrid.refine (defect correction; no
+    reference counterpart). Returns the Refinement."""
+    u, v, w = (f.data for f in grid.velocity_fields())
+    N.call("plume_project_begin", grid.info, N.ptr(u), N.ptr(v), N.ptr(w), N.ptr(grid.divergence), N.stream())
+    refinement = multigrid.refine(grid, rel_tol, max_corrections)
+    N.call("plume_subtract_gradient", grid.info, N.ptr(u), N.ptr(v), N.ptr(w), N.ptr(grid.pressure), N.stream())
+    return refinement
+
+
 def compute_divergence(grid):
     """Fills and returns grid.divergence from the current face velocities."""
     u, v, w = (f.data for f in grid.velocity_fields())
