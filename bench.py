@@ -265,6 +265,157 @@ def adjoint_variant(device: str) -> dict:
             "adjoint_over_forward": backward / forward}
 
 
+def square_view(view, pixels: int):
+    """The domain view re-sampled to pixels x pixels, the whole domain inside (the larger side fits)."""
+    import dataclasses
+
+    extent = max(view.width_px, view.height_px) * view.pixel_m
+    return dataclasses.replace(view, pixel_m=extent / pixels, width_px=pixels, height_px=pixels)
+
+
+def device_ms(fn) -> float:
+    """Device time of fn() on the current stream (CUDA events, synchronised)."""
+    import torch
+
+    start, end = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    torch.cuda.synchronize()
+    start.record()
+    fn()
+    end.record()
+    torch.cuda.synchronize()
+    return start.elapsed_time(end)
+
+
+def operators_variant(recipe, derived, fields, device: str) -> dict:
+    """The operator-level case's single calls on its seeded fields: MacCormack advection of the five fields
+    (dt = 1/96 s), buoyancy + vorticity confinement, a projection of the resulting divergence solved to
+    relative residual 1e-6 by defect correction, and a 256 x 256 orthographic march (light volume + march);
+    device milliseconds of each, the projection's corrections and residual ratios."""
+    import torch
+
+    from plume_b200.render.camera import sheet_domain_view
+    from plume_b200.render.frame_renderer import FrameRenderer
+    from plume_b200.sim.advect import advect_maccormack
+    from plume_b200.sim.forces import apply_buoyancy
+    from plume_b200.sim.grid import make_grid
+    from plume_b200.sim.multigrid import Multigrid
+    from plume_b200.sim.pressure import project_refined
+    from plume_b200.sim.vorticity import VorticityConfinement
+
+    d, f = recipe.domain, recipe.forces
+    grid = make_grid(derived, d.cell_m, d.faces, d.ambient_k, device)
+    for name, values in fields.items():
+        getattr(grid, name).data.copy_(torch.from_numpy(values))
+    dt = derived.dt_s
+    velocity = tuple(field.data for field in grid.velocity_fields())
+
+    def advect():
+        for name in ("u", "v", "w", "smoke", "temperature"):
+            advect_maccormack(getattr(grid, name), velocity, grid, dt)
+
+    confinement = VorticityConfinement(grid)
+
+    def forces():
+        apply_buoyancy(grid, f.gravity_mps2, f.heat_buoyancy, f.smoke_weight, d.ambient_k, dt)
+        confinement.apply(grid, f.vorticity_confinement, dt)
+
+    advect()  # warm-up (allocations)
+    forces()
+    advect_ms, forces_ms = device_ms(advect), device_ms(forces)
+    multigrid = Multigrid(grid, recipe.solver.multigrid_cycles, recipe.solver.multigrid_sweeps)
+    grid.pressure.zero_()
+    torch.cuda.synchronize()
+    start = time.perf_counter()
+    refinement = project_refined(grid, multigrid, rel_tol=1e-6)
+    torch.cuda.synchronize()
+    project_ms = (time.perf_counter() - start) * 1e3
+    view = square_view(sheet_domain_view(recipe, derived), 256)
+    renderer = FrameRenderer(view, recipe.render, derived.cells, recipe.output.channels, device)
+    renderer.render(grid)
+    render_ms = device_ms(lambda: (renderer.prepare(grid.smoke.data, grid.info.cell_m),
+                                   renderer.march(grid.smoke.data, grid.temperature.data, grid.info,
+                                                  renderer.view_params, renderer.image)))
+    return {"cells": list(derived.cells), "advect_five_fields_ms": advect_ms, "buoyancy_confinement_ms": forces_ms,
+            "projection": {"rel_tol": 1e-6, "corrections": refinement.corrections, "ratio": refinement.ratio,
+                           "ratios": list(refinement.ratios), "ms_with_host_syncs": project_ms},
+            "march_256x256_ms": render_ms}
+
+
+def large_mixed_variant(device: str, steps: int = 8, frames: int = 2) -> dict:
+    """The large mixed-precision case at 256 x 384 x 256 (dx = 1/128 m, emitter radius 24 cells), seeded on the
+    device: the fields stored as bfloat16 (float arithmetic) against the plain FP32 GPU run of the same state.
+    Mcell-substeps/s of each; the projection of the FP32 state's divergence refined to relative residual 1e-7
+    (defect correction, the pressure as a compensated float pair); a 512 x 512 march; and after `frames`
+    frames of 4 substeps, the largest per-frame thickness and heat difference of the bfloat16 run from the FP32
+    run (heat relative to the FP32 frame's largest heat)."""
+    import numpy as np
+    import torch
+
+    from plume_b200.recipe.derived import derive
+    from plume_b200.render.camera import sheet_domain_view
+    from plume_b200.render.frame_renderer import FrameRenderer
+    from plume_b200.sim.grid import make_grid
+    from plume_b200.sim.multigrid import Multigrid
+    from plume_b200.sim.pressure import compute_divergence
+    from plume_b200.sim.stepper import Stepper
+    from plume_b200.workloads import device_operator_fields, plain_step_recipe
+
+    cells = (256, 384, 256)
+    recipe = plain_step_recipe(cells)
+    derived = derive(recipe)
+    d = recipe.domain
+    fields = device_operator_fields(cells, 20261203, d.ambient_k, device)
+    view = square_view(sheet_domain_view(recipe, derived), 512)
+    out, runs = {"cells": list(cells)}, {}
+    for label, storage in (("f32", torch.float32), ("bf16", torch.bfloat16)):
+        grid = make_grid(derived, d.cell_m, d.faces, d.ambient_k, device, storage=storage)
+        for name, values in fields.items():
+            getattr(grid, name).data.copy_(values)
+        if label == "f32":
+            multigrid = Multigrid(grid, recipe.solver.multigrid_cycles, recipe.solver.multigrid_sweeps)
+            compute_divergence(grid)
+            grid.pressure.zero_()
+            torch.cuda.synchronize()
+            start = time.perf_counter()
+            refinement = multigrid.refine(grid, rel_tol=1e-7)
+            torch.cuda.synchronize()
+            out["projection"] = {"rel_tol": 1e-7, "corrections": refinement.corrections, "ratio": refinement.ratio,
+                                 "float_ratio": refinement.float_ratio,
+                                 "ms_with_host_syncs": (time.perf_counter() - start) * 1e3}
+            grid.pressure.zero_()
+            renderer = FrameRenderer(view, recipe.render, derived.cells, recipe.output.channels, device)
+            renderer.render(grid)
+            out["march_512x512_ms"] = device_ms(lambda: (
+                renderer.prepare(grid.smoke.data, grid.info.cell_m),
+                renderer.march(grid.smoke.data, grid.temperature.data, grid.info, renderer.view_params,
+                               renderer.image)))
+        stepper = Stepper(grid, recipe)
+        for n in range(3):  # warm-up: the solve's graph capture, allocations
+            stepper.step(n * derived.dt_s, derived.dt_s)
+        ms = device_ms(lambda: [stepper.step((3 + n) * derived.dt_s, derived.dt_s) for n in range(steps)])
+        out[label] = {"value": math.prod(cells) * steps / (ms / 1e3) / 1e6, "unit": METRIC, "steps": steps}
+        for name, values in fields.items():  # the frames restart from the seeded state
+            getattr(grid, name).data.copy_(values)
+        grid.pressure.zero_()
+        stepper = Stepper(grid, recipe)
+        renderer = FrameRenderer(view, recipe.render, derived.cells, recipe.output.channels, device)
+        rendered = []
+        for frame in range(frames):
+            for n in range(4):
+                stepper.step((4 * frame + n) * derived.dt_s, derived.dt_s)
+            rendered.append(renderer.render(grid))
+        runs[label] = rendered
+        del grid, stepper, renderer
+        torch.cuda.empty_cache()
+    heat_scale = [max(float(np.abs(f[..., 0]).max()), 1e-30) for f in runs["f32"]]
+    out["bf16"]["thickness_difference_vs_f32"] = [float(np.abs(a[..., 1] - b[..., 1]).max())
+                                                  for a, b in zip(runs["bf16"], runs["f32"])]
+    out["bf16"]["heat_difference_vs_f32"] = [float(np.abs(a[..., 0] - b[..., 0]).max()) / s
+                                             for a, b, s in zip(runs["bf16"], runs["f32"], heat_scale)]
+    out["bf16"]["ratio_to_f32"] = out["bf16"]["value"] / out["f32"]["value"]
+    return out
+
+
 def run_reference(args, cells):
     """--impl reference: the oracle port of the reference's CPU path on the host cores."""
     world, rank, _ = dist_env()
@@ -459,7 +610,9 @@ def main():
     }
     if not args.no_variants:
         line["variants"] = {"storage": storage_variants(recipe, derived, fields, args.steps, device),
-                            "batched": batched_variant(device), "adjoint": adjoint_variant(device)}
+                            "batched": batched_variant(device), "adjoint": adjoint_variant(device),
+                            "operators": operators_variant(recipe, derived, fields, device),
+                            "large_mixed": large_mixed_variant(device)}
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         line["cpu_baseline"] = cpu_baseline(recipe, derived, fields)
     if rank == 0:

@@ -50,6 +50,31 @@ def operator_fields(cells, seed: int = DEFAULT_SEED, ambient_k: float = 1.0) -> 
     return {name: value.astype(np.float32) for name, value in fields.items()}
 
 
+def device_operator_fields(cells, seed: int = DEFAULT_SEED, ambient_k: float = 1.0, device: str = "cuda:0") -> dict:
+    """operator_fields' distributions generated on the device (torch's generator, float32 box filters): for
+    grids too large to fill quickly on the host. The values differ from operator_fields'."""
+    import torch
+    import torch.nn.functional as F
+
+    generator = torch.Generator(device=device).manual_seed(seed)
+    nx, ny, nz = cells
+
+    def smoothed(shape):
+        x = torch.rand(shape, generator=generator, device=device) * 2.0 - 1.0
+        for _ in range(3):
+            x = F.avg_pool3d(F.pad(x[None, None], (1, 1, 1, 1, 1, 1), mode="replicate"), 3, stride=1)[0, 0]
+        return x.contiguous()
+
+    fields = {"u": smoothed((nx + 1, ny, nz)), "v": smoothed((nx, ny + 1, nz)), "w": smoothed((nx, ny, nz + 1))}
+    idx = [torch.arange(n, device=device, dtype=torch.float32) + 0.5 - n / 2.0 for n in cells]
+    dist2 = idx[0][:, None, None] ** 2 + idx[1][None, :, None] ** 2 + idx[2][None, None, :] ** 2
+    radius = 40.0 * nx / 128.0
+    smoke = torch.rand(cells, generator=generator, device=device)
+    fields["smoke"] = torch.where(dist2 <= radius * radius, smoke, torch.zeros_like(smoke))
+    fields["temperature"] = ambient_k + 0.8 * fields["smoke"]
+    return fields
+
+
 def plain_step_recipe(cells=(128, 192, 128), cycles: int = 4, frames: int = 24, substeps: int = 4):
     nx, ny, nz = cells
     cell_m = (128.0 / nx) / 64.0
