@@ -36,12 +36,50 @@ class FrameRenderer:
         # scratch for the marched smoke's brick map (empty-space skipping; built by every march)
         self.bricks = torch.empty(N.lib().plume_brick_floats(N.c_int3(*cells)), dtype=torch.float32, device=device)
         self._host = torch.empty(self.image.shape, dtype=torch.float32, pin_memory=True)
+        self._side = None  # render_async's stream, snapshot and last completion event
+        self._snapshot = None
+        self._last_done = None
 
     def render(self, grid) -> np.ndarray:
         return self.render_fields(grid.smoke.data, grid.temperature.data, grid.info)
 
+    def render_async(self, grid) -> "PendingFrame":
+        """render(grid) overlapped with what the caller enqueues next (no reference counterpart). Smoke and
+        temperature are copied to a snapshot on the caller's stream; the volume pass, the march and the copy
+        to pinned host memory then run on the renderer's own stream, so the caller's next substeps may
+        overwrite the grid at once. PendingFrame.result() waits for the frame. Frames of one renderer complete
+        in order; a new snapshot waits for the previous frame's march."""
+        main = torch.cuda.current_stream()
+        smoke, temperature = grid.smoke.data, grid.temperature.data
+        if self._side is None:
+            self._side = torch.cuda.Stream(device=smoke.device)
+        if self._snapshot is None or self._snapshot[0].shape != smoke.shape or self._snapshot[0].dtype != smoke.dtype:
+            self._snapshot = (torch.empty_like(smoke), torch.empty_like(temperature))
+        if self._last_done is not None:
+            main.wait_event(self._last_done)
+        self._snapshot[0].copy_(smoke)
+        self._snapshot[1].copy_(temperature)
+        ready = torch.cuda.Event()
+        ready.record(main)
+        host = torch.empty(self.image.shape, dtype=torch.float32, pin_memory=True)
+        with torch.cuda.stream(self._side):
+            self._side.wait_event(ready)
+            self.prepare(self._snapshot[0], grid.info.cell_m)
+            self.march(self._snapshot[0], self._snapshot[1], grid.info, self.view_params, self.image)
+            host.copy_(self.image, non_blocking=True)
+            done = torch.cuda.Event()
+            done.record(self._side)
+        self._last_done = done
+        return PendingFrame(done, host)
+
+    def wait_for(self, stream=None) -> None:
+        """Makes `stream` (the current stream by default) wait for every frame render_async has enqueued."""
+        if self._last_done is not None:
+            (stream or torch.cuda.current_stream()).wait_event(self._last_done)
+
     def render_fields(self, smoke, temperature, info) -> np.ndarray:
         """The raw frame of these fields over the domain view, copied to the host."""
+        self.wait_for()  # frames render_async has in flight use the same scratch
         self.prepare(smoke, info.cell_m)
         self.march(smoke, temperature, info, self.view_params, self.image)
         self._host.copy_(self.image, non_blocking=True)
@@ -67,6 +105,18 @@ class FrameRenderer:
                N.ptr(self.gradient), gradient_shape,
                N.ptr(self.light), N.shape3(self.light), view, self.look_params, N.ptr(image), image.shape[0],
                image.shape[1], bricks, N.stream())
+
+
+class PendingFrame:
+    """A frame FrameRenderer.render_async has enqueued: result() waits for it and returns the (H, W, 5) array."""
+
+    def __init__(self, done, host):
+        self._done = done
+        self._host = host
+
+    def result(self) -> np.ndarray:
+        self._done.synchronize()
+        return self._host.numpy().copy()
 
 
 def toward_light_world(camera, light_dir) -> np.ndarray:

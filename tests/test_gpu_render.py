@@ -192,3 +192,36 @@ def test_perspective_march_matches_the_oracle(cuda_device):
     oracle.prepare(o.smoke.data, o.cell_m)
     oracle.march(o.smoke.data, o.temperature.data, o.info, oparams, expected)
     assert np.abs(host(image)[..., 1:] - expected[..., 1:]).max() < MARCH_ATOL * 10
+
+
+@pytest.mark.parametrize("channels", [SHADE_LAYOUT, NORMAL_LAYOUT])
+def test_render_async_gives_the_frames_render_gives(cuda_device, channels):
+    """Frames enqueued by render_async while the next substeps already run are bit-identical to render()."""
+    import torch
+
+    from plume_b200.recipe.derived import derive
+    from plume_b200.render.camera import sheet_domain_view
+    from plume_b200.render.frame_renderer import FrameRenderer
+    from plume_b200.sim.grid import make_grid
+    from plume_b200.sim.stepper import Stepper
+    from plume_b200.workloads import operator_fields, plain_step_recipe
+
+    recipe = plain_step_recipe((32, 48, 32), cycles=2)
+    derived = derive(recipe)
+    d = recipe.domain
+    frames = {}
+    for arm in ("sync", "async"):
+        grid = make_grid(derived, d.cell_m, d.faces, d.ambient_k, "cuda:0")
+        for name, values in operator_fields(derived.cells, 5, d.ambient_k).items():
+            getattr(grid, name).data.copy_(torch.from_numpy(values))
+        stepper = Stepper(grid, recipe)
+        renderer = FrameRenderer(sheet_domain_view(recipe, derived), recipe.render, derived.cells, channels, "cuda:0")
+        out = []
+        for frame in range(4):
+            for n in range(2):
+                stepper.step((2 * frame + n) * derived.dt_s, derived.dt_s)
+            out.append(renderer.render(grid) if arm == "sync" else renderer.render_async(grid))
+        frames[arm] = out if arm == "sync" else [pending.result() for pending in out]
+    for index, (a, b) in enumerate(zip(frames["sync"], frames["async"])):
+        assert np.array_equal(a, b), f"frame {index}"
+    assert frames["sync"][-1][..., 1].max() > 0.1
