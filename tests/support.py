@@ -74,3 +74,35 @@ def max_rel(actual, expected, floor: float = 0.0) -> float:
     scale = np.maximum(np.abs(e), floor)
     scale = np.where(scale == 0.0, 1.0, scale)
     return float(np.max(np.abs(a - e) / scale)) if a.size else 0.0
+
+
+# The end-to-end test recipe (a 1.2 m box of 0.05 m cells, one smoke puff, 4 frames in 1 s), as a table so a
+# test states only what it changes; a section given as a dict is merged into that section.
+TINY_TABLE = {
+    "seed": 1,
+    "domain": {"size_m": [1.2, 1.2, 1.2], "cell_m": 0.05},
+    "time": {"duration_s": 1.0, "frames": 4},
+    "emitter": [{"name": "puff", "center_m": [0.0, 0.3, 0.0], "radius_m": 0.2, "end_s": 0.5,
+                 "smoke_per_s": 5.0}],
+}
+
+
+def tiny_recipe(**changes):
+    import copy
+
+    from plume_b200.recipe.load import fill_dependent_defaults, parse_recipe
+
+    table = copy.deepcopy(TINY_TABLE)
+    for key, value in changes.items():
+        if isinstance(value, dict) and isinstance(table.get(key), dict):
+            table[key].update(value)
+        else:
+            table[key] = value
+    return fill_dependent_defaults(parse_recipe(table), "tiny")
+
+
+def put(tensor, values) -> None:
+    """Copies a numpy array into a CUDA tensor of the same shape (as float32, or the tensor's storage)."""
+    import torch
+
+    tensor.copy_(torch.from_numpy(np.ascontiguousarray(values, dtype=np.float32)))
