@@ -416,6 +416,27 @@ def large_mixed_variant(device: str, steps: int = 8, frames: int = 2) -> dict:
     return out
 
 
+def preview_run_variant(device: str) -> dict:
+    """The smoke-puff preview (38 x 48 x 38 cells, 16 frames, 192 substeps) end to end on the device through
+    plume_b200.run.run_recipe: simulate, render every frame, assemble the sheet, measure the numbers; wall
+    seconds of a second run (the first warms the graphs and allocations), and frames per second."""
+    import torch
+
+    from plume_b200.recipe.load import load_recipe
+    from plume_b200.run import run_recipe
+
+    recipe = load_recipe(REPO / "tests" / "golden" / "smoke_puff.toml", preview=True)
+    run_recipe(recipe, "recipes/smoke_puff.toml", device)
+    torch.cuda.synchronize()
+    start = time.perf_counter()
+    run = run_recipe(recipe, "recipes/smoke_puff.toml", device)
+    torch.cuda.synchronize()
+    seconds = time.perf_counter() - start
+    return {"cells": list(run.derived.cells), "frames": recipe.time.frames, "substeps": run.steps.total_steps,
+            "seconds": seconds, "frames_per_s": recipe.time.frames / seconds,
+            "mcell_substeps_per_s": math.prod(run.derived.cells) * run.steps.total_steps / seconds / 1e6}
+
+
 def run_reference(args, cells):
     """--impl reference: the oracle port of the reference's CPU path on the host cores."""
     world, rank, _ = dist_env()
@@ -617,7 +638,7 @@ def main():
         line["variants"] = {"storage": storage_variants(recipe, derived, fields, args.steps, device),
                             "batched": batched_variant(device), "adjoint": adjoint_variant(device),
                             "operators": operators_variant(recipe, derived, fields, device),
-                            "large_mixed": large_mixed_variant(device)}
+                            "large_mixed": large_mixed_variant(device), "preview_run": preview_run_variant(device)}
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         line["cpu_baseline"] = cpu_baseline(recipe, derived, fields)
     if rank == 0:
