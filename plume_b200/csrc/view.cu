@@ -339,6 +339,7 @@ extern "C" int plume_view_boundary_layers(const float* smoke, const int32_t shap
 extern "C" int plume_view_narrow(const float* src, void* dst, long long count, void* stream) {
   VIEW_CHECK(src && dst && count >= 0, "view_narrow: bad argument");
   if (count == 0) return PLUME_OK;
+  if (count == 0) return PLUME_OK;
   k_narrow<<<(int)std::min<long long>((count + 255) / 256, 148 * 16), 256, 0, as_stream(stream)>>>(
       src, static_cast<__half*>(dst), (long)count);
   return launch_status("narrow");
@@ -346,6 +347,7 @@ extern "C" int plume_view_narrow(const float* src, void* dst, long long count, v
 
 extern "C" int plume_view_widen(const void* src, float* dst, long long count, void* stream) {
   VIEW_CHECK(src && dst && count >= 0, "view_widen: bad argument");
+  if (count == 0) return PLUME_OK;
   if (count == 0) return PLUME_OK;
   k_widen<<<(int)std::min<long long>((count + 255) / 256, 148 * 16), 256, 0, as_stream(stream)>>>(
       static_cast<const __half*>(src), dst, (long)count);
