@@ -1,5 +1,5 @@
 """Whole-substep and whole-run parity of the CUDA path (plume_step through Stepper, and the frame loop)
-against the FP32 oracle. North-star tolerance for one substep: 1e-4 relative; in practice every field
+against the FP32 oracle. Tolerance for one substep: 1e-4 relative; in practice every field
 matches to the last bit except where the emitter's pow differs by an ulp."""
 
 import json
