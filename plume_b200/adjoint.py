@@ -12,6 +12,7 @@ checkpoint every `checkpoint_every` substeps; the backward pass walks the segmen
 each segment's smoke states from its checkpoint and then applying the adjoint substep by substep.
 """
 
+import dataclasses
 import math
 
 import torch
@@ -79,6 +80,25 @@ class SourceFit:
                N.ptr(grid.smoke.data), N.ptr(target), height, width, N.ptr(thickness), N.ptr(loss, torch.float64),
                N.ptr(scratch), N.stream())
         return float(loss.item())
+
+    def with_forces(self, **forces) -> "SourceFit":
+        """The same fit with some of recipe.forces changed (e.g. heat_buoyancy, drag_per_s)."""
+        recipe = dataclasses.replace(self.recipe, forces=dataclasses.replace(self.recipe.forces, **forces))
+        return SourceFit(recipe, self.source_shape, self.corner, self.substeps, self.device, self.window, self.every,
+                         self.initial_state)
+
+    def scalar_gradients(self, source: torch.Tensor, target: torch.Tensor, names=("heat_buoyancy", "drag_per_s"),
+                         h: float = 1e-2) -> dict:
+        """d loss / d each named recipe.forces scalar, by central differences of the forward loss (two forward
+        runs per scalar, step h). These scalars move the velocity, whose adjoint is not built: the source
+        field's gradient is the adjoint's (loss_and_grad), the scalars' are finite differences."""
+        grads = {}
+        for name in names:
+            value = getattr(self.recipe.forces, name)
+            up = self.with_forces(**{name: value + h}).loss(source, target)
+            down = self.with_forces(**{name: value - h}).loss(source, target)
+            grads[name] = (up - down) / (2.0 * h)
+        return grads
 
     def _smoke_substep(self, smoke, n, source, scratch):
         """Recomputes substep n's smoke path from `smoke` (its start state); returns (data, hat, next_pre,
