@@ -423,22 +423,22 @@ struct FieldSet {
   int count;
 };
 
-template <class T>
-__device__ __forceinline__ int pick_field(const FieldSet<T>& set, int& slab) {
-  int which = 0;
-  while (which + 1 < set.count && slab >= set.f[which].d.n0) {
-    slab -= set.f[which].d.n0;
-    ++which;
-  }
-  return which;
-}
-
 // semi_lagrangian_kernel (advect.py:24-31): the forward pass into `hat` (or, for plain semi-Lagrangian
 // advection, into `next`).
-template <class T>
-__global__ void k_advect_forward(PlumeGridInfo info, VelT<T> vel, FieldSet<T> set, float dt_over_cell, int write_next) {
+// Calls body(group, slab) with the group of `set` that blockIdx.z falls in, as a constant index into the kernel
+// parameters (each group's body is compiled on its own, with its descriptor at fixed parameter offsets).
+template <class T, class Body>
+__device__ __forceinline__ void for_group(const FieldSet<T>& set, Body body) {
   int slab = blockIdx.z;
-  const FieldDesc<T>& fd = set.f[pick_field(set, slab)];
+  if (slab < set.f[0].d.n0 || set.count == 1) return body(set.f[0], slab);
+  slab -= set.f[0].d.n0;
+  if (slab < set.f[1].d.n0 || set.count == 2) return body(set.f[1], slab);
+  body(set.f[2], slab - set.f[1].d.n0);
+}
+
+template <class T>
+__device__ __forceinline__ void advect_forward_at(const PlumeGridInfo& info, const VelT<T>& vel, const FieldDesc<T>& fd,
+                                                  int slab, float dt_over_cell, int write_next) {
   const int i = slab, j = blockIdx.y * blockDim.y + threadIdx.y, k = blockIdx.x * blockDim.x + threadIdx.x;
   if (j >= fd.d.n1 || k >= fd.d.n2) return;
   const int c = at(fd.d, i, j, k);
@@ -454,13 +454,17 @@ __global__ void k_advect_forward(PlumeGridInfo info, VelT<T> vel, FieldSet<T> se
   }
 }
 
+template <class T>
+__global__ void k_advect_forward(PlumeGridInfo info, VelT<T> vel, FieldSet<T> set, float dt_over_cell, int write_next) {
+  for_group(set, [&](const FieldDesc<T>& fd, int slab) { advect_forward_at(info, vel, fd, slab, dt_over_cell, write_next); });
+}
+
 // maccormack_correct_kernel (advect.py:34-50) with the backward pass (advect.py:64) evaluated in place:
 // back = sample(hat, trace(p, -dt)), corrected = hat + (data - back) / 2, clamped to the range of the eight
 // values the forward sample blended.
 template <class T, bool STORED_RANGE>
-__global__ void k_advect_correct(PlumeGridInfo info, VelT<T> vel, FieldSet<T> set, float dt_over_cell) {
-  int slab = blockIdx.z;
-  const FieldDesc<T>& fd = set.f[pick_field(set, slab)];
+__device__ __forceinline__ void advect_correct_at(const PlumeGridInfo& info, const VelT<T>& vel, const FieldDesc<T>& fd,
+                                                  int slab, float dt_over_cell) {
   const int i = slab, j = blockIdx.y * blockDim.y + threadIdx.y, k = blockIdx.x * blockDim.x + threadIdx.x;
   if (j >= fd.d.n1 || k >= fd.d.n2) return;
   const int c = at(fd.d, i, j, k);
@@ -489,6 +493,13 @@ __global__ void k_advect_correct(PlumeGridInfo info, VelT<T> vel, FieldSet<T> se
     }
     st_f(fd.next[n] + c, clampf_(corrected, lo, hi));
   }
+}
+
+template <class T, bool STORED_RANGE>
+__global__ void k_advect_correct(PlumeGridInfo info, VelT<T> vel, FieldSet<T> set, float dt_over_cell) {
+  for_group(set, [&](const FieldDesc<T>& fd, int slab) {
+    advect_correct_at<T, STORED_RANGE>(info, vel, fd, slab, dt_over_cell);
+  });
 }
 
 template <class T>
