@@ -436,7 +436,8 @@ __device__ __forceinline__ void for_group(const FieldSet<T>& set, Body body) {
   body(set.f[2], slab - set.f[1].d.n0);
 }
 
-template <class T>
+// FIELDS: the group's field count when fixed at compile time, 0 to read it from the descriptor.
+template <int FIELDS, class T>
 __device__ __forceinline__ void advect_forward_at(const PlumeGridInfo& info, const VelT<T>& vel, const FieldDesc<T>& fd,
                                                   int slab, float dt_over_cell, int write_next) {
   const int i = slab, j = blockIdx.y * blockDim.y + threadIdx.y, k = blockIdx.x * blockDim.x + threadIdx.x;
@@ -446,7 +447,7 @@ __device__ __forceinline__ void advect_forward_at(const PlumeGridInfo& info, con
   const F3 src = trace_from(vel, p, velocity_at_node(vel, p), dt_over_cell);
   const bool outside = fd.uses_outside == 1 && is_outside_open_face(src, info);
   const F3 g = sub3(src, fd.offset);
-  for (int n = 0; n < fd.fields; ++n) {
+  for (int n = 0; n < (FIELDS ? FIELDS : fd.fields); ++n) {
     float value = fd.outside[n], lo = fd.outside[n], hi = fd.outside[n];
     if (!outside) value = sample_with_range(fd.data[n], fd.d, g, lo, hi);
     st_f((write_next ? fd.next[n] : fd.hat[n]) + c, value);
@@ -456,13 +457,18 @@ __device__ __forceinline__ void advect_forward_at(const PlumeGridInfo& info, con
 
 template <class T>
 __global__ void k_advect_forward(PlumeGridInfo info, VelT<T> vel, FieldSet<T> set, float dt_over_cell, int write_next) {
-  for_group(set, [&](const FieldDesc<T>& fd, int slab) { advect_forward_at(info, vel, fd, slab, dt_over_cell, write_next); });
+  // a single field (a velocity component) with its count known to the compiler; measured on B200, that helps
+  // the velocity pass (-1%) but a two-field count known to it slowed the smoke-and-temperature pass (+1.5%)
+  for_group(set, [&](const FieldDesc<T>& fd, int slab) {
+    if (fd.fields == 1) advect_forward_at<1>(info, vel, fd, slab, dt_over_cell, write_next);
+    else advect_forward_at<0>(info, vel, fd, slab, dt_over_cell, write_next);
+  });
 }
 
 // maccormack_correct_kernel (advect.py:34-50) with the backward pass (advect.py:64) evaluated in place:
 // back = sample(hat, trace(p, -dt)), corrected = hat + (data - back) / 2, clamped to the range of the eight
 // values the forward sample blended.
-template <class T, bool STORED_RANGE>
+template <int FIELDS, class T, bool STORED_RANGE>
 __device__ __forceinline__ void advect_correct_at(const PlumeGridInfo& info, const VelT<T>& vel, const FieldDesc<T>& fd,
                                                   int slab, float dt_over_cell) {
   const int i = slab, j = blockIdx.y * blockDim.y + threadIdx.y, k = blockIdx.x * blockDim.x + threadIdx.x;
@@ -480,7 +486,7 @@ __device__ __forceinline__ void advect_correct_at(const PlumeGridInfo& info, con
     source_outside = fd.uses_outside == 1 && is_outside_open_face(source, info);
     gs = sub3(source, fd.offset);
   }
-  for (int n = 0; n < fd.fields; ++n) {
+  for (int n = 0; n < (FIELDS ? FIELDS : fd.fields); ++n) {
     const float back = back_outside ? fd.outside[n] : sample_index_space(fd.hat[n], fd.d, gb);
     const float corrected = ldg_f(fd.hat[n] + c) + 0.5f * (ldg_f(fd.data[n] + c) - back);
     float lo = fd.outside[n], hi = fd.outside[n];
@@ -498,7 +504,8 @@ __device__ __forceinline__ void advect_correct_at(const PlumeGridInfo& info, con
 template <class T, bool STORED_RANGE>
 __global__ void k_advect_correct(PlumeGridInfo info, VelT<T> vel, FieldSet<T> set, float dt_over_cell) {
   for_group(set, [&](const FieldDesc<T>& fd, int slab) {
-    advect_correct_at<T, STORED_RANGE>(info, vel, fd, slab, dt_over_cell);
+    if (fd.fields == 1) advect_correct_at<1, T, STORED_RANGE>(info, vel, fd, slab, dt_over_cell);
+    else advect_correct_at<0, T, STORED_RANGE>(info, vel, fd, slab, dt_over_cell);
   });
 }
 
