@@ -455,13 +455,13 @@ __device__ __forceinline__ void advect_forward_at(const PlumeGridInfo& info, con
   }
 }
 
-template <class T>
+// ONE_FIELD: every group holds one field (the velocity components), a count the compiler then knows. Measured
+// on B200 that helps the velocity pass (-1%); the smoke-and-temperature pass keeps the count as data, since a
+// compiled-in count of two, and the registers it took, slowed it (+1.5%).
+template <class T, bool ONE_FIELD>
 __global__ void k_advect_forward(PlumeGridInfo info, VelT<T> vel, FieldSet<T> set, float dt_over_cell, int write_next) {
-  // a single field (a velocity component) with its count known to the compiler; measured on B200, that helps
-  // the velocity pass (-1%) but a two-field count known to it slowed the smoke-and-temperature pass (+1.5%)
   for_group(set, [&](const FieldDesc<T>& fd, int slab) {
-    if (fd.fields == 1) advect_forward_at<1>(info, vel, fd, slab, dt_over_cell, write_next);
-    else advect_forward_at<0>(info, vel, fd, slab, dt_over_cell, write_next);
+    advect_forward_at<ONE_FIELD ? 1 : 0>(info, vel, fd, slab, dt_over_cell, write_next);
   });
 }
 
@@ -501,11 +501,10 @@ __device__ __forceinline__ void advect_correct_at(const PlumeGridInfo& info, con
   }
 }
 
-template <class T, bool STORED_RANGE>
+template <class T, bool STORED_RANGE, bool ONE_FIELD>
 __global__ void k_advect_correct(PlumeGridInfo info, VelT<T> vel, FieldSet<T> set, float dt_over_cell) {
   for_group(set, [&](const FieldDesc<T>& fd, int slab) {
-    if (fd.fields == 1) advect_correct_at<1, T, STORED_RANGE>(info, vel, fd, slab, dt_over_cell);
-    else advect_correct_at<0, T, STORED_RANGE>(info, vel, fd, slab, dt_over_cell);
+    advect_correct_at<ONE_FIELD ? 1 : 0, T, STORED_RANGE>(info, vel, fd, slab, dt_over_cell);
   });
 }
 
@@ -519,15 +518,19 @@ static int launch_advect(const PlumeGridInfo& info, const VelT<T>& vel, const Fi
     n2 = std::max(n2, set.f[n].d.n2);
   }
   dim3 grid((n2 + TZ - 1) / TZ, (n1 + TY - 1) / TY, slabs);
+  bool one_field = true;
+  for (int n = 0; n < set.count; ++n) one_field = one_field && set.f[n].fields == 1;
+  auto forward = one_field ? k_advect_forward<T, true> : k_advect_forward<T, false>;
   if (!maccormack) {
-    k_advect_forward<T><<<grid, cell_block(), 0, st>>>(info, vel, set, dt_over_cell, 1);
+    forward<<<grid, cell_block(), 0, st>>>(info, vel, set, dt_over_cell, 1);
     CHECK_LAUNCH("semi-Lagrangian advection");
     return PLUME_OK;
   }
-  k_advect_forward<T><<<grid, cell_block(), 0, st>>>(info, vel, set, dt_over_cell, 0);
+  forward<<<grid, cell_block(), 0, st>>>(info, vel, set, dt_over_cell, 0);
   CHECK_LAUNCH("MacCormack forward pass");
-  if (set.f[0].range[0]) k_advect_correct<T, true><<<grid, cell_block(), 0, st>>>(info, vel, set, dt_over_cell);
-  else k_advect_correct<T, false><<<grid, cell_block(), 0, st>>>(info, vel, set, dt_over_cell);
+  auto correct = set.f[0].range[0] ? (one_field ? k_advect_correct<T, true, true> : k_advect_correct<T, true, false>)
+                                   : (one_field ? k_advect_correct<T, false, true> : k_advect_correct<T, false, false>);
+  correct<<<grid, cell_block(), 0, st>>>(info, vel, set, dt_over_cell);
   CHECK_LAUNCH("MacCormack correction");
   return PLUME_OK;
 }
