@@ -455,13 +455,13 @@ __device__ __forceinline__ void advect_forward_at(const PlumeGridInfo& info, con
   }
 }
 
-// ONE_FIELD: every group holds one field (the velocity components), a count the compiler then knows. Measured
-// on B200 that helps the velocity pass (-1%); the smoke-and-temperature pass keeps the count as data, since a
-// compiled-in count of two, and the registers it took, slowed it (+1.5%).
-template <class T, bool ONE_FIELD>
+// FIELDS: every group of the launch holds this many fields (1: the velocity components, 2: smoke and
+// temperature), a count the compiler then knows; 0 reads each group's count. Measured on B200, as kernels of
+// their own: velocity advection -3.5%, scalar advection -4%.
+template <class T, int FIELDS>
 __global__ void k_advect_forward(PlumeGridInfo info, VelT<T> vel, FieldSet<T> set, float dt_over_cell, int write_next) {
   for_group(set, [&](const FieldDesc<T>& fd, int slab) {
-    advect_forward_at<ONE_FIELD ? 1 : 0>(info, vel, fd, slab, dt_over_cell, write_next);
+    advect_forward_at<FIELDS>(info, vel, fd, slab, dt_over_cell, write_next);
   });
 }
 
@@ -501,10 +501,10 @@ __device__ __forceinline__ void advect_correct_at(const PlumeGridInfo& info, con
   }
 }
 
-template <class T, bool STORED_RANGE, bool ONE_FIELD>
+template <class T, bool STORED_RANGE, int FIELDS>
 __global__ void k_advect_correct(PlumeGridInfo info, VelT<T> vel, FieldSet<T> set, float dt_over_cell) {
   for_group(set, [&](const FieldDesc<T>& fd, int slab) {
-    advect_correct_at<ONE_FIELD ? 1 : 0, T, STORED_RANGE>(info, vel, fd, slab, dt_over_cell);
+    advect_correct_at<FIELDS, T, STORED_RANGE>(info, vel, fd, slab, dt_over_cell);
   });
 }
 
@@ -518,9 +518,10 @@ static int launch_advect(const PlumeGridInfo& info, const VelT<T>& vel, const Fi
     n2 = std::max(n2, set.f[n].d.n2);
   }
   dim3 grid((n2 + TZ - 1) / TZ, (n1 + TY - 1) / TY, slabs);
-  bool one_field = true;
-  for (int n = 0; n < set.count; ++n) one_field = one_field && set.f[n].fields == 1;
-  auto forward = one_field ? k_advect_forward<T, true> : k_advect_forward<T, false>;
+  int fields = set.f[0].fields;  // the groups' common field count, or 0 when they differ
+  for (int n = 1; n < set.count; ++n)
+    if (set.f[n].fields != fields) fields = 0;
+  auto forward = fields == 1 ? k_advect_forward<T, 1> : (fields == 2 ? k_advect_forward<T, 2> : k_advect_forward<T, 0>);
   if (!maccormack) {
     forward<<<grid, cell_block(), 0, st>>>(info, vel, set, dt_over_cell, 1);
     CHECK_LAUNCH("semi-Lagrangian advection");
@@ -528,8 +529,11 @@ static int launch_advect(const PlumeGridInfo& info, const VelT<T>& vel, const Fi
   }
   forward<<<grid, cell_block(), 0, st>>>(info, vel, set, dt_over_cell, 0);
   CHECK_LAUNCH("MacCormack forward pass");
-  auto correct = set.f[0].range[0] ? (one_field ? k_advect_correct<T, true, true> : k_advect_correct<T, true, false>)
-                                   : (one_field ? k_advect_correct<T, false, true> : k_advect_correct<T, false, false>);
+  auto correct = set.f[0].range[0]
+                      ? (fields == 1 ? k_advect_correct<T, true, 1>
+                                     : (fields == 2 ? k_advect_correct<T, true, 2> : k_advect_correct<T, true, 0>))
+                      : (fields == 1 ? k_advect_correct<T, false, 1>
+                                     : (fields == 2 ? k_advect_correct<T, false, 2> : k_advect_correct<T, false, 0>));
   correct<<<grid, cell_block(), 0, st>>>(info, vel, set, dt_over_cell);
   CHECK_LAUNCH("MacCormack correction");
   return PLUME_OK;
