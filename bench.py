@@ -556,10 +556,10 @@ def main():
     phase_ms = {name: sum(row[i].elapsed_time(row[i + 1]) for row in events) / args.steps
                 for i, name in enumerate(phases)}
 
-    # e2e: the public API frame loop (StepCap.plan readback, Stepper.step x substeps, then
-    # FrameRenderer.render_async: the frame's volume pass, march and copy to pinned host memory on the
-    # renderer's stream, overlapping the next frame's substeps) from a state uploaded from pinned host memory
-    # inside the timed region, which ends after the last frame's copy
+    # e2e: the public API frame loop (StepCap.plan readback, Stepper.step x substeps, FrameRenderer.render
+    # copying the raw frame to the host) from a state uploaded from pinned host memory inside the timed region.
+    # The synchronous render measured steadier and faster than FrameRenderer.render_async here (1426-1430 vs
+    # 1205-1499 Mcell-substeps/s over three runs each): the overlapped frame competes with the substeps for SMs.
     pinned = {name: torch.from_numpy(values).pin_memory() for name, values in fields.items()}
     view = sheet_domain_view(recipe, derived)
     renderer = FrameRenderer(view, recipe.render, derived.cells, recipe.output.channels, device)
@@ -568,8 +568,7 @@ def main():
     frames = max(1, args.steps // substeps)
     grid2 = make_grid(derived, d.cell_m, d.faces, d.ambient_k, device)
     stepper2 = Stepper(grid2, recipe)
-    renderer.render(grid2)  # warm the renderer (and its stream, snapshot and pinned buffers)
-    renderer.render_async(grid2).result()
+    renderer.render(grid2)  # warm the renderer
     torch.cuda.synchronize()
     if world > 1:
         dist.barrier()
@@ -578,7 +577,6 @@ def main():
     for name, tensor in pinned.items():
         getattr(grid2, name).data.copy_(tensor, non_blocking=True)
     steps_run = 0
-    pending = []
     for frame in range(frames):  # run_block of plume_b200.sim.run, one frame per block
         start_s, length_s = frame * substeps * dt, substeps * dt
         steps = cap.plan(grid2, start_s, length_s, substeps, f"frame {frame}").steps
@@ -588,8 +586,7 @@ def main():
             else:
                 stepper2.step(start_s + index * length_s / steps, length_s / steps)
         steps_run += steps
-        pending.append(renderer.render_async(grid2))  # overlaps the next frame's substeps
-    renderer.wait_for(stream)
+        renderer.render(grid2)
     e2e_end.record(stream)
     torch.cuda.synchronize()
     e2e_ms = torch.tensor([e2e_start.elapsed_time(e2e_end)], dtype=torch.float64, device=device)
