@@ -95,3 +95,20 @@ def test_tuning_rejects_bad_values(tuning):
     for bad in (dict(tiled_min_cells=0), dict(bottom_max_cells=-1), dict(bottom_kind=2)):
         with pytest.raises(RuntimeError):
             tune_solver(dataclasses.replace(tuning, **bad))
+
+
+def test_the_autotuner_picks_the_fastest_candidate_and_restores_the_pressure(tuning):
+    import torch
+
+    from plume_b200.sim.autotune import autotune_solver
+    from plume_b200.sim.multigrid import solver_tuning
+    from plume_b200.sim.pressure import compute_divergence
+
+    _, c = seeded_pair((38, 48, 38), OPEN)
+    compute_divergence(c)
+    before = c.pressure.clone()
+    result = autotune_solver(c, 2, 2, repeats=2)
+    assert len(result.ms_per_solve) == 5 and all(ms > 0.0 for ms in result.ms_per_solve.values())
+    assert result.best == min(result.ms_per_solve, key=result.ms_per_solve.get)
+    assert solver_tuning() == result.best
+    assert torch.equal(c.pressure, before)
