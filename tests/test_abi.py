@@ -62,3 +62,25 @@ def test_kernels_refuse_host_tensors():
 
     with pytest.raises(RuntimeError, match="CUDA"):
         N.ptr(torch.zeros(4))
+
+
+def test_newer_entry_points_reject_bad_arguments_without_a_gpu():
+    """Argument checks come before any device work: a null array, a missing scratch or an aliased output is
+    refused with status -1 and a message."""
+    lib = N.lib()
+    info = N.PlumeGridInfo()
+    info.dims = type(info.dims)(8, 8, 8)
+    shape = N.c_int3(8, 8, 8)
+    toward = N.f3((0.0, 1.0, 0.0))
+    assert lib.plume_march_light_volume(shape, None, 0, toward, 0.1, 1.0, None, None, None) == -1
+    assert b"march_light_volume" in lib.plume_last_error()
+    fake = ctypes.c_void_p(0x1000)
+    assert lib.plume_march_light_volume(shape, fake, 0, toward, 0.1, 1.0, fake, None, None) == -1  # no bricks
+    assert lib.plume_residual_f64(ctypes.byref(info), None, None, None, None, None, None, None) == -1
+    assert b"residual_f64" in lib.plume_last_error()
+    assert lib.plume_norm_scratch_doubles(ctypes.byref(info)) > 0
+    level = (N.PlumeLevel * 1)()
+    level[0].info = info
+    level[0].q = level[0].rhs = level[0].residual = 0x1000  # q aliases the residual array
+    assert lib.plume_multigrid_correct(level, 1, 2, ctypes.c_void_p(0x2000), None, None) == -1
+    assert b"multigrid_correct" in lib.plume_last_error()

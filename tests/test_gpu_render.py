@@ -225,3 +225,44 @@ def test_render_async_gives_the_frames_render_gives(cuda_device, channels):
     for index, (a, b) in enumerate(zip(frames["sync"], frames["async"])):
         assert np.array_equal(a, b), f"frame {index}"
     assert frames["sync"][-1][..., 1].max() > 0.1
+
+
+def test_bfloat16_storage_skips_and_lights_exactly_as_without_the_shortcuts(cuda_device):
+    """With bfloat16 fields: the light volume a march reads equals the whole light volume at the read cells,
+    and the march with its brick map equals the march without it, bit for bit."""
+    import torch
+
+    from plume_b200 import _native as N
+    from plume_b200.render.frame_renderer import FrameRenderer
+    from plume_b200.sim.grid import make_grid
+    from support import small_derived
+
+    cells = (48, 64, 40)
+    _, c = render_pair(cells)
+    g = make_grid(small_derived(cells, 0.05), 0.05, OPEN, 293.0, "cuda:0", storage=torch.bfloat16)
+    for name in ("u", "v", "w", "smoke", "temperature"):
+        getattr(g, name).data.copy_(getattr(c, name).data)
+    smoke = g.smoke.data
+    toward = N.f3(np.array([0.5, 0.8, 0.3]) / np.linalg.norm([0.5, 0.8, 0.3]))
+    bricks = torch.empty(N.lib().plume_brick_floats(N.shape3(smoke)), dtype=torch.float32, device="cuda:0")
+    whole = torch.empty(cells, dtype=torch.float32, device="cuda:0")
+    marched = torch.empty_like(whole)
+    N.call("plume_light_volume", N.shape3(smoke), N.field_ptr(smoke), N.storage_of(smoke), toward, 0.05, 4.0,
+           N.ptr(whole), N.ptr(bricks), N.stream())
+    N.call("plume_march_light_volume", N.shape3(smoke), N.field_ptr(smoke), N.storage_of(smoke), toward, 0.05, 4.0,
+           N.ptr(marched), N.ptr(bricks), N.stream())
+    read = read_by_march(host(smoke.float()))
+    assert np.array_equal(host(marched)[read], host(whole)[read]) and np.all(host(marched)[~read] == 1.0)
+
+    size = tuple(n * 0.05 for n in cells)
+    view = make_domain_view(make_camera(20.0, 30.0), (-size[0] / 2, 0.0, -size[2] / 2), size, 0.05, 2.0)
+    renderer = FrameRenderer(view, RenderSettings(glow_start_k=293.0, light_dir=(0.5, 0.8, 0.3)), cells,
+                             SHADE_LAYOUT, "cuda:0")
+    renderer.prepare(smoke, g.info.cell_m)
+    skipped, full = torch.zeros_like(renderer.image), torch.zeros_like(renderer.image)
+    renderer.march(smoke, g.temperature.data, g.info, renderer.view_params, skipped)
+    N.call("plume_raymarch", g.info, N.field_ptr(smoke), N.field_ptr(g.temperature.data), N.storage_of(smoke),
+           N.ptr(renderer.gradient), N.c_int3(*renderer.gradient.shape[:3]), N.ptr(renderer.light),
+           N.shape3(renderer.light), renderer.view_params, renderer.look_params, N.ptr(full), full.shape[0],
+           full.shape[1], None, N.stream())
+    assert torch.equal(skipped, full) and float(full[..., 1].max()) > 0.1
