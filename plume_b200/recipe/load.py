@@ -8,12 +8,16 @@ keeps the full run's length), then fill the "empty means derived" defaults.
 import dataclasses
 import difflib
 import math
+import re
 import tomllib
 import typing
 from pathlib import Path
 
 from plume_b200.recipe.errors import RecipeError
 from plume_b200.recipe.schema import CHANNEL_LAYOUTS, FACE_KINDS, SEED_MAX, Recipe
+
+# output names become file and folder names: one plain name, no path parts (recipe/rules.py:10-18)
+PLAIN_NAME = re.compile(r"^[A-Za-z0-9_][A-Za-z0-9._-]*$")
 
 
 def load_recipe(path: Path, preview: bool = False, sets=()) -> Recipe:
@@ -79,6 +83,8 @@ def check_rules(recipe: Recipe) -> None:
     time, solver = recipe.time, recipe.solver
     if time.duration_s <= 0 or time.frames < 1 or time.substeps < 1 or time.warmup_s < 0:
         raise RecipeError("time.duration_s must be above 0, frames and substeps at least 1, warmup_s at least 0")
+    if not math.isfinite(time.frames * time.substeps / time.duration_s):
+        raise RecipeError(f"time.duration_s is too small for {time.frames} frames, got {time.duration_s}")
     if solver.multigrid_cycles < 1 or solver.pressure_iterations < 1 or solver.max_substeps < 1:
         raise RecipeError("solver.multigrid_cycles, pressure_iterations and max_substeps must be at least 1")
     if solver.multigrid_sweeps < 2:
@@ -88,7 +94,13 @@ def check_rules(recipe: Recipe) -> None:
         raise RecipeError("solver.max_cells_per_step must be above 0")
     if not recipe.emitter:
         raise RecipeError("emitter needs at least one [[emitter]]")
+    names = []
     for index, e in enumerate(recipe.emitter):
+        if not e.name or any(mark in e.name for mark in ".[]"):  # key paths name emitters as emitter.<name>.<key>
+            raise RecipeError(f"emitter[{index}].name must be a name without '.', '[' or ']'; got {e.name!r}")
+        if e.name in names:
+            raise RecipeError(f"emitter[{index}].name {e.name!r} is used twice")
+        names.append(e.name)
         if e.shape == "sphere" and e.radius_m <= 0:
             raise RecipeError(f"emitter[{index}].radius_m must be above 0")
         if e.shape == "box" and any(size <= 0 for size in e.size_m):
@@ -100,6 +112,12 @@ def check_rules(recipe: Recipe) -> None:
         if e.noise.scale_m <= 0 or e.noise.strength < 0 or e.smoke_per_s < 0:
             raise RecipeError(f"emitter[{index}] noise.scale_m must be above 0, noise.strength and "
                               f"smoke_per_s at least 0")
+        _check_reaches_domain(domain.size_m, f"emitter[{index}]", e)
+    if recipe.camera.seat and recipe.camera.seat not in names:
+        raise RecipeError(f"camera.seat {recipe.camera.seat!r} is not an emitter; emitters are {', '.join(names)}")
+    if recipe.output.name and (not PLAIN_NAME.match(recipe.output.name) or ".." in recipe.output.name):
+        raise RecipeError(f"output.name must be a plain name of letters, digits, '.', '_' and '-'; got "
+                          f"{recipe.output.name!r} (when output.name is empty the recipe's file name is used)")
     forces = recipe.forces
     if forces.drag_per_s < 0 or forces.vorticity_confinement < 0 or forces.turbulence.scale_m <= 0:
         raise RecipeError("forces.drag_per_s and vorticity_confinement must be at least 0, "
@@ -109,6 +127,17 @@ def check_rules(recipe: Recipe) -> None:
                           "the wind")
     if recipe.output.channels not in CHANNEL_LAYOUTS:
         raise RecipeError(f"output.channels must be one of {', '.join(CHANNEL_LAYOUTS)}")
+
+
+def _check_reaches_domain(size, where: str, emitter) -> None:
+    """An emitter must reach into the domain (x and z span -size/2..size/2, y 0..size); its centre may lie
+    outside, as a source half sunk below the floor does (recipe/rules.py:86-99)."""
+    ranges = ((-size[0] / 2, size[0] / 2), (0.0, size[1]), (-size[2] / 2, size[2] / 2))
+    reaches = (emitter.radius_m,) * 3 if emitter.shape == "sphere" else tuple(s / 2 for s in emitter.size_m)
+    for axis, centre, reach, (low, high) in zip("xyz", emitter.center_m, reaches, ranges):
+        if centre - reach > high or centre + reach < low:
+            raise RecipeError(f"{where} lies outside the domain on {axis}: its center {centre:g} m reaches "
+                              f"{reach:g} m, and the domain spans {low:g} to {high:g} m")
 
 
 def _build(cls: type, table: dict, where: str):
@@ -137,9 +166,15 @@ def _convert(value, annotation, path: str):
     if dataclasses.is_dataclass(annotation):
         return _build(annotation, value, path)
     if annotation is float:
-        if isinstance(value, bool) or not isinstance(value, (int, float)) or not math.isfinite(float(value)):
-            raise RecipeError(f"{path} must be a finite number, got {value!r}")
-        return float(value)
+        if isinstance(value, bool) or not isinstance(value, (int, float)):
+            raise RecipeError(f"{path} must be a number, got {value!r}")
+        try:
+            number = float(value)
+        except OverflowError:  # a whole number beyond the float range
+            number = math.inf
+        if not math.isfinite(number):  # nan and inf would pass every range rule and fail deep in a run
+            raise RecipeError(f"{path} must be a finite number, got {number}")
+        return number
     if annotation is int:
         if isinstance(value, bool) or not isinstance(value, int):
             raise RecipeError(f"{path} must be a whole number, got {value!r}")
@@ -150,7 +185,8 @@ def _convert(value, annotation, path: str):
         return value
     args = typing.get_args(annotation)
     if not isinstance(value, list):
-        raise RecipeError(f"{path} must be a list, got {value!r}")
+        hint = f" (write [[{path}]] for each one)" if isinstance(value, dict) else ""
+        raise RecipeError(f"{path} must be a list, got {value!r}{hint}")
     if len(args) == 2 and args[1] is Ellipsis:
         return tuple(_convert(item, args[0], f"{path}[{i}]") for i, item in enumerate(value))
     if len(value) != len(args):
