@@ -94,3 +94,26 @@ def test_refined_pressure_matches_a_converged_fp64_solve(cuda_device):
     assert refined.ratio <= 1e-6
     exact = o.pressure
     assert np.abs(host(c.pressure) - exact).max() <= 1e-5 * np.abs(exact).max()
+
+
+@pytest.mark.parametrize("cells,faces", [((19, 24, 17), ALL_CLOSED), ((38, 48, 38), OPEN)],
+                         ids=["19x24x17-closed", "38x48x38-open"])
+def test_refine_on_closed_and_uneven_grids(cuda_device, cells, faces):
+    """All walls closed (the pressure is defined up to a constant; the walls are closed first, as a projection
+    does, so the divergence sums to zero) and levels with overhanging cells: the corrections shrink the
+    residual far below the plain cycles' and the pressure stays finite."""
+    import torch
+
+    from plume_b200.sim.multigrid import Multigrid
+    from plume_b200.sim.pressure import GaussSeidel, compute_divergence, project
+
+    c = cuda_grid(cells, 1.0 / 64.0, faces, 1.0)
+    for name, values in operator_fields(cells, 11, 1.0).items():
+        getattr(c, name).data.copy_(torch.from_numpy(values))
+    project(c, GaussSeidel(0))  # closes the walls
+    compute_divergence(c)
+    c.pressure.zero_()
+    refined = Multigrid(c, 4, 2).refine(c, rel_tol=1e-7)
+    print(f"{cells}: {refined.corrections} corrections: {', '.join(f'{r:.2e}' for r in refined.ratios)}")
+    assert refined.ratio <= 1e-5 and refined.ratios[-1] < refined.ratios[0]
+    assert torch.isfinite(c.pressure).all()
