@@ -423,28 +423,86 @@ struct FieldSet {
   int count;
 };
 
+// Where a launch's groups sit on the MAC grid, when the host can tell (layout_of): on the velocity
+// components' faces, group g holding component g, or on cell centres. The first velocity sample of every trace
+// is then formed from its corners with the weights known in advance: 1/2 between two corners, and one corner
+// alone where the clamp meets a wall (only along the axis in which the sample sits half a cell from the
+// element). The float operations and their order are velocity_at_node's, so the values are the same.
+enum AdvectLayout { LAYOUT_ANY = 0, LAYOUT_FACES = 1, LAYOUT_CELLS = 2 };
+
+template <int G>
+struct GroupIndex {
+  static constexpr int value = G;
+};
+
+// velocity_at_node (sample.py:74-82 at p = index + offset) for element (i, j, k) of group G.
+template <int LAYOUT, int G, class T>
+__device__ __forceinline__ F3 node_velocity(const VelT<T>& vel, int i, int j, int k, F3 p) {
+  if constexpr (LAYOUT == LAYOUT_ANY) {
+    return velocity_at_node(vel, p);
+  } else if constexpr (LAYOUT == LAYOUT_CELLS) {  // p = (i + 1/2, j + 1/2, k + 1/2): u, v, w halfway along x, y, z
+    const T* u = vel.u + at(vel.du, i, j, k);
+    const T* v = vel.v + at(vel.dv, i, j, k);
+    const T* w = vel.w + at(vel.dw, i, j, k);
+    return f3(lerpf_(ldg_f(u), ldg_f(u + vel.du.n1 * vel.du.n2), 0.5f), lerpf_(ldg_f(v), ldg_f(v + vel.dv.n2), 0.5f),
+              lerpf_(ldg_f(w), ldg_f(w + 1), 0.5f));
+  } else if constexpr (G == 0) {  // a u face, p = (i, j + 1/2, k + 1/2): v and w halfway along x except at the walls
+    const int nx = vel.dv.n0, i0 = imax_(i - 1, 0);
+    const bool wall = i == 0 || i == nx;
+    const int sv = vel.dv.n1 * vel.dv.n2, sw = vel.dw.n1 * vel.dw.n2;
+    auto along_x = [&](const T* q, int s) { return wall ? ldg_f(q) : lerpf_(ldg_f(q), ldg_f(q + s), 0.5f); };
+    const T* v = vel.v + at(vel.dv, i0, j, k);
+    const T* w = vel.w + at(vel.dw, i0, j, k);
+    return f3(ldg_f(vel.u + at(vel.du, i, j, k)), lerpf_(along_x(v, sv), along_x(v + vel.dv.n2, sv), 0.5f),
+              lerpf_(along_x(w, sw), along_x(w + 1, sw), 0.5f));
+  } else if constexpr (G == 1) {  // a v face, p = (i + 1/2, j, k + 1/2): u and w halfway along y except at the walls
+    const int ny = vel.du.n1, j0 = imax_(j - 1, 0);
+    const bool wall = j == 0 || j == ny;
+    const int su = vel.du.n1 * vel.du.n2;
+    const T* u = vel.u + at(vel.du, i, j0, k);
+    const T* w = vel.w + at(vel.dw, i, j0, k);
+    auto u_x = [&](const T* q) { return lerpf_(ldg_f(q), ldg_f(q + su), 0.5f); };
+    const float u_lo = u_x(u);
+    const float u_at = wall ? u_lo : lerpf_(u_lo, u_x(u + vel.du.n2), 0.5f);
+    auto w_y = [&](const T* q) { return wall ? ldg_f(q) : lerpf_(ldg_f(q), ldg_f(q + vel.dw.n2), 0.5f); };
+    return f3(u_at, ldg_f(vel.v + at(vel.dv, i, j, k)), lerpf_(w_y(w), w_y(w + 1), 0.5f));
+  } else {  // a w face, p = (i + 1/2, j + 1/2, k): u and v halfway along z except at the walls
+    const int nz = vel.du.n2, k0 = imax_(k - 1, 0);
+    const bool wall = k == 0 || k == nz;
+    const int su = vel.du.n1 * vel.du.n2;
+    const T* u = vel.u + at(vel.du, i, j, k0);
+    const T* v = vel.v + at(vel.dv, i, j, k0);
+    auto u_x = [&](const T* q) { return lerpf_(ldg_f(q), ldg_f(q + su), 0.5f); };
+    auto v_y = [&](const T* q) { return lerpf_(ldg_f(q), ldg_f(q + vel.dv.n2), 0.5f); };
+    const float u_lo = u_x(u), v_lo = v_y(v);
+    return f3(wall ? u_lo : lerpf_(u_lo, u_x(u + 1), 0.5f), wall ? v_lo : lerpf_(v_lo, v_y(v + 1), 0.5f),
+              ldg_f(vel.w + at(vel.dw, i, j, k)));
+  }
+}
+
 // semi_lagrangian_kernel (advect.py:24-31): the forward pass into `hat` (or, for plain semi-Lagrangian
 // advection, into `next`).
-// Calls body(group, slab) with the group of `set` that blockIdx.z falls in, as a constant index into the kernel
-// parameters (each group's body is compiled on its own, with its descriptor at fixed parameter offsets).
+// Calls body(group, slab, GroupIndex<g>) with the group of `set` that blockIdx.z falls in, as a constant index
+// into the kernel parameters (each group's body is compiled on its own, with its descriptor at fixed parameter
+// offsets).
 template <class T, class Body>
 __device__ __forceinline__ void for_group(const FieldSet<T>& set, Body body) {
   int slab = blockIdx.z;
-  if (slab < set.f[0].d.n0 || set.count == 1) return body(set.f[0], slab);
+  if (slab < set.f[0].d.n0 || set.count == 1) return body(set.f[0], slab, GroupIndex<0>{});
   slab -= set.f[0].d.n0;
-  if (slab < set.f[1].d.n0 || set.count == 2) return body(set.f[1], slab);
-  body(set.f[2], slab - set.f[1].d.n0);
+  if (slab < set.f[1].d.n0 || set.count == 2) return body(set.f[1], slab, GroupIndex<1>{});
+  body(set.f[2], slab - set.f[1].d.n0, GroupIndex<2>{});
 }
 
 // FIELDS: the group's field count when fixed at compile time, 0 to read it from the descriptor.
-template <int FIELDS, class T>
+template <int FIELDS, int LAYOUT, int G, class T>
 __device__ __forceinline__ void advect_forward_at(const PlumeGridInfo& info, const VelT<T>& vel, const FieldDesc<T>& fd,
                                                   int slab, float dt_over_cell, int write_next) {
   const int i = slab, j = blockIdx.y * blockDim.y + threadIdx.y, k = blockIdx.x * blockDim.x + threadIdx.x;
   if (j >= fd.d.n1 || k >= fd.d.n2) return;
   const int c = at(fd.d, i, j, k);
   const F3 p = add3(f3((float)i, (float)j, (float)k), fd.offset);
-  const F3 src = trace_from(vel, p, velocity_at_node(vel, p), dt_over_cell);
+  const F3 src = trace_from(vel, p, node_velocity<LAYOUT, G>(vel, i, j, k, p), dt_over_cell);
   const bool outside = fd.uses_outside == 1 && is_outside_open_face(src, info);
   const F3 g = sub3(src, fd.offset);
   for (int n = 0; n < (FIELDS ? FIELDS : fd.fields); ++n) {
@@ -458,24 +516,25 @@ __device__ __forceinline__ void advect_forward_at(const PlumeGridInfo& info, con
 // FIELDS: every group of the launch holds this many fields (1: the velocity components, 2: smoke and
 // temperature), a count the compiler then knows; 0 reads each group's count. Measured on B200, as kernels of
 // their own: velocity advection -3.5%, scalar advection -4%.
-template <class T, int FIELDS>
+// LAYOUT: an AdvectLayout the host found for every group of the launch.
+template <class T, int FIELDS, int LAYOUT>
 __global__ void k_advect_forward(PlumeGridInfo info, VelT<T> vel, FieldSet<T> set, float dt_over_cell, int write_next) {
-  for_group(set, [&](const FieldDesc<T>& fd, int slab) {
-    advect_forward_at<FIELDS>(info, vel, fd, slab, dt_over_cell, write_next);
+  for_group(set, [&](const FieldDesc<T>& fd, int slab, auto group) {
+    advect_forward_at<FIELDS, LAYOUT, decltype(group)::value>(info, vel, fd, slab, dt_over_cell, write_next);
   });
 }
 
 // maccormack_correct_kernel (advect.py:34-50) with the backward pass (advect.py:64) evaluated in place:
 // back = sample(hat, trace(p, -dt)), corrected = hat + (data - back) / 2, clamped to the range of the eight
 // values the forward sample blended.
-template <int FIELDS, class T, bool STORED_RANGE>
+template <int FIELDS, int LAYOUT, int G, class T, bool STORED_RANGE>
 __device__ __forceinline__ void advect_correct_at(const PlumeGridInfo& info, const VelT<T>& vel, const FieldDesc<T>& fd,
                                                   int slab, float dt_over_cell) {
   const int i = slab, j = blockIdx.y * blockDim.y + threadIdx.y, k = blockIdx.x * blockDim.x + threadIdx.x;
   if (j >= fd.d.n1 || k >= fd.d.n2) return;
   const int c = at(fd.d, i, j, k);
   const F3 p = add3(f3((float)i, (float)j, (float)k), fd.offset);
-  const F3 vp = velocity_at_node(vel, p);
+  const F3 vp = node_velocity<LAYOUT, G>(vel, i, j, k, p);
   const F3 back_src = trace_from(vel, p, vp, -dt_over_cell);
   const bool back_outside = fd.uses_outside == 1 && is_outside_open_face(back_src, info);
   const F3 gb = sub3(back_src, fd.offset);
@@ -501,11 +560,54 @@ __device__ __forceinline__ void advect_correct_at(const PlumeGridInfo& info, con
   }
 }
 
-template <class T, bool STORED_RANGE, int FIELDS>
+template <class T, bool STORED_RANGE, int FIELDS, int LAYOUT>
 __global__ void k_advect_correct(PlumeGridInfo info, VelT<T> vel, FieldSet<T> set, float dt_over_cell) {
-  for_group(set, [&](const FieldDesc<T>& fd, int slab) {
-    advect_correct_at<FIELDS, T, STORED_RANGE>(info, vel, fd, slab, dt_over_cell);
+  for_group(set, [&](const FieldDesc<T>& fd, int slab, auto group) {
+    advect_correct_at<FIELDS, LAYOUT, decltype(group)::value, T, STORED_RANGE>(info, vel, fd, slab, dt_over_cell);
   });
+}
+
+// The AdvectLayout of a launch: LAYOUT_FACES when its three groups are the velocity components' faces in
+// order, LAYOUT_CELLS when every group sits at the cell centres, LAYOUT_ANY otherwise.
+template <class T>
+static int layout_of(const PlumeGridInfo& info, const FieldSet<T>& set) {
+  const int nx = info.dims[0], ny = info.dims[1], nz = info.dims[2];
+  auto is = [](const FieldDesc<T>& f, Dims d, float ox, float oy, float oz) {
+    return f.d.n0 == d.n0 && f.d.n1 == d.n1 && f.d.n2 == d.n2 && f.offset[0] == ox && f.offset[1] == oy &&
+           f.offset[2] == oz;
+  };
+  if (set.count == 3 && is(set.f[0], Dims{nx + 1, ny, nz}, 0.0f, 0.5f, 0.5f) &&
+      is(set.f[1], Dims{nx, ny + 1, nz}, 0.5f, 0.0f, 0.5f) && is(set.f[2], Dims{nx, ny, nz + 1}, 0.5f, 0.5f, 0.0f))
+    return LAYOUT_FACES;
+  for (int n = 0; n < set.count; ++n)
+    if (!is(set.f[n], Dims{nx, ny, nz}, 0.5f, 0.5f, 0.5f)) return LAYOUT_ANY;
+  return LAYOUT_CELLS;
+}
+
+// The compiled forms: the velocity components on their faces (one field a group), smoke and temperature or a
+// single scalar at the cell centres, and the general kernels for any other launch.
+template <class T>
+using ForwardKernel = void (*)(PlumeGridInfo, VelT<T>, FieldSet<T>, float, int);
+template <class T>
+using CorrectKernel = void (*)(PlumeGridInfo, VelT<T>, FieldSet<T>, float);
+
+template <class T>
+static ForwardKernel<T> forward_kernel(int fields, int layout) {
+  if (layout == LAYOUT_FACES && fields == 1) return k_advect_forward<T, 1, LAYOUT_FACES>;
+  if (layout == LAYOUT_CELLS && fields == 1) return k_advect_forward<T, 1, LAYOUT_CELLS>;
+  if (layout == LAYOUT_CELLS && fields == 2) return k_advect_forward<T, 2, LAYOUT_CELLS>;
+  return fields == 1 ? k_advect_forward<T, 1, LAYOUT_ANY>
+                     : (fields == 2 ? k_advect_forward<T, 2, LAYOUT_ANY> : k_advect_forward<T, 0, LAYOUT_ANY>);
+}
+
+template <class T, bool STORED_RANGE>
+static CorrectKernel<T> correct_kernel(int fields, int layout) {
+  if (layout == LAYOUT_FACES && fields == 1) return k_advect_correct<T, STORED_RANGE, 1, LAYOUT_FACES>;
+  if (layout == LAYOUT_CELLS && fields == 1) return k_advect_correct<T, STORED_RANGE, 1, LAYOUT_CELLS>;
+  if (layout == LAYOUT_CELLS && fields == 2) return k_advect_correct<T, STORED_RANGE, 2, LAYOUT_CELLS>;
+  return fields == 1 ? k_advect_correct<T, STORED_RANGE, 1, LAYOUT_ANY>
+                     : (fields == 2 ? k_advect_correct<T, STORED_RANGE, 2, LAYOUT_ANY>
+                                    : k_advect_correct<T, STORED_RANGE, 0, LAYOUT_ANY>);
 }
 
 template <class T>
@@ -521,7 +623,8 @@ static int launch_advect(const PlumeGridInfo& info, const VelT<T>& vel, const Fi
   int fields = set.f[0].fields;  // the groups' common field count, or 0 when they differ
   for (int n = 1; n < set.count; ++n)
     if (set.f[n].fields != fields) fields = 0;
-  auto forward = fields == 1 ? k_advect_forward<T, 1> : (fields == 2 ? k_advect_forward<T, 2> : k_advect_forward<T, 0>);
+  const int layout = layout_of(info, set);
+  const ForwardKernel<T> forward = forward_kernel<T>(fields, layout);
   if (!maccormack) {
     forward<<<grid, cell_block(), 0, st>>>(info, vel, set, dt_over_cell, 1);
     CHECK_LAUNCH("semi-Lagrangian advection");
@@ -529,11 +632,8 @@ static int launch_advect(const PlumeGridInfo& info, const VelT<T>& vel, const Fi
   }
   forward<<<grid, cell_block(), 0, st>>>(info, vel, set, dt_over_cell, 0);
   CHECK_LAUNCH("MacCormack forward pass");
-  auto correct = set.f[0].range[0]
-                      ? (fields == 1 ? k_advect_correct<T, true, 1>
-                                     : (fields == 2 ? k_advect_correct<T, true, 2> : k_advect_correct<T, true, 0>))
-                      : (fields == 1 ? k_advect_correct<T, false, 1>
-                                     : (fields == 2 ? k_advect_correct<T, false, 2> : k_advect_correct<T, false, 0>));
+  const CorrectKernel<T> correct =
+      set.f[0].range[0] ? correct_kernel<T, true>(fields, layout) : correct_kernel<T, false>(fields, layout);
   correct<<<grid, cell_block(), 0, st>>>(info, vel, set, dt_over_cell);
   CHECK_LAUNCH("MacCormack correction");
   return PLUME_OK;

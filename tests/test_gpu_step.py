@@ -11,7 +11,7 @@ import pytest
 from oracle import oracle as O
 from plume_b200.recipe.derived import derive
 from plume_b200.workloads import operator_fields, plain_step_recipe
-from support import FIELDS, host, load_state, max_rel
+from support import FIELDS, assert_same, host, load_state, max_rel
 
 pytestmark = pytest.mark.gpu
 GOLDEN = Path(__file__).resolve().parent / "golden"
@@ -46,6 +46,31 @@ def test_one_substep_matches_the_oracle(cuda_device, cells):
     os_.step(0.0, derived.dt_s)
     cs.step(0.0, derived.dt_s)
     compare_fields(o, c, SUBSTEP_RTOL, "one substep")
+
+
+@pytest.mark.parametrize("cells,faces", [((19, 24, 17), None), ((16, 12, 20), "closed"), ((2, 3, 1), None)],
+                         ids=["19x24x17-open", "16x12x20-closed", "2x3x1-open"])
+def test_a_substep_without_exp_or_pow_gives_the_oracles_floats(cuda_device, cells, faces):
+    """With the emitter finished and no drag or dissipation, no operator of the substep calls exp or pow, so
+    every field, the pressure included, is the oracle's to the last bit: the step's velocity advection (the
+    three face arrays in one launch) and its smoke and temperature advection, walls included."""
+    import dataclasses
+
+    recipe = plain_step_recipe(cells, cycles=2)
+    recipe = dataclasses.replace(
+        recipe, emitter=[dataclasses.replace(recipe.emitter[0], end_s=0.01)],
+        forces=dataclasses.replace(recipe.forces, drag_per_s=0.0),
+        dissipation=dataclasses.replace(recipe.dissipation, smoke_per_s=0.0, cooling_per_s=0.0))
+    if faces == "closed":
+        recipe = dataclasses.replace(recipe, domain=dataclasses.replace(
+            recipe.domain, faces=dataclasses.replace(recipe.domain.faces, **{
+                f.name: "closed" for f in dataclasses.fields(recipe.domain.faces)})))
+    o, c, os_, cs, derived = stepper_pair(recipe)
+    os_.step(1.0, derived.dt_s)
+    cs.step(1.0, derived.dt_s)
+    for name in FIELDS:
+        assert_same(host(getattr(c, name).data), getattr(o, name).data, name)
+    assert_same(host(c.pressure), o.pressure, "pressure")
 
 
 def test_eight_substeps_with_turbulence_and_dissipation_match_the_oracle(cuda_device):
