@@ -211,9 +211,16 @@ def batched_variant(device: str, count: int = 32, frames: int = 24) -> dict:
     import torch
 
     from plume_b200.sim.batch import Batch, run_one_at_a_time
-    from plume_b200.workloads import batched_recipes
+    from plume_b200.workloads import BATCH_GRIDS, batched_recipes
 
     recipes = batched_recipes(count=count, frames=frames)
+    # both schedules once on a short run of every grid size first, so that neither timed arm pays for the
+    # first launches of its kernels and graphs (without this the arm run first measured up to 25% slow)
+    warm = [r for grid in BATCH_GRIDS for r in batched_recipes(count=1, frames=2, grids=(grid,))]
+    run_one_at_a_time(warm, device)
+    Batch(warm, device).run()
+    torch.cuda.synchronize()
+    torch.cuda.empty_cache()
     result = {}
     for arm in ("one_at_a_time", "batched"):
         torch.cuda.synchronize()
