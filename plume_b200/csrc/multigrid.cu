@@ -138,6 +138,33 @@ __global__ void k_rb_colour(PlumeGridInfo info, float* q, const float* __restric
     q[idx] = out;
 }
 
+// The same colour pass with each thread updating one cell in each of two neighbouring planes (i, i + 1): two
+// independent updates whose loads are in flight together. The two cells are the same colour and not face
+// neighbours, and every update is the one above, so the result is the same. Measured on B200: the 4-cycle
+// solve at 256x384x256 went from 3.727 to 3.570 ms with every level swept this way, but at 128x192x128 from
+// 0.780 to 0.828 ms: it pays only on levels that do not fit in L2 (RB_PAIR_MIN_CELLS).
+template <bool UNIFORM>
+__global__ void k_rb_colour_pair(PlumeGridInfo info, float* q, const float* __restrict__ rhs, int color,
+                                 float relaxation) {
+  wait_for_previous_grid();
+  const int nx = info.dims[0], ny = info.dims[1], nz = info.dims[2];
+  const int i = 2 * blockIdx.z, j = blockIdx.y * blockDim.y + threadIdx.y;
+  const int kp = 2 * (blockIdx.x * blockDim.x + threadIdx.x);
+  const int k0 = kp + ((i + j + color) & 1), k1 = kp + ((i + 1 + j + color) & 1);
+  if (j >= ny) return;
+  const bool has0 = k0 < nz, has1 = i + 1 < nx && k1 < nz;
+  const Dims d = dims_of(info);
+  auto load = [&](int a, int b, int c) { return q[at(d, a, b, c)]; };
+  const float ghost = ghost_coupling(info);
+  const int idx0 = at(d, i, j, k0), idx1 = at(d, i + 1, j, k1);
+  float out0 = 0.0f, out1 = 0.0f;
+  bool w0 = false, w1 = false;
+  if (has0) w0 = relax_cell(UNIFORM, info, ghost, i, j, k0, q[idx0], __ldg(rhs + idx0), relaxation, load, out0);
+  if (has1) w1 = relax_cell(UNIFORM, info, ghost, i + 1, j, k1, q[idx1], __ldg(rhs + idx1), relaxation, load, out1);
+  if (w0) q[idx0] = out0;
+  if (w1) q[idx1] = out1;
+}
+
 // prolong_add_kernel (multigrid.py:63-68), used when a level has no post-smoothing sweep to fold it into.
 __global__ void k_prolong_add(Dims coarse, Dims fine, const float* __restrict__ cq, float* __restrict__ q) {
   wait_for_previous_grid();
@@ -805,8 +832,22 @@ static void launch_tiled(const PlumeGridInfo& info, Pressure& q, const float* rh
     k_rb_sweep<PROLONG, false><<<tile_grid(info), SWEEP_THREADS, 0, st>>>(info, q.cur, q.other, rhs, relaxation, coarse_q, cd);
 }
 
+// Levels of at least this many cells (q and rhs over 64 MB) sweep two planes per thread (k_rb_colour_pair).
+constexpr long RB_PAIR_MIN_CELLS = 1L << 23;
+
 static int colour_sweep(const PlumeGridInfo& info, float* q, const float* rhs, float relaxation, cudaStream_t st) {
   const Dims d = dims_of(info);
+  if (cells_of(info) >= RB_PAIR_MIN_CELLS) {
+    const dim3 grid(((d.n2 + 1) / 2 + TZ - 1) / TZ, (d.n1 + TY - 1) / TY, (d.n0 + 1) / 2);
+    for (int color = 0; color < 2; ++color) {
+      int status = uniform_level(info) ? launch_solve_kernel(k_rb_colour_pair<true>, grid, cell_block(), 0, st,
+                                                             "red-black colour", info, q, rhs, color, relaxation)
+                                       : launch_solve_kernel(k_rb_colour_pair<false>, grid, cell_block(), 0, st,
+                                                             "red-black colour", info, q, rhs, color, relaxation);
+      if (status != PLUME_OK) return status;
+    }
+    return PLUME_OK;
+  }
   const dim3 grid(((d.n2 + 1) / 2 + TZ - 1) / TZ, (d.n1 + TY - 1) / TY, d.n0);
   for (int color = 0; color < 2; ++color) {
     const float* none = nullptr;

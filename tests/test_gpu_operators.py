@@ -123,6 +123,25 @@ def test_projection_matches_the_oracle(cuda_device, cells, faces):
         assert_same(host(compute_divergence(c)), O.compute_divergence(o), f"{solver} divergence")
 
 
+@pytest.mark.parametrize("cells", [(128, 256, 256), (129, 256, 255)], ids=["128x256x256", "129x256x255"])
+def test_projection_on_a_level_beyond_l2_matches_the_oracle(cuda_device, cells):
+    """Levels of at least 2^23 cells sweep two planes per thread: Gauss-Seidel sweeps and a V-cycle at that
+    size (an odd plane count and an odd row length in the second case) give the oracle's floats."""
+    from plume_b200.sim.multigrid import Multigrid
+    from plume_b200.sim.pressure import GaussSeidel, project
+
+    assert cells[0] * cells[1] * cells[2] >= 1 << 23
+    fields = operator_fields(cells, 11, 1.0)
+    for solver in ("gauss_seidel", "multigrid"):
+        o, c = oracle_grid(cells, 1.0 / 64.0, OPEN, 1.0), cuda_grid(cells, 1.0 / 64.0, OPEN, 1.0)
+        load_state(o, c, fields)
+        os_, cs = (O.GaussSeidel(3), GaussSeidel(3)) if solver == "gauss_seidel" else (O.Multigrid(o, 1, 2),
+                                                                                     Multigrid(c, 1, 2))
+        O.project(o, os_)
+        project(c, cs)
+        assert_same(host(c.pressure), o.pressure, f"{solver} pressure")
+
+
 def test_multigrid_residual_matches_the_oracle(cuda_device):
     from plume_b200.sim.multigrid import Multigrid
     from plume_b200.sim.pressure import compute_divergence
