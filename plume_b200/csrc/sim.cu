@@ -850,15 +850,24 @@ __global__ void k_line_partials(Dims d, const T* __restrict__ a, const T* __rest
 }
 
 // totals[0..2] = before, semi-Lagrangian, MacCormack; factor = held / MacCormack (1 when MacCormack <= 0).
+// One warp per total (threadIdx.y): the lanes load 32 block partials at a time and every lane adds them in
+// block order from the shuffles, the same additions in the same order as one thread walking the partials.
+// Measured on B200 at 128x192x128 (96 partials per total), cold under ncu: 13.0-16.7 us on one thread,
+// 3.7-5.0 us this way; the scalar advection phase went from 0.176 to 0.172 ms (1.154 to 1.137 ms at
+// 256x384x256).
 __global__ void k_budget_factor(const double* __restrict__ partial, int blocks, float* factor, double* totals_out,
                                 int want_factor) {
-  if (threadIdx.x != 0 || blockIdx.x != 0) return;
-  double t[3];
-  for (int which = 0; which < 3; ++which) {
-    double total = 0.0;
-    for (int b = 0; b < blocks; ++b) total = total + partial[which * blocks + b];
-    t[which] = total;
+  __shared__ double t[3];
+  const int which = threadIdx.y, lane = threadIdx.x;
+  double total = 0.0;
+  for (int base = 0; base < blocks; base += 32) {
+    const double mine = base + lane < blocks ? partial[which * blocks + base + lane] : 0.0;
+    const int count = blocks - base < 32 ? blocks - base : 32;
+    for (int l = 0; l < count; ++l) total = total + __shfl_sync(0xffffffffu, mine, l);
   }
+  if (lane == 0) t[which] = total;
+  __syncthreads();
+  if (threadIdx.x != 0 || threadIdx.y != 0) return;
   if (totals_out) {
     totals_out[0] = t[0];
     totals_out[1] = t[1];
@@ -885,7 +894,7 @@ static int launch_triple_sum(const Dims& d, const T* a, const T* b, const T* c, 
   const int blocks = sum_blocks(d);
   k_line_partials<T><<<dim3(blocks, 3), SUM_BLOCK, 0, st>>>(d, a, b, c, sums, blocks);
   CHECK_LAUNCH("line sums");
-  k_budget_factor<<<1, 32, 0, st>>>(sums, blocks, factor, totals_out, factor != nullptr);
+  k_budget_factor<<<1, dim3(32, 3), 0, st>>>(sums, blocks, factor, totals_out, factor != nullptr);
   CHECK_LAUNCH("budget factor");
   return PLUME_OK;
 }
