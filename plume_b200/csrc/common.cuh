@@ -194,9 +194,13 @@ __host__ __device__ __forceinline__ VelT<T> make_vel(const T* u, const T* v, con
 
 template <class T>
 __device__ __forceinline__ F3 velocity_at(const VelT<T>& vel, F3 p) {  // sample.py:74-82
-  return f3(sample_index_space(vel.u, vel.du, sub3(p, f3(0.0f, 0.5f, 0.5f))),
-            sample_index_space(vel.v, vel.dv, sub3(p, f3(0.5f, 0.0f, 0.5f))),
-            sample_index_space(vel.w, vel.dw, sub3(p, f3(0.5f, 0.5f, 0.0f))));
+  // The three extents from one set of cell counts (make_vel's), so that the axes two components share (the
+  // same coordinate and extent: x of v and w, y of u and w, z of u and v) are visibly one computation.
+  const int nx = vel.dv.n0, ny = vel.du.n1, nz = vel.du.n2;
+  const Dims du{nx + 1, ny, nz}, dv{nx, ny + 1, nz}, dw{nx, ny, nz + 1};
+  return f3(sample_index_space(vel.u, du, sub3(p, f3(0.0f, 0.5f, 0.5f))),
+            sample_index_space(vel.v, dv, sub3(p, f3(0.5f, 0.0f, 0.5f))),
+            sample_index_space(vel.w, dw, sub3(p, f3(0.5f, 0.5f, 0.0f))));
 }
 
 // Midpoint backtrace (advect.py:16-21); a negative dt_over_cell traces forward.

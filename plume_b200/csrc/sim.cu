@@ -517,8 +517,10 @@ __device__ __forceinline__ void advect_forward_at(const PlumeGridInfo& info, con
 // temperature), a count the compiler then knows; 0 reads each group's count. Measured on B200, as kernels of
 // their own: velocity advection -3.5%, scalar advection -4%.
 // LAYOUT: an AdvectLayout the host found for every group of the launch.
+// 32 registers (8 blocks of 256 a SM): without the bound the shared velocity axes take 40-43 and the lower
+// occupancy costs more than the sharing saves. Measured on B200 with the bound: velocity advection -2.2%.
 template <class T, int FIELDS, int LAYOUT>
-__global__ void k_advect_forward(PlumeGridInfo info, VelT<T> vel, FieldSet<T> set, float dt_over_cell, int write_next) {
+__global__ void __launch_bounds__(256, 8) k_advect_forward(PlumeGridInfo info, VelT<T> vel, FieldSet<T> set, float dt_over_cell, int write_next) {
   for_group(set, [&](const FieldDesc<T>& fd, int slab, auto group) {
     advect_forward_at<FIELDS, LAYOUT, decltype(group)::value>(info, vel, fd, slab, dt_over_cell, write_next);
   });
@@ -560,8 +562,10 @@ __device__ __forceinline__ void advect_correct_at(const PlumeGridInfo& info, con
   }
 }
 
+// With a stored range, 32 registers as in the forward pass. Tracing forward again needs more: it spills at 32
+// and at 40, so those forms get 48.
 template <class T, bool STORED_RANGE, int FIELDS, int LAYOUT>
-__global__ void k_advect_correct(PlumeGridInfo info, VelT<T> vel, FieldSet<T> set, float dt_over_cell) {
+__global__ void __launch_bounds__(256, STORED_RANGE ? 8 : 5) k_advect_correct(PlumeGridInfo info, VelT<T> vel, FieldSet<T> set, float dt_over_cell) {
   for_group(set, [&](const FieldDesc<T>& fd, int slab, auto group) {
     advect_correct_at<FIELDS, LAYOUT, decltype(group)::value, T, STORED_RANGE>(info, vel, fd, slab, dt_over_cell);
   });
