@@ -441,6 +441,12 @@ def preview_run_variant(device: str) -> dict:
             "mcell_substeps_per_s": math.prod(run.derived.cells) * run.steps.total_steps / seconds / 1e6}
 
 
+def workload_name(derived, cycles: int) -> str:
+    """The workload both arms time, by what it is and its sizes."""
+    return (f"plain FP32 fluid step {'x'.join(map(str, derived.cells))} (seeded smoothed velocities, masked smoke "
+            f"sphere), {cycles} multigrid V-cycles x 2+2 sweeps, confinement + drag + emitter, dt 1/96 s")
+
+
 def run_reference(args, cells):
     """--impl reference: the oracle port of the reference's CPU path on the host cores."""
     world, rank, _ = dist_env()
@@ -474,8 +480,8 @@ def run_reference(args, cells):
             "warmup": args.warmup, "ms_per_step": elapsed * 1e3 / timed, "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
             "impl": "reference",
-            "config": {"workload": f"plain FP32 fluid step {'x'.join(map(str, derived.cells))}, 4 multigrid V-cycles",
-                       "cells": list(derived.cells), "parallelism": "replicas"},
+            "config": {"workload": workload_name(derived, recipe.solver.multigrid_cycles),
+                       "cells": list(derived.cells), "parallelism": f"replicas x{world}"},
             "cpu_baseline": {"value": value, "unit": METRIC, "cores": threads, "kind": "port", "sample": sample},
             "e2e": {"value": value, "unit": METRIC, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
     print(json.dumps(line), flush=True)
@@ -617,9 +623,7 @@ def main():
         "metric": METRIC, "value": value, "unit": METRIC, "n_gpus": world, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": max_ms / args.steps, "higher_is_better": True, "scaling": "weak",
         "vs_baseline": None, "dtype": "f32", "data": "synthetic",
-        "config": {"workload": f"plain FP32 fluid step {'x'.join(map(str, derived.cells))} (seeded smoothed "
-                               f"velocities, masked smoke sphere), {cycles} multigrid V-cycles x 2+2 sweeps, "
-                               f"confinement + drag + emitter, dt 1/96 s",
+        "config": {"workload": workload_name(derived, cycles),
                    "cells": list(derived.cells), "parallelism": f"replicas x{world}",
                    "l2": f"inputs larger than L2 ({resident_gb:.2f} GB resident per grid; L2 is 126 MB)"},
         "roofline": {"bound": "hbm", "kernel": f"{dominant} phase of plume_step", "achieved": achieved, "peak": peak,
