@@ -80,6 +80,15 @@ class ClockSampler:
             self.proc = subprocess.Popen(cmd, stdout=self.file, stderr=subprocess.DEVNULL)
         except OSError:
             self.proc = None
+        # nvidia-smi takes a moment to start: wait (at most 3 s) for its first row, so that the timed region is
+        # sampled from its start, and leave out the rows taken before it
+        self.skip = 0
+        deadline = time.perf_counter() + 3.0
+        while self.proc is not None and self.proc.poll() is None and time.perf_counter() < deadline:
+            self.skip = len(self._rows())
+            if self.skip:
+                break
+            time.sleep(0.01)
         return self
 
     def __exit__(self, *exc):
@@ -90,10 +99,14 @@ class ClockSampler:
             except subprocess.TimeoutExpired:
                 self.proc.kill()
 
-    def summary(self) -> dict:
+    def _rows(self) -> list[list[str]]:
         self.file.flush()
         rows = [line.split(",") for line in Path(self.file.name).read_text().splitlines() if line.strip()]
-        rows = [[c.strip() for c in r] for r in rows if len(r) >= 10]
+        return [[c.strip() for c in r] for r in rows if len(r) >= 10]
+
+    def summary(self) -> dict:
+        rows = self._rows()
+        rows = rows[self.skip:] or rows
         if not rows:
             return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unsampled"]}
         sm = [float(r[2]) for r in rows if r[2].replace(".", "").isdigit()]
