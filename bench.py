@@ -13,13 +13,16 @@ cores) on the same workload; the reference itself is Python driving NVIDIA Warp,
 """
 
 import argparse
+import datetime
 import json
 import math
 import os
+import shutil
+import signal
 import statistics
 import subprocess
 import sys
-import tempfile
+import threading
 import time
 from pathlib import Path
 
@@ -61,60 +64,104 @@ def peaks() -> tuple[float, str]:
 
 
 class ClockSampler:
-    """nvidia-smi clock and throttle samples for one GPU while the timed region runs."""
+    """nvidia-smi clock and throttle samples for one GPU while the timed region runs.
 
-    QUERY = ("index,uuid,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+    Each row carries nvidia-smi's own timestamp, and only the rows stamped between `mark_start()` and the exit
+    of the `with` block count. nvidia-smi runs line-buffered (stdbuf) into a pipe that a thread reads, and it
+    is stopped with SIGINT so that it flushes its last rows. With no row inside the region the summary says
+    "unsampled" instead of reporting a clock taken outside it."""
+
+    QUERY = ("timestamp,index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+    REASONS = ("hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap")
 
-    def __init__(self, uuid: str | None):
+    def __init__(self, uuid: str | None, command: list[str] | None = None, period_ms: int = 20):
         self.uuid = uuid
-        self.file = tempfile.NamedTemporaryFile("w+", suffix=".csv", delete=False)
+        self.command = command
+        self.period_ms = period_ms
         self.proc = None
+        self.thread = None
+        self.rows: list[list[str]] = []
+        self.lock = threading.Lock()
+        self.start_s = self.end_s = None
+
+    def _cmd(self) -> list[str]:
+        if self.command is not None:
+            return list(self.command)
+        cmd = ["nvidia-smi", f"--query-gpu={self.QUERY}", "--format=csv,noheader,nounits", "-lms", str(self.period_ms)]
+        if self.uuid:
+            cmd += ["-i", self.uuid]
+        return (["stdbuf", "-oL"] if shutil.which("stdbuf") else []) + cmd
+
+    def _read(self):
+        for line in self.proc.stdout:
+            cols = [c.strip() for c in line.split(",")]
+            if len(cols) >= 10:
+                with self.lock:
+                    self.rows.append(cols)
 
     def __enter__(self):
         try:
-            cmd = ["nvidia-smi", f"--query-gpu={self.QUERY}", "--format=csv,noheader,nounits", "-lms", "20"]
-            if self.uuid:
-                cmd += ["-i", self.uuid]
-            self.proc = subprocess.Popen(cmd, stdout=self.file, stderr=subprocess.DEVNULL)
+            self.proc = subprocess.Popen(self._cmd(), stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True,
+                                         bufsize=1)
         except OSError:
             self.proc = None
-        # nvidia-smi takes a moment to start: wait (at most 3 s) for its first row, so that the timed region is
-        # sampled from its start, and leave out the rows taken before it
-        self.skip = 0
-        deadline = time.perf_counter() + 3.0
-        while self.proc is not None and self.proc.poll() is None and time.perf_counter() < deadline:
-            self.skip = len(self._rows())
-            if self.skip:
-                break
-            time.sleep(0.01)
+        if self.proc is not None:
+            self.thread = threading.Thread(target=self._read, daemon=True)
+            self.thread.start()
+            deadline = time.perf_counter() + 3.0  # nvidia-smi takes a moment to start: wait for its first row
+            while self.proc.poll() is None and time.perf_counter() < deadline:
+                with self.lock:
+                    if self.rows:
+                        break
+                time.sleep(0.01)
+        self.mark_start()
         return self
 
+    def mark_start(self):
+        """The timed region starts now (wall clock, as nvidia-smi stamps its rows)."""
+        self.start_s = time.time()
+
     def __exit__(self, *exc):
+        self.end_s = time.time()
         if self.proc is not None:
-            self.proc.terminate()
+            time.sleep(2 * self.period_ms / 1e3)  # let a row stamped inside the region reach the pipe
             try:
-                self.proc.wait(timeout=5)
+                self.proc.send_signal(signal.SIGINT)
+                self.proc.wait(timeout=3)
             except subprocess.TimeoutExpired:
                 self.proc.kill()
+                self.proc.wait()
+            if self.thread is not None:
+                self.thread.join(timeout=3)
 
-    def _rows(self) -> list[list[str]]:
-        self.file.flush()
-        rows = [line.split(",") for line in Path(self.file.name).read_text().splitlines() if line.strip()]
-        return [[c.strip() for c in r] for r in rows if len(r) >= 10]
+    @staticmethod
+    def _stamp(text: str) -> float | None:
+        for fmt in ("%Y/%m/%d %H:%M:%S.%f", "%Y/%m/%d %H:%M:%S"):
+            try:
+                return datetime.datetime.strptime(text, fmt).timestamp()
+            except ValueError:
+                continue
+        return None
 
     def summary(self) -> dict:
-        rows = self._rows()
-        rows = rows[self.skip:] or rows
-        if not rows:
-            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unsampled"]}
-        sm = [float(r[2]) for r in rows if r[2].replace(".", "").isdigit()]
-        max_sm = [float(r[3]) for r in rows if r[3].replace(".", "").isdigit()]
-        names = ("hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap")
-        reasons = sorted({name for r in rows for name, flag in zip(names, r[6:10]) if flag.lower() == "active"})
+        with self.lock:
+            rows = list(self.rows)
+        inside = []
+        for r in rows:
+            t = self._stamp(r[0])
+            if t is not None and self.start_s is not None and self.end_s is not None and \
+                    self.start_s <= t <= self.end_s:
+                inside.append(r)
+        if not inside:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unsampled"], "samples": 0,
+                    "rows_outside_region": len(rows)}
+        sm = [float(r[2]) for r in inside if r[2].replace(".", "").isdigit()]
+        max_sm = [float(r[3]) for r in inside if r[3].replace(".", "").isdigit()]
+        reasons = sorted({name for r in inside for name, flag in zip(self.REASONS, r[6:10]) if flag.lower() == "active"})
         return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": max(max_sm) if max_sm else None,
-                "reasons": reasons, "samples": len(rows)}
+                "reasons": reasons, "samples": len(inside), "rows_outside_region": len(rows) - len(inside)}
 
 
 def dist_env():

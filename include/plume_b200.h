@@ -255,8 +255,10 @@ int plume_smoke_budget(const PlumeGridInfo* info, const float* data, const float
  * fixed 96 KiB array inside the library, reserved on every device that loads it until the process exits; no
  * memory is allocated or freed by the call. Limit: ny * nz <= 1048576 (1 << 20) lines, else PLUME_ERR_INVALID.
  * The first call on a device looks up the array's device address on that device (make it before any stream
- * capture). All calls share the one array: calls that overlap on the GPU (other streams, other threads) race
- * and must be ordered by the caller. */
+ * capture). That address is kept for the life of the process: after cudaDeviceReset, or a release and
+ * re-creation of the device's primary context, the library's module reloads and the kept address is stale, so
+ * a process that resets a device must not call this entry point again on it. All calls share the one array:
+ * calls that overlap on the GPU (other streams, other threads) race and must be ordered by the caller. */
 int plume_smoke_budget_static(const PlumeGridInfo* info, const float* data, const float* hat, float* next,
                               double* totals_out, void* stream);
 

@@ -80,13 +80,16 @@ class Batch:
             grid = make_grid(derived, d.cell_m, d.faces, d.ambient_k, device, storage=storage)
             if initial_state is not None:
                 initial_state(index, grid)
+            # Everything that fills device memory on the current stream (the grid, the stepper's multigrid
+            # levels and scratch, the speed slot) is enqueued before the instance's stream waits on it.
+            stepper = Stepper(grid, recipe)
+            speed = torch.zeros(1, dtype=torch.float32, device=device)
+            host_speed = torch.zeros(1, dtype=torch.float32, pin_memory=True)
             stream = torch.cuda.Stream(device)
-            stream.wait_stream(current)  # the allocations and initial state above
+            stream.wait_stream(current)
             self.instances.append(_Instance(
-                recipe=recipe, derived=derived, grid=grid, stepper=Stepper(grid, recipe), cap=StepCap(recipe),
-                stream=stream, blocks=_blocks(recipe, derived),
-                speed=torch.zeros(1, dtype=torch.float32, device=device),
-                host_speed=torch.zeros(1, dtype=torch.float32, pin_memory=True)))
+                recipe=recipe, derived=derived, grid=grid, stepper=stepper, cap=StepCap(recipe),
+                stream=stream, blocks=_blocks(recipe, derived), speed=speed, host_speed=host_speed))
 
     def _request_speed(self, inst: _Instance) -> None:
         with torch.cuda.stream(inst.stream):

@@ -1,6 +1,6 @@
 """Regenerates the oracle's golden fixtures and pins the oracle against the reference.
 
-Run from the repository root, in a container where chadmv/plume is mounted at /root/reference:
+Run from the repository root, in a container where chadmv/plume is mounted at /root/reference (or at $PLUME_REFERENCE):
 
     python tests/golden/make_golden.py
 
@@ -19,6 +19,7 @@ statistics; they never read the reference.
 
 import hashlib
 import json
+import os
 import sys
 from pathlib import Path
 
@@ -26,7 +27,7 @@ import numpy as np
 
 HERE = Path(__file__).resolve().parent
 REPO = HERE.parents[1]
-REFERENCE_SRC = Path("/root/reference/src")
+REFERENCE_SRC = Path(os.environ.get("PLUME_REFERENCE", "/root/reference")) / "src"
 sys.path.insert(0, str(REPO))
 
 from oracle import oracle as O  # noqa: E402

@@ -48,3 +48,25 @@ def test_batch_matches_one_at_a_time(cuda_device, storage):
         for name, values in fields.items():
             assert torch.equal(together[key][name], values), (key, name)
     assert any(log.added_steps > 0 for log in logs_alone)  # the CFL cap split some blocks
+
+
+def test_batch_waits_for_its_setup_on_a_delayed_stream(cuda_device):
+    """The instances' streams start only after the grid, the stepper's levels and scratch and the speed slot
+    are filled on the current stream: with that stream held busy while the batch is built, the batch still
+    gives the bytes and step counts of running each recipe alone."""
+    import torch
+
+    from plume_b200.sim.batch import Batch, run_one_at_a_time
+
+    recipes = batched_recipes(count=3, frames=3, seed=9, grids=SMALL_GRIDS)
+    alone, together = {}, {}
+    logs_alone = run_one_at_a_time(recipes, "cuda:0", initial_state=seeded,
+                                   capture=lambda i, f, g: alone.__setitem__((i, f), g.smoke.data.clone()))
+    torch.cuda.synchronize()
+    torch.cuda._sleep(200_000_000)  # keeps the current stream busy for tens of milliseconds
+    batch = Batch(recipes, "cuda:0", initial_state=seeded)
+    logs = batch.run(capture=lambda i, f, g: together.__setitem__((i, f), g.smoke.data.clone()))
+    torch.cuda.synchronize()
+    assert logs == logs_alone
+    for key, values in alone.items():
+        assert torch.equal(together[key], values), key

@@ -5,6 +5,7 @@ through the reference's own sheet and report code (when the reference is mounted
 import copy
 import hashlib
 import json
+import os
 from pathlib import Path
 
 import numpy as np
@@ -16,6 +17,7 @@ from plume_b200.recipe.load import resolve_table
 from plume_b200.render.camera import make_camera, make_domain_view
 
 GOLDEN = Path(__file__).resolve().parent / "golden"
+REFERENCE = Path(os.environ.get("PLUME_REFERENCE", "/root/reference"))
 DIGESTS = json.loads((GOLDEN / "raw_frame_digests.json").read_text())
 
 
@@ -35,7 +37,7 @@ def test_oracle_reproduces_the_reference_raw_frame_digest(channels):
     assert hashlib.sha256(frame.tobytes()).hexdigest() == DIGESTS["digests"][channels]
 
 
-@pytest.mark.skipif(not Path("/root/reference/src/plume").exists(), reason="the reference is not mounted")
+@pytest.mark.skipif(not (REFERENCE / "src" / "plume").exists(), reason="the reference is not mounted")
 def test_oracle_preview_matches_the_reference_golden_numbers():
     import importlib.util
 

@@ -3,6 +3,7 @@ check, tests/view/test_viewport.py:47-72: within one byte), and its composite is
 (report/composite.py, when the reference is mounted); the product's colour tables are the reference's."""
 
 import itertools
+import os
 from pathlib import Path
 
 import numpy as np
@@ -16,7 +17,7 @@ BYTES = np.arange(0, 256, 15, dtype=np.uint8)
 HEAT_DIVISOR, SHADE_DIVISOR = 7.3, 0.8
 BACKGROUND = "#aac476"
 LIGHT_DIR = (0.5, 0.8, 0.3)
-REFERENCE = Path("/root/reference/src")
+REFERENCE = Path(os.environ.get("PLUME_REFERENCE", "/root/reference")) / "src"
 
 
 def byte_grid(shade: bool) -> np.ndarray:

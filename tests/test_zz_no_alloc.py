@@ -44,7 +44,7 @@ def budget_static(grid, next_field):
     return totals
 
 
-@pytest.mark.parametrize("cells", [(32, 48, 32), (15, 17, 13)])
+@pytest.mark.parametrize("cells", [(32, 48, 32), (15, 17, 13), (1, 1024, 1024)])
 def test_static_budget_matches_the_scratch_budget_on_two_calls_in_a_row(cuda_device, cells):
     for call, seed in enumerate((1, 2)):  # the second call reuses the array the first one left behind
         grid = budget_inputs(cells, seed + sum(cells))
