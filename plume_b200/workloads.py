@@ -19,17 +19,21 @@ DEFAULT_SEED = 20261203
 
 
 def box_filter(field: np.ndarray, passes: int = 3) -> np.ndarray:
-    """`passes` 3x3x3 box-filter passes with edge clamp, in float64."""
+    """`passes` 3x3x3 box-filter passes with edge clamp, in float64. Each pass runs as three 3-tap sums, one
+    per axis (the 27-cell box is their product, edge replication included), then divides by 27."""
     out = field.astype(np.float64)
     for _ in range(passes):
-        padded = np.pad(out, 1, mode="edge")
-        total = np.zeros_like(out)
-        n0, n1, n2 = out.shape
-        for a in range(3):
-            for b in range(3):
-                for c in range(3):
-                    total += padded[a:a + n0, b:b + n1, c:c + n2]
-        out = total / 27.0
+        for axis in range(3):
+            n = out.shape[axis]
+            pad = [(1, 1) if a == axis else (0, 0) for a in range(3)]
+            padded = np.pad(out, pad, mode="edge")
+
+            def window(start):
+                return padded[tuple(slice(start, start + n) if a == axis else slice(None) for a in range(3))]
+
+            out = window(0) + window(1)
+            out += window(2)
+        out /= 27.0
     return out
 
 
@@ -37,17 +41,18 @@ def operator_fields(cells, seed: int = DEFAULT_SEED, ambient_k: float = 1.0) -> 
     nx, ny, nz = cells
     rng = np.random.default_rng(seed)
     fields = {
-        "u": box_filter(rng.uniform(-1.0, 1.0, (nx + 1, ny, nz))),
-        "v": box_filter(rng.uniform(-1.0, 1.0, (nx, ny + 1, nz))),
-        "w": box_filter(rng.uniform(-1.0, 1.0, (nx, ny, nz + 1))),
+        "u": box_filter(rng.uniform(-1.0, 1.0, (nx + 1, ny, nz))).astype(np.float32),
+        "v": box_filter(rng.uniform(-1.0, 1.0, (nx, ny + 1, nz))).astype(np.float32),
+        "w": box_filter(rng.uniform(-1.0, 1.0, (nx, ny, nz + 1))).astype(np.float32),
     }
     smoke = rng.uniform(0.0, 1.0, cells)
-    idx = np.indices(cells).astype(np.float64) + 0.5
+    centre = [np.arange(n, dtype=np.float64) + 0.5 - n / 2.0 for n in cells]
+    dist2 = centre[0][:, None, None] ** 2 + centre[1][None, :, None] ** 2 + centre[2][None, None, :] ** 2
     radius = 40.0 * nx / 128.0
-    inside = sum((idx[a] - cells[a] / 2.0) ** 2 for a in range(3)) <= radius * radius
-    fields["smoke"] = np.where(inside, smoke, 0.0)
-    fields["temperature"] = ambient_k + 0.8 * fields["smoke"]
-    return {name: value.astype(np.float32) for name, value in fields.items()}
+    fields["smoke"] = np.where(dist2 <= radius * radius, smoke, 0.0).astype(np.float32)
+    del smoke, dist2
+    fields["temperature"] = (ambient_k + 0.8 * fields["smoke"].astype(np.float64)).astype(np.float32)
+    return fields
 
 
 def device_operator_fields(cells, seed: int = DEFAULT_SEED, ambient_k: float = 1.0, device: str = "cuda:0") -> dict:

@@ -9,6 +9,8 @@ import sys
 from pathlib import Path
 
 REPO = Path(__file__).resolve().parents[1]
+if str(REPO) not in sys.path:
+    sys.path.insert(0, str(REPO))
 
 
 def run_bench(*args, env=None):
@@ -27,7 +29,14 @@ def test_the_reference_arm_prints_one_line_of_the_contract():
     assert line["higher_is_better"] is True and line["value"] > 0
     assert line["steps"] == 1 and line["n_gpus"] == 1
     assert line["config"]["cells"] == [32, 48, 32]
-    assert line["config"]["workload"].startswith("plain FP32 fluid step 32x48x32 (seeded smoothed velocities")
+    assert line["config"]["workload"].startswith("32x48x32 plain FP32 fluid step, 4 MG V-cycles")
+    assert len(line["config"]["workload"]) <= 128
+    import bench
+    from plume_b200.recipe.derived import derive
+    from plume_b200.workloads import plain_step_recipe
+
+    # the CUDA arm prints the same config for the same workload
+    assert line["config"] == bench.bench_config(derive(plain_step_recipe((32, 48, 32), cycles=4)), 4, 1)
     baseline = line["cpu_baseline"]
     assert baseline["kind"] == "port" and baseline["cores"] >= 1 and baseline["value"] == line["value"]
     assert "whole-grid substeps" in baseline["sample"]
