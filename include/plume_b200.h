@@ -262,6 +262,30 @@ int plume_smoke_budget(const PlumeGridInfo* info, const float* data, const float
 int plume_smoke_budget_static(const PlumeGridInfo* info, const float* data, const float* hat, float* next,
                               double* totals_out, void* stream);
 
+/* No counterpart in the reference. plume_step advects velocity, smoke and temperature with the fused passes
+ * below (the default, enable = 1) or with the two-pass kernels of plume_advect_maccormack (enable = 0), whose
+ * blends keep the reference's a*(1-t) + b*t. A process-wide switch, for comparison and tests. */
+int plume_use_fused_advection(int32_t enable);
+
+/* advect.py:59-68 advect_maccormack of u, v and w by themselves (the step's velocity advection,
+ * stepper.py:46-52), in one fused pass: the forward semi-Lagrangian value is kept in on-chip memory and never
+ * stored, and the limiter's range comes from the same samples. Trilinear blends are fused multiply-adds, so
+ * values agree with the three-pass form to about an ulp. next arrays must not alias the data arrays. */
+int plume_maccormack_velocity(const PlumeGridInfo* info, const float* u, const float* v, const float* w,
+                              float* u_next, float* v_next, float* w_next, float dt_over_cell, void* stream);
+
+/* advect.py:59-68 advect_maccormack of smoke and temperature by (u, v, w) in one fused pass (they share every
+ * trace), with the smoke budget's line sums (reduce.py:12-25) of data, hat and next taken on the way:
+ * `scratch` needs plume_maccormack_scratch_floats(info) floats and `sums` plume_smoke_scratch_doubles(info)
+ * doubles; if `totals_out` is not null, the three totals (before, semi-Lagrangian, MacCormack; 3 doubles on the
+ * device) are written there. Values beyond open faces are smoke_outside and heat_outside when uses_outside is
+ * 1 (sample.py:64-71). next is not rescaled: plume_step applies the held factor afterwards. */
+long long plume_maccormack_scratch_floats(const PlumeGridInfo* info);
+int plume_maccormack_scalars(const PlumeGridInfo* info, const float* u, const float* v, const float* w,
+                             const float* smoke, const float* temperature, float* smoke_next, float* temperature_next,
+                             float dt_over_cell, float smoke_outside, float heat_outside, int32_t uses_outside,
+                             float* scratch, double* sums, double* totals_out, void* stream);
+
 /* reduce.py:28-38 TripleSum: the three totals (device, 3 doubles) without scaling. */
 int plume_triple_sum(const int32_t shape[3], const float* a, const float* b, const float* c, double* sums,
                      double* totals_out, void* stream);

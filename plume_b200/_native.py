@@ -121,6 +121,10 @@ SIGNATURES = {
     "plume_advect_scratch_floats": [_INFO],
     "plume_smoke_budget": [_INFO, _P, _P, _P, _P, _P, _P, _P],
     "plume_triple_sum": [_SHAPE, _P, _P, _P, _P, _P, _P],
+    "plume_use_fused_advection": [_I],
+    "plume_maccormack_scratch_floats": [_INFO],
+    "plume_maccormack_velocity": [_INFO, _P, _P, _P, _P, _P, _P, _F, _P],
+    "plume_maccormack_scalars": [_INFO, _P, _P, _P, _P, _P, _P, _P, _F, _F, _F, _I, _P, _P, _P, _P],
     "plume_smoke_budget_static": [_INFO, _P, _P, _P, _P, _P],
     "plume_dissipate": [_INFO, _P, _P, _F, _F, _F, _P],
     "plume_grid_speed": [_INFO, _P, _P, _P, _I, _P, _P],
@@ -173,7 +177,8 @@ def lib() -> ctypes.CDLL:
         for name, argtypes in SIGNATURES.items():
             fn = getattr(loaded, name)
             fn.argtypes = argtypes
-            wide = name in ("plume_advect_scratch_floats", "plume_brick_floats", "plume_norm_scratch_doubles")
+            wide = name in ("plume_advect_scratch_floats", "plume_brick_floats", "plume_norm_scratch_doubles",
+                            "plume_maccormack_scratch_floats")
             fn.restype = ctypes.c_longlong if wide else ctypes.c_int
         _lib = loaded
     return _lib

@@ -10,8 +10,10 @@
 #include <cstring>
 #include <mutex>
 #include <string>
+#include <type_traits>
 #include <vector>
 
+#include "advect.cuh"
 #include "poisson.cuh"
 
 namespace plume {
@@ -203,21 +205,75 @@ static int launch_emit(const PlumeGridInfo& info, T* smoke, T* temperature, T* u
   return PLUME_OK;
 }
 
+// ---- streaming kernels: several x-planes per thread -----------------------------------------------------
+// The one-pass stencil kernels of the step (buoyancy, curl, push, face forces, divergence, gradient) handle
+// PLANES x-planes per thread with every load issued before any store, so more bytes are in flight per SM than
+// with one element per thread. Each element's arithmetic is unchanged. PLUME_STREAM_PLANES = 1, 2 or 4
+// (default 4) selects the count.
+static int stream_planes() {
+  static const int n = [] {
+    const char* v = getenv("PLUME_STREAM_PLANES");
+    const int p = v ? atoi(v) : 4;
+    return p == 1 || p == 2 ? p : 4;
+  }();
+  return n;
+}
+
+// Calls f(std::integral_constant<int, P>) with P the streaming kernels' planes per thread.
+template <class F>
+static int with_planes(F f) {
+  switch (stream_planes()) {
+    case 1: return f(std::integral_constant<int, 1>{});
+    case 2: return f(std::integral_constant<int, 2>{});
+    default: return f(std::integral_constant<int, 4>{});
+  }
+}
+
+static dim3 cell_grid_planes(int n0, int n1, int n2, int planes) {
+  return dim3((n2 + TZ - 1) / TZ, (n1 + TY - 1) / TY, (n0 + planes - 1) / planes);
+}
+
 // ---- buoyancy: forces.py:13-23 -----------------------------------------------------------------------------
-template <class T>
+template <class T, int PLANES>
 __global__ void k_buoyancy(PlumeGridInfo info, T* __restrict__ v, const T* __restrict__ smoke,
                            const T* __restrict__ temperature, float gravity, float heat_buoyancy, float smoke_weight,
                            float ambient, float dt) {
-  const int ny = info.dims[1], nz = info.dims[2];
-  const int i = blockIdx.z, j = blockIdx.y * blockDim.y + threadIdx.y, k = blockIdx.x * blockDim.x + threadIdx.x;
+  const int nx = info.dims[0], ny = info.dims[1], nz = info.dims[2];
+  const int i0 = blockIdx.z * PLANES, j = blockIdx.y * blockDim.y + threadIdx.y, k = blockIdx.x * blockDim.x + threadIdx.x;
   if (j > ny || k >= nz) return;
   const int below = imax_(j - 1, 0), above = imin_(j, ny - 1);
-  const int cb = (i * ny + below) * nz + k, ca = (i * ny + above) * nz + k;
-  float heat = 0.5f * (ldg_f(temperature + cb) + ldg_f(temperature + ca));
-  float density = 0.5f * (ldg_f(smoke + cb) + ldg_f(smoke + ca));
-  float lift = heat_buoyancy * (heat - ambient) / ambient - smoke_weight * density;
-  const int c = (i * (ny + 1) + j) * nz + k;
-  st_f(v + c, ld_f(v + c) + gravity * lift * dt);
+  const long cell_plane = (long)ny * nz, face_plane = (long)(ny + 1) * nz;
+  float tb[PLANES], ta[PLANES], sb[PLANES], sa[PLANES], vv[PLANES];
+#pragma unroll
+  for (int p = 0; p < PLANES; ++p) {
+    if (i0 + p >= nx) break;
+    const long cb = (i0 + p) * cell_plane + below * nz + k, ca = (i0 + p) * cell_plane + above * nz + k;
+    tb[p] = ldg_f(temperature + cb);
+    ta[p] = ldg_f(temperature + ca);
+    sb[p] = ldg_f(smoke + cb);
+    sa[p] = ldg_f(smoke + ca);
+    vv[p] = ld_f(v + (i0 + p) * face_plane + (long)j * nz + k);
+  }
+#pragma unroll
+  for (int p = 0; p < PLANES; ++p) {
+    if (i0 + p >= nx) break;
+    float heat = 0.5f * (tb[p] + ta[p]);
+    float density = 0.5f * (sb[p] + sa[p]);
+    float lift = heat_buoyancy * (heat - ambient) / ambient - smoke_weight * density;
+    st_f(v + (i0 + p) * face_plane + (long)j * nz + k, vv[p] + gravity * lift * dt);
+  }
+}
+
+template <class T>
+static int launch_buoyancy(const PlumeGridInfo& info, T* v, const T* smoke, const T* temperature, float gravity,
+                           float heat_buoyancy, float smoke_weight, float ambient, float dt, cudaStream_t st) {
+  const int nx = info.dims[0], ny = info.dims[1], nz = info.dims[2];
+  return with_planes([&](auto P) {
+    constexpr int PL = decltype(P)::value;
+    k_buoyancy<T, PL><<<cell_grid_planes(nx, ny + 1, nz, PL), cell_block(), 0, st>>>(
+        info, v, smoke, temperature, gravity, heat_buoyancy, smoke_weight, ambient, dt);
+    return launch_status("buoyancy");
+  });
 }
 
 // ---- vorticity confinement: vorticity.py:17-84 -------------------------------------------------------------
@@ -230,11 +286,9 @@ __device__ __forceinline__ F3 center_velocity(const VelT<T>& vel, int i, int j, 
 
 // curl_kernel (vorticity.py:38-45) with the centre velocities of center_velocity_kernel computed in place.
 template <class T>
-__global__ void k_curl(PlumeGridInfo info, VelT<T> vel, float* __restrict__ cx, float* __restrict__ cy,
-                       float* __restrict__ cz) {
+__device__ __forceinline__ void curl_at(const PlumeGridInfo& info, const VelT<T>& vel, float* __restrict__ cx,
+                                        float* __restrict__ cy, float* __restrict__ cz, int i, int j, int k) {
   const int nx = info.dims[0], ny = info.dims[1], nz = info.dims[2];
-  const int i = blockIdx.z, j = blockIdx.y * blockDim.y + threadIdx.y, k = blockIdx.x * blockDim.x + threadIdx.x;
-  if (j >= ny || k >= nz) return;
   const int cell[3] = {i, j, k};
   const int n[3] = {nx, ny, nz};
   F3 d[3];
@@ -257,18 +311,28 @@ __global__ void k_curl(PlumeGridInfo info, VelT<T> vel, float* __restrict__ cx, 
   cz[c] = d[0][1] - d[1][0];
 }
 
+template <class T, int PLANES>
+__global__ void k_curl(PlumeGridInfo info, VelT<T> vel, float* __restrict__ cx, float* __restrict__ cy,
+                       float* __restrict__ cz) {
+  const int nx = info.dims[0], ny = info.dims[1], nz = info.dims[2];
+  const int i0 = blockIdx.z * PLANES, j = blockIdx.y * blockDim.y + threadIdx.y, k = blockIdx.x * blockDim.x + threadIdx.x;
+  if (j >= ny || k >= nz) return;
+#pragma unroll
+  for (int p = 0; p < PLANES; ++p)
+    if (i0 + p < nx) curl_at(info, vel, cx, cy, cz, i0 + p, j, k);
+}
+
 __device__ __forceinline__ F3 load3(const float* __restrict__ x, const float* __restrict__ y,
                                     const float* __restrict__ z, int c) {
   return f3(__ldg(x + c), __ldg(y + c), __ldg(z + c));
 }
 
 // confinement_push_kernel (vorticity.py:53-71).
-__global__ void k_push(PlumeGridInfo info, const float* __restrict__ cx, const float* __restrict__ cy,
-                       const float* __restrict__ cz, float* __restrict__ px, float* __restrict__ py,
-                       float* __restrict__ pz, float strength) {
+__device__ __forceinline__ void push_at(const PlumeGridInfo& info, const float* __restrict__ cx,
+                                        const float* __restrict__ cy, const float* __restrict__ cz,
+                                        float* __restrict__ px, float* __restrict__ py, float* __restrict__ pz,
+                                        float strength, int i, int j, int k) {
   const int nx = info.dims[0], ny = info.dims[1], nz = info.dims[2];
-  const int i = blockIdx.z, j = blockIdx.y * blockDim.y + threadIdx.y, k = blockIdx.x * blockDim.x + threadIdx.x;
-  if (j >= ny || k >= nz) return;
   const Dims d{nx, ny, nz};
   const int cell[3] = {i, j, k};
   const int n[3] = {nx, ny, nz};
@@ -299,6 +363,18 @@ __global__ void k_push(PlumeGridInfo info, const float* __restrict__ cx, const f
   pz[c] = push[2];
 }
 
+template <int PLANES>
+__global__ void k_push(PlumeGridInfo info, const float* __restrict__ cx, const float* __restrict__ cy,
+                       const float* __restrict__ cz, float* __restrict__ px, float* __restrict__ py,
+                       float* __restrict__ pz, float strength) {
+  const int nx = info.dims[0], ny = info.dims[1], nz = info.dims[2];
+  const int i0 = blockIdx.z * PLANES, j = blockIdx.y * blockDim.y + threadIdx.y, k = blockIdx.x * blockDim.x + threadIdx.x;
+  if (j >= ny || k >= nz) return;
+#pragma unroll
+  for (int p = 0; p < PLANES; ++p)
+    if (i0 + p < nx) push_at(info, cx, cy, cz, px, py, pz, strength, i0 + p, j, k);
+}
+
 // ---- turbulence: turbulence.py:26-53 -----------------------------------------------------------------------
 constexpr int TURBULENCE_STREAM = 1 << 24;
 
@@ -323,12 +399,10 @@ struct FaceForces {
 
 // One pass over the three face arrays applying, per face and in the reference's order, the confinement push,
 // the turbulence push and drag. blockIdx.z segments: nx+1 u slices, nx v slices, nx w slices.
-template <int AXIS, class T>
-__device__ __forceinline__ void face_forces_at(const PlumeGridInfo& info, T* __restrict__ f, int i, int j, int k,
-                                               int n1, int n2, const FaceForces& ff) {
+template <int AXIS>
+__device__ __forceinline__ float face_forces_value(const PlumeGridInfo& info, float value, int i, int j, int k,
+                                                   const FaceForces& ff) {
   const int nx = info.dims[0], ny = info.dims[1], nz = info.dims[2];
-  const int c = (i * n1 + j) * n2 + k;
-  float value = ld_f(f + c);
   if (ff.confinement) {
     const int index = AXIS == 0 ? i : (AXIS == 1 ? j : k);
     const int lo = imax_(index - 1, 0), hi = imin_(index, info.dims[AXIS] - 1);
@@ -354,27 +428,68 @@ __device__ __forceinline__ void face_forces_at(const PlumeGridInfo& info, T* __r
     value = value + ff.strength * curl * ff.dt;
   }
   if (ff.drag) value = ff.wind[AXIS] + (value - ff.wind[AXIS]) * ff.keep;
-  st_f(f + c, value);
+  return value;
+}
+
+// The face kernels' blockIdx.z: groups of PLANES x-planes of u (nx + 1 planes), then of v, then of w.
+template <int PLANES>
+__device__ __forceinline__ void face_planes(const PlumeGridInfo& info, int& axis, int& i0) {
+  const int nx = info.dims[0];
+  const int gu = (nx + 1 + PLANES - 1) / PLANES, gv = (nx + PLANES - 1) / PLANES;
+  int z = blockIdx.z;
+  axis = 0;
+  if (z >= gu) {
+    z -= gu;
+    axis = 1;
+    if (z >= gv) {
+      z -= gv;
+      axis = 2;
+    }
+  }
+  i0 = z * PLANES;
+}
+
+static dim3 face_grid(const PlumeGridInfo& info, int planes) {
+  const int nx = info.dims[0], ny = info.dims[1], nz = info.dims[2];
+  return dim3((nz + 1 + TZ - 1) / TZ, (ny + 1 + TY - 1) / TY,
+              (nx + 1 + planes - 1) / planes + 2 * ((nx + planes - 1) / planes));
+}
+
+// confinement push, turbulence and drag on PLANES faces per thread, every face loaded before any is stored
+template <int AXIS, int PLANES, class T>
+__device__ __forceinline__ void face_forces_planes(const PlumeGridInfo& info, T* __restrict__ f, int i0, int j, int k,
+                                                   const FaceForces& ff) {
+  const Dims d = {info.dims[0] + (AXIS == 0), info.dims[1] + (AXIS == 1), info.dims[2] + (AXIS == 2)};
+  if (j >= d.n1 || k >= d.n2) return;
+  const long plane = (long)d.n1 * d.n2, at_jk = (long)j * d.n2 + k;
+  float value[PLANES];
+#pragma unroll
+  for (int p = 0; p < PLANES; ++p)
+    if (i0 + p < d.n0) value[p] = ld_f(f + (i0 + p) * plane + at_jk);
+#pragma unroll
+  for (int p = 0; p < PLANES; ++p)
+    if (i0 + p < d.n0) st_f(f + (i0 + p) * plane + at_jk, face_forces_value<AXIS>(info, value[p], i0 + p, j, k, ff));
+}
+
+template <class T, int PLANES>
+__global__ void k_face_forces(PlumeGridInfo info, T* __restrict__ u, T* __restrict__ v, T* __restrict__ w,
+                              FaceForces ff) {
+  int axis, i0;
+  face_planes<PLANES>(info, axis, i0);
+  const int j = blockIdx.y * blockDim.y + threadIdx.y, k = blockIdx.x * blockDim.x + threadIdx.x;
+  if (axis == 0) face_forces_planes<0, PLANES>(info, u, i0, j, k, ff);
+  else if (axis == 1) face_forces_planes<1, PLANES>(info, v, i0, j, k, ff);
+  else face_forces_planes<2, PLANES>(info, w, i0, j, k, ff);
 }
 
 template <class T>
-__global__ void k_face_forces(PlumeGridInfo info, T* __restrict__ u, T* __restrict__ v, T* __restrict__ w,
-                              FaceForces ff) {
-  const int nx = info.dims[0], ny = info.dims[1], nz = info.dims[2];
-  int slab = blockIdx.z, axis = 0;
-  if (slab >= nx + 1) { slab -= nx + 1; axis = 1; }
-  if (axis == 1 && slab >= nx) { slab -= nx; axis = 2; }
-  const int i = slab, j = blockIdx.y * blockDim.y + threadIdx.y, k = blockIdx.x * blockDim.x + threadIdx.x;
-  const int n1 = ny + (axis == 1), n2 = nz + (axis == 2);
-  if (j >= n1 || k >= n2) return;
-  if (axis == 0) face_forces_at<0>(info, u, i, j, k, n1, n2, ff);
-  else if (axis == 1) face_forces_at<1>(info, v, i, j, k, n1, n2, ff);
-  else face_forces_at<2>(info, w, i, j, k, n1, n2, ff);
-}
-
-static dim3 face_grid(const PlumeGridInfo& info) {
-  const int nx = info.dims[0], ny = info.dims[1], nz = info.dims[2];
-  return dim3((nz + 1 + TZ - 1) / TZ, (ny + 1 + TY - 1) / TY, (nx + 1) + nx + nx);
+static int launch_face_forces(const PlumeGridInfo& info, T* u, T* v, T* w, const FaceForces& ff, const char* what,
+                              cudaStream_t st) {
+  return with_planes([&](auto P) {
+    constexpr int PL = decltype(P)::value;
+    k_face_forces<T, PL><<<face_grid(info, PL), cell_block(), 0, st>>>(info, u, v, w, ff);
+    return launch_status(what);
+  });
 }
 
 template <class T>
@@ -383,13 +498,15 @@ static int launch_confinement_push(const PlumeGridInfo& info, const T* u, const 
                                    cudaStream_t st) {
   const int nx = info.dims[0], ny = info.dims[1], nz = info.dims[2];
   VelT<T> vel = make_vel(u, v, w, info.dims);
-  k_curl<<<cell_grid(nx, ny, nz), cell_block(), 0, st>>>(info, vel, curl[0], curl[1], curl[2]);
-  CHECK_LAUNCH("curl");
-  if (!apply) return PLUME_OK;
-  k_push<<<cell_grid(nx, ny, nz), cell_block(), 0, st>>>(info, curl[0], curl[1], curl[2], push[0], push[1], push[2],
-                                                         strength);
-  CHECK_LAUNCH("confinement push");
-  return PLUME_OK;
+  return with_planes([&](auto P) {
+    constexpr int PL = decltype(P)::value;
+    k_curl<T, PL><<<cell_grid_planes(nx, ny, nz, PL), cell_block(), 0, st>>>(info, vel, curl[0], curl[1], curl[2]);
+    CHECK_LAUNCH("curl");
+    if (!apply) return PLUME_OK;
+    k_push<PL><<<cell_grid_planes(nx, ny, nz, PL), cell_block(), 0, st>>>(info, curl[0], curl[1], curl[2], push[0],
+                                                                          push[1], push[2], strength);
+    return launch_status("confinement push");
+  });
 }
 
 // ---- advection: advect.py -----------------------------------------------------------------------------------
@@ -677,53 +794,93 @@ __global__ void k_zero_walls(PlumeGridInfo info, T* __restrict__ u, T* __restric
   }
 }
 
-template <class T>
+template <class T, int PLANES>
 __global__ void k_divergence(PlumeGridInfo info, const T* __restrict__ u, const T* __restrict__ v,
                              const T* __restrict__ w, float* __restrict__ div) {  // pressure.py:31-36
-  const int ny = info.dims[1], nz = info.dims[2];
-  const int i = blockIdx.z, j = blockIdx.y * blockDim.y + threadIdx.y, k = blockIdx.x * blockDim.x + threadIdx.x;
+  const int nx = info.dims[0], ny = info.dims[1], nz = info.dims[2];
+  const int i0 = blockIdx.z * PLANES, j = blockIdx.y * blockDim.y + threadIdx.y, k = blockIdx.x * blockDim.x + threadIdx.x;
   if (j >= ny || k >= nz) return;
-  float flux = (ldg_f(u + ((i + 1) * ny + j) * nz + k) - ldg_f(u + (i * ny + j) * nz + k)) +
-               (ldg_f(v + (i * (ny + 1) + j + 1) * nz + k) - ldg_f(v + (i * (ny + 1) + j) * nz + k)) +
-               (ldg_f(w + (i * ny + j) * (nz + 1) + k + 1) - ldg_f(w + (i * ny + j) * (nz + 1) + k));
-  div[(i * ny + j) * nz + k] = flux / info.cell_m;
+#pragma unroll
+  for (int p = 0; p < PLANES; ++p) {
+    const int i = i0 + p;
+    if (i >= nx) break;
+    float flux = (ldg_f(u + ((i + 1) * ny + j) * nz + k) - ldg_f(u + (i * ny + j) * nz + k)) +
+                 (ldg_f(v + (i * (ny + 1) + j + 1) * nz + k) - ldg_f(v + (i * (ny + 1) + j) * nz + k)) +
+                 (ldg_f(w + (i * ny + j) * (nz + 1) + k + 1) - ldg_f(w + (i * ny + j) * (nz + 1) + k));
+    div[(i * ny + j) * nz + k] = flux / info.cell_m;
+  }
 }
 
 // subtract_gradient_kernel (pressure.py:95-116) over the three face arrays (blockIdx.z segments).
-template <int AXIS, class T>
-__device__ __forceinline__ void subtract_gradient_at(const PlumeGridInfo& info, T* __restrict__ f,
-                                                     const float* __restrict__ q, int i, int j, int k, int n1, int n2) {
+// The face's pressure difference (q_above - q_below); false for a closed wall face, which is left alone.
+template <int AXIS>
+__device__ __forceinline__ bool gradient_at(const PlumeGridInfo& info, const float* __restrict__ q, int i, int j, int k,
+                                            float& q_above, float& q_below) {
   const Dims d = dims_of(info);
   const int index = AXIS == 0 ? i : (AXIS == 1 ? j : k);
   const int below = AXIS == 0 ? at(d, i - 1, j, k) : (AXIS == 1 ? at(d, i, j - 1, k) : at(d, i, j, k - 1));
-  float q_above = 0.0f, q_below = 0.0f;
+  q_above = 0.0f;
+  q_below = 0.0f;
   if (index == 0) {
-    if (info.open_lo[AXIS] == 0) return;
+    if (info.open_lo[AXIS] == 0) return false;
     q_above = __ldg(q + at(d, i, j, k));
   } else if (index == info.dims[AXIS]) {
-    if (info.open_hi[AXIS] == 0) return;
+    if (info.open_hi[AXIS] == 0) return false;
     q_below = __ldg(q + below);
   } else {
     q_above = __ldg(q + at(d, i, j, k));
     q_below = __ldg(q + below);
   }
-  const int c = (i * n1 + j) * n2 + k;
-  st_f(f + c, ld_f(f + c) - (q_above - q_below) / info.cell_m);
+  return true;
+}
+
+template <int AXIS, int PLANES, class T>
+__device__ __forceinline__ void subtract_gradient_planes(const PlumeGridInfo& info, T* __restrict__ f,
+                                                         const float* __restrict__ q, int i0, int j, int k) {
+  const Dims d = {info.dims[0] + (AXIS == 0), info.dims[1] + (AXIS == 1), info.dims[2] + (AXIS == 2)};
+  if (j >= d.n1 || k >= d.n2) return;
+  const long plane = (long)d.n1 * d.n2, at_jk = (long)j * d.n2 + k;
+  float value[PLANES], above[PLANES], below[PLANES];
+  bool apply[PLANES];
+#pragma unroll
+  for (int p = 0; p < PLANES; ++p) {
+    apply[p] = i0 + p < d.n0 && gradient_at<AXIS>(info, q, i0 + p, j, k, above[p], below[p]);
+    if (apply[p]) value[p] = ld_f(f + (i0 + p) * plane + at_jk);
+  }
+#pragma unroll
+  for (int p = 0; p < PLANES; ++p)
+    if (apply[p]) st_f(f + (i0 + p) * plane + at_jk, value[p] - (above[p] - below[p]) / info.cell_m);
+}
+
+template <class T, int PLANES>
+__global__ void k_subtract_gradient(PlumeGridInfo info, T* __restrict__ u, T* __restrict__ v, T* __restrict__ w,
+                                    const float* __restrict__ q) {
+  int axis, i0;
+  face_planes<PLANES>(info, axis, i0);
+  const int j = blockIdx.y * blockDim.y + threadIdx.y, k = blockIdx.x * blockDim.x + threadIdx.x;
+  if (axis == 0) subtract_gradient_planes<0, PLANES>(info, u, q, i0, j, k);
+  else if (axis == 1) subtract_gradient_planes<1, PLANES>(info, v, q, i0, j, k);
+  else subtract_gradient_planes<2, PLANES>(info, w, q, i0, j, k);
 }
 
 template <class T>
-__global__ void k_subtract_gradient(PlumeGridInfo info, T* __restrict__ u, T* __restrict__ v, T* __restrict__ w,
-                                    const float* __restrict__ q) {
-  const int nx = info.dims[0], ny = info.dims[1], nz = info.dims[2];
-  int slab = blockIdx.z, axis = 0;
-  if (slab >= nx + 1) { slab -= nx + 1; axis = 1; }
-  if (axis == 1 && slab >= nx) { slab -= nx; axis = 2; }
-  const int i = slab, j = blockIdx.y * blockDim.y + threadIdx.y, k = blockIdx.x * blockDim.x + threadIdx.x;
-  const int n1 = ny + (axis == 1), n2 = nz + (axis == 2);
-  if (j >= n1 || k >= n2) return;
-  if (axis == 0) subtract_gradient_at<0>(info, u, q, i, j, k, n1, n2);
-  else if (axis == 1) subtract_gradient_at<1>(info, v, q, i, j, k, n1, n2);
-  else subtract_gradient_at<2>(info, w, q, i, j, k, n1, n2);
+static int launch_divergence(const PlumeGridInfo& info, const T* u, const T* v, const T* w, float* div,
+                             cudaStream_t st) {
+  return with_planes([&](auto P) {
+    constexpr int PL = decltype(P)::value;
+    k_divergence<T, PL><<<cell_grid_planes(info.dims[0], info.dims[1], info.dims[2], PL), cell_block(), 0, st>>>(
+        info, u, v, w, div);
+    return launch_status("divergence");
+  });
+}
+
+template <class T>
+static int launch_subtract_gradient(const PlumeGridInfo& info, T* u, T* v, T* w, const float* q, cudaStream_t st) {
+  return with_planes([&](auto P) {
+    constexpr int PL = decltype(P)::value;
+    k_subtract_gradient<T, PL><<<face_grid(info, PL), cell_block(), 0, st>>>(info, u, v, w, q);
+    return launch_status("subtract gradient");
+  });
 }
 
 // ---- residual (multigrid.py:36-43), for callers that inspect it ---------------------------------------------
@@ -903,6 +1060,10 @@ static int launch_triple_sum(const Dims& d, const T* a, const T* b, const T* c, 
   return PLUME_OK;
 }
 
+// plume_step advects with the fused march (advect.cu) unless plume_use_fused_advection(0) selected the
+// two-pass kernels (hat and the clamp ranges through global memory, the reference's blend arithmetic).
+static bool g_fused_advection = true;
+
 static int grid_stride_blocks(long n) {
   long b = (n + 255) / 256;
   return (int)std::min<long>(b, 148L * 16);
@@ -920,7 +1081,7 @@ __global__ void k_scalar_finish(T* __restrict__ smoke, T* __restrict__ temperatu
     float value = to_f<T>(from_f<T>(ld_f(smoke + idx) * s));
     if (dissipate) {
       value = value * smoke_keep;
-      st_f(temperature + idx, ambient + (ld_f(temperature + idx) - ambient) * heat_keep);
+      if (temperature) st_f(temperature + idx, ambient + (ld_f(temperature + idx) - ambient) * heat_keep);
     }
     st_f(smoke + idx, value);
   }
@@ -999,10 +1160,8 @@ extern "C" int plume_buoyancy(const PlumeGridInfo* info, float* v, const float* 
                               void* stream) {
   CHECK_ARG(info && v && smoke && temperature, "buoyancy: null argument");
   CHECK_ARG(valid_dims(info->dims), "buoyancy: bad dims");
-  const int nx = info->dims[0], ny = info->dims[1], nz = info->dims[2];
-  k_buoyancy<<<cell_grid(nx, ny + 1, nz), cell_block(), 0, as_stream(stream)>>>(
-      *info, v, smoke, temperature, gravity, heat_buoyancy, smoke_weight, ambient_k, dt);
-  return launch_status("buoyancy");
+  return launch_buoyancy<float>(*info, v, smoke, temperature, gravity, heat_buoyancy, smoke_weight, ambient_k, dt,
+                                as_stream(stream));
 }
 
 extern "C" int plume_drag(const PlumeGridInfo* info, float* u, float* v, float* w, const float wind[3], float keep,
@@ -1015,8 +1174,7 @@ extern "C" int plume_drag(const PlumeGridInfo* info, float* u, float* v, float* 
   ff.wind[1] = wind[1];
   ff.wind[2] = wind[2];
   ff.keep = keep;
-  k_face_forces<<<face_grid(*info), cell_block(), 0, as_stream(stream)>>>(*info, u, v, w, ff);
-  return launch_status("drag");
+  return launch_face_forces<float>(*info, u, v, w, ff, "drag", as_stream(stream));
 }
 
 extern "C" int plume_confinement(const PlumeGridInfo* info, float* u, float* v, float* w, float* curl_xyz[3],
@@ -1033,8 +1191,7 @@ extern "C" int plume_confinement(const PlumeGridInfo* info, float* u, float* v, 
   ff.push[1] = push_xyz[1];
   ff.push[2] = push_xyz[2];
   ff.dt = dt;
-  k_face_forces<<<face_grid(*info), cell_block(), 0, st>>>(*info, u, v, w, ff);
-  return launch_status("add face push");
+  return launch_face_forces<float>(*info, u, v, w, ff, "add face push", st);
 }
 
 extern "C" int plume_turbulence(const PlumeGridInfo* info, float* u, float* v, float* w, int32_t seed, float scale_m,
@@ -1048,17 +1205,14 @@ extern "C" int plume_turbulence(const PlumeGridInfo* info, float* u, float* v, f
   ff.strength = strength;
   ff.pattern_time = pattern_time;
   ff.dt = dt;
-  k_face_forces<<<face_grid(*info), cell_block(), 0, as_stream(stream)>>>(*info, u, v, w, ff);
-  return launch_status("turbulence");
+  return launch_face_forces<float>(*info, u, v, w, ff, "turbulence", as_stream(stream));
 }
 
 extern "C" int plume_divergence(const PlumeGridInfo* info, const float* u, const float* v, const float* w,
                                 float* divergence, void* stream) {
   CHECK_ARG(info && u && v && w && divergence, "divergence: null argument");
   CHECK_ARG(valid_dims(info->dims), "divergence: bad dims");
-  const int nx = info->dims[0], ny = info->dims[1], nz = info->dims[2];
-  k_divergence<<<cell_grid(nx, ny, nz), cell_block(), 0, as_stream(stream)>>>(*info, u, v, w, divergence);
-  return launch_status("divergence");
+  return launch_divergence<float>(*info, u, v, w, divergence, as_stream(stream));
 }
 
 namespace plume {
@@ -1069,8 +1223,7 @@ static int project_begin(const PlumeGridInfo& info, T* u, T* v, T* w, float* div
   const int m = std::max(nx, ny) + 1, n = std::max(ny, nz) + 1;
   k_zero_walls<T><<<dim3((n + TZ - 1) / TZ, (m + TY - 1) / TY, 6), cell_block(), 0, st>>>(info, u, v, w);
   CHECK_LAUNCH("zero closed faces");
-  k_divergence<T><<<cell_grid(nx, ny, nz), cell_block(), 0, st>>>(info, u, v, w, divergence);
-  return launch_status("divergence");
+  return launch_divergence<T>(info, u, v, w, divergence, st);
 }
 }  // namespace plume
 
@@ -1085,8 +1238,7 @@ extern "C" int plume_subtract_gradient(const PlumeGridInfo* info, float* u, floa
                                        void* stream) {
   CHECK_ARG(info && u && v && w && q, "subtract_gradient: null argument");
   CHECK_ARG(valid_dims(info->dims), "subtract_gradient: bad dims");
-  k_subtract_gradient<<<face_grid(*info), cell_block(), 0, as_stream(stream)>>>(*info, u, v, w, q);
-  return launch_status("subtract gradient");
+  return launch_subtract_gradient<float>(*info, u, v, w, q, as_stream(stream));
 }
 
 extern "C" int plume_red_black_sweeps(const PlumeGridInfo* info, float* q, float* scratch, const float* rhs,
@@ -1181,6 +1333,43 @@ extern "C" int plume_smoke_budget(const PlumeGridInfo* info, const float* data, 
   return launch_status("smoke budget scale");
 }
 
+extern "C" int plume_use_fused_advection(int32_t enable) {
+  g_fused_advection = enable != 0;
+  return PLUME_OK;
+}
+
+extern "C" long long plume_maccormack_scratch_floats(const PlumeGridInfo* info) {
+  if (!info || !valid_dims(info->dims)) return fail(PLUME_ERR_INVALID, "maccormack_scratch_floats: bad dims");
+  return mac_partial_floats(*info);
+}
+
+extern "C" int plume_maccormack_velocity(const PlumeGridInfo* info, const float* u, const float* v, const float* w,
+                                         float* u_next, float* v_next, float* w_next, float dt_over_cell,
+                                         void* stream) {
+  CHECK_ARG(info && u && v && w && u_next && v_next && w_next, "maccormack_velocity: null argument");
+  CHECK_ARG(valid_dims(info->dims), "maccormack_velocity: bad dims");
+  CHECK_ARG(u_next != u && v_next != v && w_next != w, "maccormack_velocity: next must not alias data");
+  return launch_mac_velocity<float>(*info, u, v, w, u_next, v_next, w_next, dt_over_cell, as_stream(stream));
+}
+
+extern "C" int plume_maccormack_scalars(const PlumeGridInfo* info, const float* u, const float* v, const float* w,
+                                        const float* smoke, const float* temperature, float* smoke_next,
+                                        float* temperature_next, float dt_over_cell, float smoke_outside,
+                                        float heat_outside, int32_t uses_outside, float* scratch, double* sums,
+                                        double* totals_out, void* stream) {
+  CHECK_ARG(info && u && v && w && smoke && temperature && smoke_next && temperature_next && scratch && sums,
+            "maccormack_scalars: null argument");
+  CHECK_ARG(valid_dims(info->dims), "maccormack_scalars: bad dims");
+  CHECK_ARG(smoke_next != smoke && temperature_next != temperature, "maccormack_scalars: next must not alias data");
+  cudaStream_t st = as_stream(stream);
+  int status = launch_mac_scalars<float>(*info, u, v, w, smoke, temperature, smoke_next, temperature_next,
+                                         smoke_outside, heat_outside, uses_outside, scratch, sums, 0, 1.0f, 0.0f,
+                                         dt_over_cell, st);
+  if (status != PLUME_OK || !totals_out) return status;
+  k_budget_factor<<<1, dim3(32, 3), 0, st>>>(sums, sum_blocks(dims_of(*info)), nullptr, totals_out, 0);
+  return launch_status("maccormack_scalars: totals");
+}
+
 extern "C" int plume_dissipate(const PlumeGridInfo* info, float* smoke, float* temperature, float smoke_keep,
                                float heat_keep, float ambient_k, void* stream) {
   CHECK_ARG(info && smoke && temperature, "dissipate: null argument");
@@ -1243,9 +1432,9 @@ static int step(const PlumeStepState* s, const PlumeStepParams* p, void* stream)
   if ((status = launch_emit<T>(info, sd, td, ud, vd, wd, p->emitters, p->emitter_count, p->seed, p->time_s, p->dt,
                                st)) != PLUME_OK)
     return status;
-  k_buoyancy<T><<<cell_grid(nx, ny + 1, nz), cell_block(), 0, st>>>(info, vd, sd, td, p->gravity, p->heat_buoyancy,
-                                                                    p->smoke_weight, p->ambient_k, p->dt);
-  CHECK_LAUNCH("buoyancy");
+  if ((status = launch_buoyancy<T>(info, vd, sd, td, p->gravity, p->heat_buoyancy, p->smoke_weight, p->ambient_k, p->dt,
+                                   st)) != PLUME_OK)
+    return status;
   // confinement, turbulence, drag (stepper.py:35-40): one face pass after the push is known
   FaceForces ff{};
   ff.dt = p->dt;
@@ -1274,12 +1463,15 @@ static int step(const PlumeStepState* s, const PlumeStepParams* p, void* stream)
     ff.keep = p->drag_keep;
   }
   if (ff.confinement || ff.turbulence || ff.drag) {
-    k_face_forces<T><<<face_grid(info), cell_block(), 0, st>>>(info, ud, vd, wd, ff);
-    CHECK_LAUNCH("face forces");
+    if ((status = launch_face_forces<T>(info, ud, vd, wd, ff, "face forces", st)) != PLUME_OK) return status;
   }
   if ((status = mark()) != PLUME_OK) return status;
   // advect velocity (stepper.py:46-52)
-  {
+  if (s->advect_scratch && g_fused_advection) {
+    if ((status = launch_mac_velocity<T>(info, ud, vd, wd, static_cast<T*>(s->u.next), static_cast<T*>(s->v.next),
+                                         static_cast<T*>(s->w.next), p->dt_over_cell, st)) != PLUME_OK)
+      return status;
+  } else {
     FieldSet<T> set{};
     set.count = 3;
     set.f[0] = single_field<T>(ud, static_cast<T*>(s->u.hat), static_cast<T*>(s->u.next), Dims{nx + 1, ny, nz},
@@ -1313,10 +1505,26 @@ static int step(const PlumeStepState* s, const PlumeStepParams* p, void* stream)
     return status;
   }
   if ((status = mark()) != PLUME_OK) return status;
-  k_subtract_gradient<T><<<face_grid(info), cell_block(), 0, st>>>(info, u, v, w, s->pressure);
-  CHECK_LAUNCH("subtract gradient");
+  if ((status = launch_subtract_gradient<T>(info, u, v, w, s->pressure, st)) != PLUME_OK) return status;
   if ((status = mark()) != PLUME_OK) return status;
   // advect smoke and temperature (stepper.py:54-60): the smoke budget holds smoke.next before its swap
+  const long n = (long)nx * ny * nz;
+  if (s->advect_scratch && g_fused_advection) {
+    // one pass: smoke and temperature advected together, temperature dissipated as it is stored, the smoke
+    // line sums of data, hat and next from the march; then the held factor and the smoke's scale + dissipation
+    if ((status = launch_mac_scalars<T>(info, u, v, w, sd, td, static_cast<T*>(s->smoke.next),
+                                        static_cast<T*>(s->temperature.next), 0.0f, p->ambient_k, 1,
+                                        s->advect_scratch, s->sums, p->apply_dissipation, p->heat_keep, p->ambient_k,
+                                        p->dt_over_cell, st)) != PLUME_OK)
+      return status;
+    k_budget_factor<<<1, dim3(32, 3), 0, st>>>(s->sums, sum_blocks(dims_of(info)), s->factor, nullptr, 1);
+    CHECK_LAUNCH("budget factor");
+    k_scalar_finish<T><<<grid_stride_blocks(n), 256, 0, st>>>(static_cast<T*>(s->smoke.next), nullptr, n, s->factor,
+                                                              p->apply_dissipation, p->smoke_keep, 1.0f,
+                                                              p->ambient_k);
+    CHECK_LAUNCH("scale and dissipate");
+    return mark();
+  }
   {
     VelT<T> vel = make_vel<T>(u, v, w, info.dims);
     FieldSet<T> set{};
@@ -1339,7 +1547,6 @@ static int step(const PlumeStepState* s, const PlumeStepParams* p, void* stream)
                                      static_cast<const T*>(s->smoke.next), s->sums, s->factor, nullptr, st)) != PLUME_OK)
     return status;
   // scale + dissipate (stepper.py:44) on the advected buffers
-  const long n = (long)nx * ny * nz;
   k_scalar_finish<T><<<grid_stride_blocks(n), 256, 0, st>>>(static_cast<T*>(s->smoke.next),
                                                             static_cast<T*>(s->temperature.next), n, s->factor,
                                                             p->apply_dissipation, p->smoke_keep, p->heat_keep,
