@@ -133,3 +133,11 @@ def sweep(path: Path, variations, preview: bool = False) -> list:
     from plume_b200.recipe.load import load_recipe
 
     return [load_recipe(path, preview=preview, sets=tuple(sets)) for sets in variations]
+
+
+def sweep_table(table: dict, variations, stem: str = "sweep", preview: bool = False) -> list:
+    """`sweep` of a recipe already parsed from TOML (extends resolved): instance n is the table with the n-th
+    list of overrides applied, named `<stem>_<n>`."""
+    from plume_b200.recipe.load import resolve_table
+
+    return [resolve_table(apply_sets(table, tuple(sets)), f"{stem}_{n}", preview) for n, sets in enumerate(variations)]

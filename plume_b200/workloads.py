@@ -163,33 +163,50 @@ if __name__ == "__main__":
 BATCH_GRIDS = ((48, 48, 48), (64, 96, 64), (96, 144, 96), (160, 240, 160))
 
 
-def batched_recipes(count: int = 64, frames: int = 48, seed: int = DEFAULT_SEED, grids=BATCH_GRIDS):
-    """`count` uneven smoke-puff recipes (parameter sweep): each instance's grid drawn from `grids` by seed,
-    in the same 2 m wide domain (so larger grids are finer and need more CFL substeps); emitter radius
-    U(4, 10) cells, its position jittered by up to 10% of the domain, heat buoyancy U(0.5, 1.5), drag
-    U(0, 0.5)/s, vorticity confinement U(0.1, 0.5); 24 fps, CFL 1 with up to 16 substeps per frame."""
+def batch_base_table(frames: int = 48) -> dict:
+    """The batched runs' base recipe: the 64 x 96 x 64 smoke puff in a 2 m wide domain, 24 fps, CFL 1 with up to
+    16 substeps per frame; every instance overrides its grid, emitter and forces."""
+    cell_m = 2.0 / 64.0
+    return {
+        "seed": 7,
+        "domain": {"size_m": [2.0, 3.0, 2.0], "cell_m": cell_m, "ambient_k": 1.0},
+        "time": {"duration_s": frames / 24.0, "frames": frames, "substeps": 1},
+        "emitter": [{"name": "puff", "center_m": [0.0, 0.25, 0.0], "radius_m": 6.0 * cell_m, "edge_softness": 0.0,
+                     "end_s": 0.5, "smoke_per_s": 1.0, "temperature_k": 2.0}],
+        "forces": {"gravity_mps2": 1.0, "heat_buoyancy": 1.0, "smoke_weight": 0.05, "drag_per_s": 0.2,
+                   "vorticity_confinement": 0.3},
+        "solver": {"multigrid_cycles": 4, "multigrid_sweeps": 2, "max_cells_per_step": 1.0, "max_substeps": 16},
+        "render": {"glow_start_k": 1.0, "light_dir": [0.5, 0.8, 0.3]},
+        "output": {"frame_px": 128},
+    }
+
+
+def batch_variations(count: int = 64, seed: int = DEFAULT_SEED, grids=BATCH_GRIDS) -> list:
+    """The `--set` overrides of each batched instance (a parameter sweep): its grid drawn from `grids` by seed
+    in the same 2 m wide domain (larger grids are finer and need more CFL substeps), emitter radius U(4, 10)
+    cells, the emitter's position jittered by up to 10% of the domain, heat buoyancy U(0.5, 1.5), drag
+    U(0, 0.5)/s, vorticity confinement U(0.1, 0.5)."""
     rng = np.random.default_rng(seed)
-    recipes = []
+    variations = []
     for index in range(count):
         nx, ny, nz = grids[int(rng.integers(len(grids)))]
         cell_m = 2.0 / nx
-        size = (nx * cell_m, ny * cell_m, nz * cell_m)
+        size = [nx * cell_m, ny * cell_m, nz * cell_m]
         radius = float(rng.uniform(4.0, 10.0)) * cell_m
         jitter = rng.uniform(-0.1, 0.1, 3) * np.array(size)
         center = [float(jitter[0]), float(8.0 * (nx / 64.0) * cell_m + abs(jitter[1]) * 0.5), float(jitter[2])]
-        table = {
-            "seed": 7 + index,
-            "domain": {"size_m": list(size), "cell_m": cell_m, "ambient_k": 1.0},
-            "time": {"duration_s": frames / 24.0, "frames": frames, "substeps": 1},
-            "emitter": [{"name": "puff", "center_m": center, "radius_m": radius, "edge_softness": 0.0,
-                         "end_s": 0.5, "smoke_per_s": 1.0, "temperature_k": 2.0}],
-            "forces": {"gravity_mps2": 1.0, "heat_buoyancy": float(rng.uniform(0.5, 1.5)), "smoke_weight": 0.05,
-                       "drag_per_s": float(rng.uniform(0.0, 0.5)),
-                       "vorticity_confinement": float(rng.uniform(0.1, 0.5))},
-            "solver": {"multigrid_cycles": 4, "multigrid_sweeps": 2, "max_cells_per_step": 1.0,
-                       "max_substeps": 16},
-            "render": {"glow_start_k": 1.0, "light_dir": [0.5, 0.8, 0.3]},
-            "output": {"frame_px": 128},
-        }
-        recipes.append(resolve_table(table, f"batch_{index}"))
-    return recipes
+        buoyancy, drag = float(rng.uniform(0.5, 1.5)), float(rng.uniform(0.0, 0.5))
+        confinement = float(rng.uniform(0.1, 0.5))
+        variations.append([f"seed={7 + index}", f"domain.size_m={size!r}", f"domain.cell_m={cell_m!r}",
+                           f"emitter.puff.radius_m={radius!r}", f"emitter.puff.center_m={center!r}",
+                           f"forces.heat_buoyancy={buoyancy!r}", f"forces.drag_per_s={drag!r}",
+                           f"forces.vorticity_confinement={confinement!r}"])
+    return variations
+
+
+def batched_recipes(count: int = 64, frames: int = 48, seed: int = DEFAULT_SEED, grids=BATCH_GRIDS):
+    """`count` uneven smoke-puff recipes: the base recipe swept over `batch_variations` through the recipe
+    front-end's `sweep_table`, so every instance passes the recipe checks."""
+    from plume_b200.recipe.variation import sweep_table
+
+    return sweep_table(batch_base_table(frames), batch_variations(count, seed, grids), "batch")

@@ -1,6 +1,7 @@
 """Whole-substep and whole-run parity of the CUDA path (plume_step through Stepper, and the frame loop)
-against the FP32 oracle. Tolerance for one substep: 1e-4 relative; in practice every field
-matches to the last bit except where the emitter's pow differs by an ulp."""
+against the FP32 oracle. Tolerance for one substep: 1e-4 relative. With the two-pass advection kernels every
+field matches to the last bit except where the emitter's pow differs by an ulp; the fused advection (the
+default) blends with fused multiply-adds and agrees to about an ulp per operator."""
 
 import json
 from pathlib import Path
@@ -50,11 +51,15 @@ def test_one_substep_matches_the_oracle(cuda_device, cells):
 
 @pytest.mark.parametrize("cells,faces", [((19, 24, 17), None), ((16, 12, 20), "closed"), ((2, 3, 1), None)],
                          ids=["19x24x17-open", "16x12x20-closed", "2x3x1-open"])
-def test_a_substep_without_exp_or_pow_gives_the_oracles_floats(cuda_device, cells, faces):
+@pytest.mark.parametrize("fused", [False, True], ids=["two-pass", "fused"])
+def test_a_substep_without_exp_or_pow_gives_the_oracles_floats(cuda_device, cells, faces, fused):
     """With the emitter finished and no drag or dissipation, no operator of the substep calls exp or pow, so
-    every field, the pressure included, is the oracle's to the last bit: the step's velocity advection (the
-    three face arrays in one launch) and its smoke and temperature advection, walls included."""
+    with the two-pass advection every field, the pressure included, is the oracle's to the last bit: the
+    step's velocity advection (the three face arrays in one launch) and its smoke and temperature advection,
+    walls included. The fused advection gives the same substep within the substep tolerance."""
     import dataclasses
+
+    from plume_b200 import _native as N
 
     recipe = plain_step_recipe(cells, cycles=2)
     recipe = dataclasses.replace(
@@ -67,7 +72,14 @@ def test_a_substep_without_exp_or_pow_gives_the_oracles_floats(cuda_device, cell
                 f.name: "closed" for f in dataclasses.fields(recipe.domain.faces)})))
     o, c, os_, cs, derived = stepper_pair(recipe)
     os_.step(1.0, derived.dt_s)
-    cs.step(1.0, derived.dt_s)
+    N.call("plume_use_fused_advection", int(fused))
+    try:
+        cs.step(1.0, derived.dt_s)
+    finally:
+        N.call("plume_use_fused_advection", 1)
+    if fused:
+        compare_fields(o, c, SUBSTEP_RTOL, "fused substep")
+        return
     for name in FIELDS:
         assert_same(host(getattr(c, name).data), getattr(o, name).data, name)
     assert_same(host(c.pressure), o.pressure, "pressure")

@@ -119,3 +119,23 @@ def test_a_sweep_resolves_one_recipe_per_variation(tmp_path):
     assert [r.forces.drag_per_s for r in recipes] == [0.0, 0.3, 0.0]
     assert [r.emitter[0].radius_m for r in recipes] == [0.25, 0.25, 0.4] and recipes[2].seed == 11
     assert all(r.time.frames == recipes[0].preview.frames for r in recipes)  # preview variants
+
+
+def test_batched_instances_are_a_sweep_of_the_base_recipe():
+    """The batched runs' instances come from the sweep front-end: the base recipe with each instance's
+    overrides applied, checked like any recipe, in order."""
+    from plume_b200.recipe.derived import derive
+    from plume_b200.recipe.variation import sweep_table
+    from plume_b200.workloads import BATCH_GRIDS, batch_base_table, batch_variations, batched_recipes
+
+    variations = batch_variations(count=5, seed=3)
+    recipes = batched_recipes(count=5, frames=6, seed=3)
+    assert [r.seed for r in recipes] == [7 + n for n in range(5)]
+    for recipe, sets in zip(recipes, variations):
+        values = dict(item.split("=", 1) for item in sets)
+        assert derive(recipe).cells in BATCH_GRIDS
+        assert recipe.domain.cell_m == float(values["domain.cell_m"])
+        assert recipe.emitter[0].radius_m == float(values["emitter.puff.radius_m"])
+        assert recipe.forces.drag_per_s == float(values["forces.drag_per_s"])
+        assert recipe.time.frames == 6
+    assert sweep_table(batch_base_table(6), variations, "batch") == recipes
