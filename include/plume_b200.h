@@ -218,6 +218,16 @@ int plume_solver_tuning(long long* tiled_min_cells, long long* bottom_max_cells,
  * caller's stream is itself being captured, launches are always made one by one into that capture. */
 int plume_use_graphs(int32_t enable);
 
+/* No counterpart in the reference (the same solve, another storage). plume_multigrid with caller scratch of
+ * plume_split_scratch_floats(&levels[0].info) floats: when the top level has at least the plume_tune_split
+ * threshold of cells (default 1 << 23, the levels larger than L2), it is swept in colour-split storage (red and
+ * black cells in separate arrays, converted in and out around the cycles), which halves the sectors a colour
+ * pass moves. Every value equals plume_multigrid's. plume_step does the same with its advect_scratch. */
+long long plume_split_scratch_floats(const PlumeGridInfo* info);
+int plume_tune_split(long long min_cells);
+int plume_multigrid_split(const PlumeLevel* levels, int32_t level_count, int32_t cycles, int32_t sweeps,
+                          float* scratch, void* stream);
+
 /* multigrid.py:36-43 residual_kernel. */
 int plume_residual(const PlumeGridInfo* info, const float* q, const float* rhs, float* residual, void* stream);
 

@@ -42,6 +42,9 @@ static long g_tiled_min_cells = 1L << 40;  // measured: per-colour sweeps win wh
 // 2048 cells (rather than 8192) saves 9% of the solve: a 16x24x16 level sweeps faster as per-colour launches
 // across the GPU than inside one block on one SM.
 static long g_bottom_max_cells = 2048;
+// The top level runs in colour-split storage (given caller scratch) when it has at least this many cells:
+// the levels that do not fit in L2, where the colour passes are bound by DRAM traffic.
+static long g_split_min_cells = 1L << 23;
 static int g_bottom_kind = 0;  // 0: the one-block solve, 1: the cluster solve
 constexpr size_t BOTTOM_MAX_SMEM = 200 * 1024;
 
@@ -202,6 +205,106 @@ __global__ void k_residual_restrict(PlumeGridInfo fine, const float* __restrict_
   const int out = at(coarse, i, j, k);
   coarse_rhs[out] = total / count;
   coarse_q[out] = 0.0f;
+}
+
+// ---- the top level in colour-split storage -----------------------------------------------------------------
+// A level larger than L2 is swept from two arrays per quantity, one per colour: cell (i, j, k) of colour
+// c = (i + j + k) & 1 sits at ((c * nx + i) * ny + j) * H + (k >> 1), H = (nz + 1) / 2. A colour pass then
+// reads and writes whole sectors of the cells it needs (its own q and rhs, the other colour's q) instead of
+// sectors shared by both colours. The updates, residuals and prolongation are the natural-layout kernels'
+// functions fed through a loader that maps (i, j, k) to the split index, so every value is the same.
+__device__ __forceinline__ long split_at(const Dims& d, int H, int i, int j, int k) {
+  return ((long)(((i + j + k) & 1) * d.n0 + i) * d.n1 + j) * H + (k >> 1);
+}
+
+// natural -> split (to_split) or split -> natural: thread (i, j, m) moves the cells k = 2m and 2m + 1
+template <bool TO_SPLIT>
+__global__ void k_split_layout(Dims d, int H, const float* __restrict__ in, float* __restrict__ out) {
+  wait_for_previous_grid();
+  const int i = blockIdx.z, j = blockIdx.y * blockDim.y + threadIdx.y, m = blockIdx.x * blockDim.x + threadIdx.x;
+  if (j >= d.n1 || m >= H) return;
+#pragma unroll
+  for (int c = 0; c < 2; ++c) {
+    const int k = 2 * m + ((i + j + c) & 1);
+    const long s = ((long)(c * d.n0 + i) * d.n1 + j) * H + m;
+    if (k < d.n2) {
+      const long n = ((long)i * d.n1 + j) * d.n2 + k;
+      if (TO_SPLIT) out[s] = in[n];
+      else out[n] = in[s];
+    } else if (TO_SPLIT) {
+      out[s] = 0.0f;  // the padding slot of an odd row
+    }
+  }
+}
+
+// One colour pass over the split arrays, PLANES x-planes per thread: every update is computed before any is
+// stored (a colour reads only the other colour).
+template <int PLANES>
+__global__ void k_rb_split(PlumeGridInfo info, int H, float* __restrict__ qs, const float* __restrict__ rs, int color,
+                           float relaxation) {
+  wait_for_previous_grid();
+  const int nx = info.dims[0], ny = info.dims[1], nz = info.dims[2];
+  const int i0 = blockIdx.z * PLANES, j = blockIdx.y * blockDim.y + threadIdx.y;
+  const int m = blockIdx.x * blockDim.x + threadIdx.x;
+  if (j >= ny || m >= H) return;
+  const Dims d = dims_of(info);
+  const float ghost = ghost_coupling(info);
+  auto load = [&](int a, int b, int c) { return qs[split_at(d, H, a, b, c)]; };
+  float out[PLANES];
+  bool write[PLANES];
+#pragma unroll
+  for (int p = 0; p < PLANES; ++p) {
+    const int i = i0 + p, k = 2 * m + ((i + j + color) & 1);
+    write[p] = false;
+    if (i < nx && k < nz) {
+      const long idx = ((long)(color * nx + i) * ny + j) * H + m;
+      write[p] = relax_cell(true, info, ghost, i, j, k, qs[idx], __ldg(rs + idx), relaxation, load, out[p]);
+    }
+  }
+#pragma unroll
+  for (int p = 0; p < PLANES; ++p)
+    if (write[p]) qs[((long)(color * nx + i0 + p) * ny + j) * H + m] = out[p];
+}
+
+// k_residual_restrict with the fine level in split storage.
+__global__ void k_residual_restrict_split(PlumeGridInfo fine, int H, const float* __restrict__ qs,
+                                          const float* __restrict__ rs, Dims coarse, float* __restrict__ coarse_rhs,
+                                          float* __restrict__ coarse_q) {
+  wait_for_previous_grid();
+  const int i = blockIdx.z, j = blockIdx.y * blockDim.y + threadIdx.y, k = blockIdx.x * blockDim.x + threadIdx.x;
+  if (j >= coarse.n1 || k >= coarse.n2) return;
+  const Dims fd = dims_of(fine);
+  auto load = [&](int a, int b, int c) { return __ldg(qs + split_at(fd, H, a, b, c)); };
+  const bool uniform = is_uniform(fine);
+  const float ghost = ghost_coupling(fine);
+  float total = 0.0f, count = 0.0f;
+#pragma unroll
+  for (int di = 0; di < 2; ++di)
+#pragma unroll
+    for (int dj = 0; dj < 2; ++dj)
+#pragma unroll
+      for (int dk = 0; dk < 2; ++dk) {
+        const int fi = 2 * i + di, fj = 2 * j + dj, fk = 2 * k + dk;
+        if (fi < fd.n0 && fj < fd.n1 && fk < fd.n2) {
+          const long idx = split_at(fd, H, fi, fj, fk);
+          total = total + residual_cell(uniform, fine, ghost, fi, fj, fk, __ldg(qs + idx), __ldg(rs + idx), load);
+          count = count + 1.0f;
+        }
+      }
+  const int out = at(coarse, i, j, k);
+  coarse_rhs[out] = total / count;
+  coarse_q[out] = 0.0f;
+}
+
+// k_prolong_add with the fine level in split storage: thread (c, i, j, m) adds to its cell of colour c.
+__global__ void k_prolong_add_split(Dims coarse, Dims fine, int H, const float* __restrict__ cq, float* __restrict__ qs) {
+  wait_for_previous_grid();
+  const int c = blockIdx.z / fine.n0, i = blockIdx.z - c * fine.n0;
+  const int j = blockIdx.y * blockDim.y + threadIdx.y, m = blockIdx.x * blockDim.x + threadIdx.x;
+  const int k = 2 * m + ((i + j + c) & 1);
+  if (j >= fine.n1 || m >= H || k >= fine.n2) return;
+  const long idx = ((long)(c * fine.n0 + i) * fine.n1 + j) * H + m;
+  qs[idx] = qs[idx] + sample_index_space(cq, coarse, prolong_point(i, j, k));
 }
 
 // ---- the cluster coarse solve --------------------------------------------------------------------------------
@@ -861,6 +964,36 @@ static int colour_sweep(const PlumeGridInfo& info, float* q, const float* rhs, f
   return PLUME_OK;
 }
 
+// The top level's split arrays: q then rhs, each 2 * nx * ny * H floats.
+struct SplitTop {
+  float* q;
+  float* rhs;
+  int H;
+};
+
+static long split_floats(const PlumeGridInfo& info) {
+  return 2L * info.dims[0] * info.dims[1] * ((info.dims[2] + 1) / 2);
+}
+
+static int split_sweeps(const PlumeGridInfo& info, const SplitTop& sp, int sweeps, const float* coarse_q,
+                        const PlumeGridInfo* coarse, cudaStream_t st) {
+  const Dims d = dims_of(info);
+  if (coarse) {
+    const Dims cd = dims_of(*coarse);
+    int status = launch_solve_kernel(k_prolong_add_split, dim3((sp.H + TZ - 1) / TZ, (d.n1 + TY - 1) / TY, 2 * d.n0),
+                                     cell_block(), 0, st, "prolong (split)", cd, d, sp.H, coarse_q, sp.q);
+    if (status != PLUME_OK) return status;
+  }
+  const dim3 grid((sp.H + TZ - 1) / TZ, (d.n1 + TY - 1) / TY, (d.n0 + 1) / 2);
+  for (int s = 0; s < sweeps; ++s)
+    for (int color = 0; color < 2; ++color) {
+      int status = launch_solve_kernel(k_rb_split<2>, grid, cell_block(), 0, st, "red-black colour (split)", info,
+                                       sp.H, sp.q, (const float*)sp.rhs, color, 1.0f);
+      if (status != PLUME_OK) return status;
+    }
+  return PLUME_OK;
+}
+
 // `sweeps` full sweeps; when `coarse` is given its correction is prolonged first (folded into the first tiled
 // sweep on large levels).
 static int sweeps_with_prolong(const PlumeGridInfo& info, Pressure& q, const float* rhs, int sweeps, float relaxation,
@@ -1014,8 +1147,27 @@ static int launch_bottom(const PlumeLevel* levels, int count, int sweeps, size_t
 // One V-cycle below `index` (multigrid.py:130-147). Every level keeps its pressure in q and uses its residual
 // array as the sweeps' second array; the residual itself is never stored (k_residual_restrict).
 static int v_cycle(const PlumeLevel* levels, int count, int index, Pressure& q, int bottom, size_t smem, int sweeps,
-                   cudaStream_t st, int coarse_f64) {
+                   cudaStream_t st, int coarse_f64, const SplitTop* split = nullptr) {
   const PlumeLevel& lv = levels[index];
+  if (index == 0 && split) {  // the top level in split storage (never the bottom or the coarsest level)
+    int status = split_sweeps(lv.info, *split, sweeps, nullptr, nullptr, st);
+    if (status != PLUME_OK) return status;
+    const PlumeLevel& coarse = levels[1];
+    const Dims cd = dims_of(coarse.info);
+    if ((status = launch_solve_kernel(k_residual_restrict_split, cell_grid(cd.n0, cd.n1, cd.n2), cell_block(), 0, st,
+                                      "residual and restriction (split)", lv.info, split->H, (const float*)split->q,
+                                      (const float*)split->rhs, cd, coarse.rhs, coarse.q)) != PLUME_OK)
+      return status;
+    Pressure coarse_q{coarse.q, coarse.residual};
+    if ((status = v_cycle(levels, count, 1, coarse_q, bottom, smem, sweeps, st, coarse_f64)) != PLUME_OK) return status;
+    if (coarse_q.cur != coarse.q) {
+      status = runtime_status("coarse pressure copy",
+                              cudaMemcpyAsync(coarse.q, coarse_q.cur, sizeof(float) * cd.n0 * cd.n1 * cd.n2,
+                                              cudaMemcpyDeviceToDevice, st));
+      if (status != PLUME_OK) return status;
+    }
+    return split_sweeps(lv.info, *split, sweeps, coarse.q, &coarse.info, st);
+  }
   if (index == bottom) {
     PlumeLevel first[BOTTOM_MAX_LEVELS];
     for (int l = bottom; l < count && l - bottom < BOTTOM_MAX_LEVELS; ++l) first[l - bottom] = levels[l];
@@ -1054,10 +1206,36 @@ static int v_cycle(const PlumeLevel* levels, int count, int index, Pressure& q, 
   return sweeps_with_prolong(lv.info, q, lv.rhs, sweeps, 1.0f, coarse.q, &coarse.info, st);
 }
 
+// Whether the top level runs split: scratch given, at least two levels with level 0 above the bottom solve,
+// uniform couplings, swept by colour (not tiled) and at least g_split_min_cells cells.
+static bool use_split(const PlumeLevel* levels, int count, int bottom, const float* scratch) {
+  const PlumeGridInfo& info = levels[0].info;
+  return scratch && count >= 2 && bottom > 0 && uniform_level(info) && cells_of(info) >= g_split_min_cells &&
+         cells_of(info) < g_tiled_min_cells;
+}
+
 static int multigrid_direct(const PlumeLevel* levels, int count, int cycles, int sweeps, cudaStream_t st,
-                            int coarse_f64) {
+                            int coarse_f64, float* split_scratch = nullptr) {
   size_t smem = 0;
   const int bottom = bottom_start(levels, count, &smem, coarse_f64);
+  if (use_split(levels, count, bottom, split_scratch)) {
+    const PlumeGridInfo& info = levels[0].info;
+    const Dims d = dims_of(info);
+    SplitTop sp{split_scratch, split_scratch + split_floats(info), (d.n2 + 1) / 2};
+    const dim3 grid((sp.H + TZ - 1) / TZ, (d.n1 + TY - 1) / TY, d.n0);
+    int status = launch_solve_kernel(k_split_layout<true>, grid, cell_block(), 0, st, "pressure to split storage", d,
+                                     sp.H, (const float*)levels[0].q, sp.q);
+    if (status != PLUME_OK) return status;
+    if ((status = launch_solve_kernel(k_split_layout<true>, grid, cell_block(), 0, st, "divergence to split storage",
+                                      d, sp.H, (const float*)levels[0].rhs, sp.rhs)) != PLUME_OK)
+      return status;
+    Pressure unused{levels[0].q, levels[0].residual};
+    for (int c = 0; c < cycles; ++c)
+      if ((status = v_cycle(levels, count, 0, unused, bottom, smem, sweeps, st, coarse_f64, &sp)) != PLUME_OK)
+        return status;
+    return launch_solve_kernel(k_split_layout<false>, grid, cell_block(), 0, st, "pressure from split storage", d,
+                               sp.H, (const float*)sp.q, levels[0].q);
+  }
   Pressure q{levels[0].q, levels[0].residual};
   for (int c = 0; c < cycles; ++c) {
     int status = v_cycle(levels, count, 0, q, bottom, smem, sweeps, st, coarse_f64);
@@ -1080,7 +1258,8 @@ namespace plume {
 struct GraphKey {
   int device;
   int count, cycles, sweeps, kind, coarse_f64;
-  long tiled, bottom;
+  long tiled, bottom, split_min;
+  float* split;
   PlumeLevel levels[16];
   bool operator==(const GraphKey& o) const { return std::memcmp(this, &o, sizeof(GraphKey)) == 0; }
 };
@@ -1121,7 +1300,7 @@ static int graph_for(const GraphKey& key, const PlumeLevel* levels, cudaGraphExe
   status = runtime_status("begin capture", cudaStreamBeginCapture(cap, cudaStreamCaptureModeThreadLocal));
   if (status != PLUME_OK) return status;
   set_launch_counting(false);
-  const int run = multigrid_direct(levels, key.count, key.cycles, key.sweeps, cap, key.coarse_f64);
+  const int run = multigrid_direct(levels, key.count, key.cycles, key.sweeps, cap, key.coarse_f64, key.split);
   set_launch_counting(true);
   cudaGraph_t graph = nullptr;
   status = runtime_status("end capture", cudaStreamEndCapture(cap, &graph));
@@ -1152,12 +1331,13 @@ static int graph_for(const GraphKey& key, const PlumeLevel* levels, cudaGraphExe
   return PLUME_OK;
 }
 
-int multigrid_cycles(const PlumeLevel* levels, int count, int cycles, int sweeps, cudaStream_t st, int coarse_f64) {
+int multigrid_cycles(const PlumeLevel* levels, int count, int cycles, int sweeps, cudaStream_t st, int coarse_f64,
+                     float* split_scratch) {
   cudaStreamCaptureStatus capturing = cudaStreamCaptureStatusNone;
   int device = 0;
   if (!g_use_graphs || count > 16 || cudaStreamIsCapturing(st, &capturing) != cudaSuccess ||
       capturing != cudaStreamCaptureStatusNone || cudaGetDevice(&device) != cudaSuccess || device < 0 || device >= 64)
-    return multigrid_direct(levels, count, cycles, sweeps, st, coarse_f64);
+    return multigrid_direct(levels, count, cycles, sweeps, st, coarse_f64, split_scratch);
   GraphKey key;
   std::memset(&key, 0, sizeof(key));
   key.device = device;
@@ -1168,6 +1348,8 @@ int multigrid_cycles(const PlumeLevel* levels, int count, int cycles, int sweeps
   key.coarse_f64 = coarse_f64;
   key.tiled = g_tiled_min_cells;
   key.bottom = g_bottom_max_cells;
+  key.split_min = g_split_min_cells;
+  key.split = split_scratch;
   std::memcpy(key.levels, levels, sizeof(PlumeLevel) * count);
   std::lock_guard<std::mutex> lock(g_graph_mutex);
   {  // the coarse solve's shared-memory attribute must be set before its first capture
@@ -1200,6 +1382,18 @@ extern "C" int plume_tune_solver(long long tiled_min_cells, long long bottom_max
   plume::g_bottom_max_cells = (long)bottom_max_cells;
   plume::g_bottom_kind = bottom_kind;
   return PLUME_OK;
+}
+
+extern "C" int plume_tune_split(long long min_cells) {
+  if (min_cells < 1) return plume::fail(PLUME_ERR_INVALID, "tune_split: min_cells must be positive");
+  plume::g_split_min_cells = (long)min_cells;
+  return PLUME_OK;
+}
+
+extern "C" long long plume_split_scratch_floats(const PlumeGridInfo* info) {
+  if (!info || info->dims[0] < 1 || info->dims[1] < 1 || info->dims[2] < 1)
+    return plume::fail(PLUME_ERR_INVALID, "split_scratch_floats: bad dims");
+  return 2 * plume::split_floats(*info);
 }
 
 extern "C" int plume_solver_tuning(long long* tiled_min_cells, long long* bottom_max_cells, int32_t* bottom_kind) {

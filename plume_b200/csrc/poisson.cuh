@@ -239,6 +239,9 @@ __device__ __forceinline__ F3 prolong_point(int i, int j, int k) {
 int red_black_sweeps(const PlumeGridInfo& info, float* q, float* scratch, const float* rhs, int sweeps,
                      float relaxation, cudaStream_t st);
 // coarse_f64: sweep the coarsest level in double (the defect-correction solve's correction cycles)
-int multigrid_cycles(const PlumeLevel* levels, int count, int cycles, int sweeps, cudaStream_t st, int coarse_f64 = 0);
+// split_scratch: plume_split_scratch_floats(levels[0].info) floats; with it the top level may run in
+// colour-split storage (same values)
+int multigrid_cycles(const PlumeLevel* levels, int count, int cycles, int sweeps, cudaStream_t st, int coarse_f64 = 0,
+                     float* split_scratch = nullptr);
 
 }  // namespace plume

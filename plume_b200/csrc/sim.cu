@@ -1258,6 +1258,16 @@ extern "C" int plume_multigrid(const PlumeLevel* levels, int32_t level_count, in
   return multigrid_cycles(levels, level_count, cycles, sweeps, as_stream(stream));
 }
 
+extern "C" int plume_multigrid_split(const PlumeLevel* levels, int32_t level_count, int32_t cycles, int32_t sweeps,
+                                     float* scratch, void* stream) {
+  CHECK_ARG(levels && level_count >= 1 && cycles >= 0 && sweeps >= 0 && scratch, "multigrid_split: bad argument");
+  for (int l = 0; l < level_count; ++l)
+    CHECK_ARG(levels[l].q && levels[l].rhs && levels[l].residual && levels[l].residual != levels[l].q &&
+                  valid_dims(levels[l].info.dims),
+              "multigrid_split: bad level %d", l);
+  return multigrid_cycles(levels, level_count, cycles, sweeps, as_stream(stream), 0, scratch);
+}
+
 extern "C" int plume_residual(const PlumeGridInfo* info, const float* q, const float* rhs, float* residual,
                               void* stream) {
   CHECK_ARG(info && q && rhs && residual, "residual: null argument");
@@ -1498,7 +1508,8 @@ static int step(const PlumeStepState* s, const PlumeStepParams* p, void* stream)
   if ((status = project_begin<T>(info, u, v, w, s->divergence, st)) != PLUME_OK) return status;
   if ((status = mark()) != PLUME_OK) return status;
   if (p->solver == 0) {
-    if ((status = multigrid_cycles(s->levels, s->level_count, p->solver_iterations, p->multigrid_sweeps, st)) != PLUME_OK)
+    if ((status = multigrid_cycles(s->levels, s->level_count, p->solver_iterations, p->multigrid_sweeps, st, 0,
+                                   s->advect_scratch)) != PLUME_OK)
       return status;
   } else if ((status = red_black_sweeps(info, s->pressure, s->levels[0].residual, s->divergence, p->solver_iterations,
                                         1.5f, st)) != PLUME_OK) {

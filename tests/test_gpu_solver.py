@@ -112,3 +112,37 @@ def test_the_autotuner_picks_the_fastest_candidate_and_restores_the_pressure(tun
     assert result.best == min(result.ms_per_solve, key=result.ms_per_solve.get)
     assert solver_tuning() == result.best
     assert torch.equal(c.pressure, before)
+
+
+@pytest.fixture
+def split_threshold(cuda_device):
+    from plume_b200 import _native as N
+
+    N.call("plume_tune_split", 1)  # every top level runs split, whatever its size
+    yield
+    N.call("plume_tune_split", 1 << 23)
+
+
+@pytest.mark.parametrize("cells,faces", CASES + [((24, 20, 33), OPEN), ((31, 17, 9), ALL_CLOSED)],
+                         ids=IDS + ["24x20x33-open", "31x17x9-closed"])
+def test_colour_split_top_level_gives_the_same_pressure(split_threshold, cells, faces):
+    """The top level swept in colour-split storage (red and black cells in separate arrays, odd rows padded)
+    gives plume_multigrid's pressure bit for bit, with a warm start and 2 or 3 sweeps."""
+    import torch
+
+    from plume_b200 import _native as N
+    from plume_b200.sim.multigrid import Multigrid
+    from plume_b200.sim.pressure import compute_divergence
+
+    for sweeps in (2, 3):
+        _, a = seeded_pair(cells, faces)
+        _, b = seeded_pair(cells, faces)
+        compute_divergence(a)
+        compute_divergence(b)
+        ma, mb = Multigrid(a, 2, sweeps), Multigrid(b, 2, sweeps)
+        ma(a)
+        scratch = torch.empty(N.lib().plume_split_scratch_floats(b.info), dtype=torch.float32, device="cuda:0")
+        levels = mb.native_levels(b)
+        N.call("plume_multigrid_split", levels, len(mb.levels), 2, sweeps, N.ptr(scratch), N.stream())
+        torch.cuda.synchronize()
+        assert_same(host(b.pressure), host(a.pressure), f"pressure, {sweeps} sweeps")

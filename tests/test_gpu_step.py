@@ -150,3 +150,29 @@ def test_same_input_gives_identical_bytes(cuda_device):
             cs.step(n * derived.dt_s, derived.dt_s)
         results.append(b"".join(host(getattr(c, name).data).tobytes() for name in FIELDS))
     assert results[0] == results[1]
+
+
+def test_a_substep_with_the_split_top_level_gives_the_oracles_floats(cuda_device):
+    """plume_step with the pressure solve's top level in colour-split storage (forced on at this size) and the
+    two-pass advection: no exp or pow in the substep, so every field and the pressure are the oracle's."""
+    import dataclasses
+
+    from plume_b200 import _native as N
+
+    recipe = plain_step_recipe((21, 24, 19), cycles=2)
+    recipe = dataclasses.replace(
+        recipe, emitter=[dataclasses.replace(recipe.emitter[0], end_s=0.01)],
+        forces=dataclasses.replace(recipe.forces, drag_per_s=0.0),
+        dissipation=dataclasses.replace(recipe.dissipation, smoke_per_s=0.0, cooling_per_s=0.0))
+    o, c, os_, cs, derived = stepper_pair(recipe)
+    os_.step(1.0, derived.dt_s)
+    N.call("plume_use_fused_advection", 0)
+    N.call("plume_tune_split", 1)
+    try:
+        cs.step(1.0, derived.dt_s)
+    finally:
+        N.call("plume_use_fused_advection", 1)
+        N.call("plume_tune_split", 1 << 23)
+    for name in FIELDS:
+        assert_same(host(getattr(c, name).data), getattr(o, name).data, name)
+    assert_same(host(c.pressure), o.pressure, "pressure")
