@@ -203,96 +203,61 @@ def cpu_baseline(recipe, derived, fields, budget_s: float = 20.0) -> dict:
                       f"warm-up, oracle C++ FP32 with OpenMP on {threads} threads ({elapsed:.1f} s)"}
 
 
-def storage_variants(recipe, derived, fields, steps: int, device: str) -> dict:
-    """The same workload with velocity, smoke and temperature stored as bfloat16 / float16 (float32
-    arithmetic): Mcell-substeps/s over `steps` substeps, and the error against an FP64 run of the plain method
-    on a small case of the same step (24 x 32 x 24, 4 substeps): the largest field error relative to the
-    field's range and the largest rendered-thickness error."""
-    import numpy as np
+def batched_variant(device: str, count: int = 64, frames: int = 48) -> dict:
+    """The batched uneven recipes (BASELINE C4): `count` instances from the sweep front-end, grids drawn among
+    48^3, 64x96x64, 96x144x96 and 160x240x160, 48 frames with CFL-limited substeps. Three arms on the same
+    instances: plain FP32 one instance after another, FP32 batched (all instances at once on their own
+    streams) and BF16 batched. Each arm is built, run once (allocations, pressure-solve graph captures), reset
+    and run again; the second run is timed with CUDA events. Each instance's last frame is rendered after the
+    timed run: thickness differences of the BF16 arm from the FP32 arm (largest pixel difference, and the
+    relative difference of the frame's total thickness), and whether the FP32 arms agree byte for byte."""
     import torch
 
-    from oracle import oracle as O
     from plume_b200.recipe.derived import derive
     from plume_b200.render.camera import sheet_domain_view
     from plume_b200.render.frame_renderer import FrameRenderer
-    from plume_b200.sim.grid import make_grid
-    from plume_b200.sim.stepper import Stepper
-    from plume_b200.workloads import operator_fields, plain_step_recipe
-
-    small = plain_step_recipe((24, 32, 24), cycles=4)
-    small_derived = derive(small)
-    sd = small.domain
-    reference = O.make_grid(small_derived, sd.cell_m, sd.faces, sd.ambient_k, "f64")
-    small_fields = operator_fields(small_derived.cells, 11, sd.ambient_k)
-    for name, values in small_fields.items():
-        getattr(reference, name).data[...] = values
-    stepper64 = O.Stepper(reference, small)
-    for n in range(4):
-        stepper64.step(n * small_derived.dt_s, small_derived.dt_s)
-    view = sheet_domain_view(small, small_derived)
-    thickness64 = O.FrameRenderer(view, small.render, small_derived.cells, small.output.channels,
-                                  "f64").render(reference)[..., 1]
-    out = {}
-    for label, storage in (("f32", torch.float32), ("bf16", torch.bfloat16), ("f16", torch.float16)):
-        d = recipe.domain
-        grid = make_grid(derived, d.cell_m, d.faces, d.ambient_k, device, storage=storage)
-        for name, values in fields.items():
-            getattr(grid, name).data.copy_(torch.from_numpy(values))
-        stepper = Stepper(grid, recipe)
-        for n in range(3):
-            stepper.step(n * derived.dt_s, derived.dt_s)
-        start, end = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-        start.record()
-        for n in range(steps):
-            stepper.step((3 + n) * derived.dt_s, derived.dt_s)
-        end.record()
-        torch.cuda.synchronize()
-        value = math.prod(derived.cells) * steps / (start.elapsed_time(end) / 1e3) / 1e6
-        del grid, stepper
-        g = make_grid(small_derived, sd.cell_m, sd.faces, sd.ambient_k, device, storage=storage)
-        for name, values in small_fields.items():
-            getattr(g, name).data.copy_(torch.from_numpy(values))
-        st = Stepper(g, small)
-        for n in range(4):
-            st.step(n * small_derived.dt_s, small_derived.dt_s)
-        field_error = max(float(np.abs(getattr(g, n).data.float().cpu().numpy() - getattr(reference, n).data).max()
-                                / np.abs(getattr(reference, n).data).max())
-                          for n in ("u", "v", "w", "smoke", "temperature"))
-        frame = FrameRenderer(view, small.render, small_derived.cells, small.output.channels, device).render(g)
-        out[label] = {"value": value, "unit": METRIC, "steps": steps,
-                      "field_error_vs_fp64": field_error,
-                      "thickness_error_vs_fp64": float(np.abs(frame[..., 1] - thickness64).max())}
-    return out
-
-
-def batched_variant(device: str, count: int = 32, frames: int = 24) -> dict:
-    """Uneven recipes (grids 48^3 to 160x240x160, sweep of emitter, buoyancy, drag and confinement) run one
-    after another through simulate_frames, then all at once on per-instance streams; Mcell-substeps/s of each
-    (whole runs, timed on the host around device-synchronised runs)."""
-    import torch
-
-    from plume_b200.recipe.derived import derive
-    from plume_b200.sim.batch import Batch, run_one_at_a_time
+    from plume_b200.sim.batch import Batch
     from plume_b200.workloads import batched_recipes
 
     recipes = batched_recipes(count=count, frames=frames)
-    runs = {"one_at_a_time": [], "batched": []}
-    # Each schedule runs twice, alternating. A whole run is timed on the host, allocation and graph capture
-    # included, and its launches come from one host thread, so it varies with the host from run to run;
-    # the best run of each schedule is reported, with every run listed.
-    for _ in range(2):
-        for arm in runs:
-            torch.cuda.synchronize()
-            start = time.perf_counter()
-            logs = run_one_at_a_time(recipes, device) if arm == "one_at_a_time" else Batch(recipes, device).run()
-            torch.cuda.synchronize()
-            elapsed = time.perf_counter() - start
-            work = sum(math.prod(derive(r).cells) * log.total_steps for r, log in zip(recipes, logs))
-            runs[arm].append(work / elapsed / 1e6)
-            torch.cuda.empty_cache()
-    best = {arm: max(rates) for arm, rates in runs.items()}
-    return {"instances": count, "frames": frames, "unit": METRIC, "value": best["batched"],
-            "one_at_a_time": best["one_at_a_time"], "ratio": best["batched"] / best["one_at_a_time"], "runs": runs}
+    arms = (("one_at_a_time_f32", torch.float32, True), ("batched_f32", torch.float32, False),
+            ("batched_bf16", torch.bfloat16, False))
+    out, last = {"instances": count, "frames": frames, "unit": METRIC}, {}
+    for name, storage, sequential in arms:
+        batch = Batch(recipes, device, storage=storage)
+        batch.run(sequential=sequential)
+        batch.reset()
+        torch.cuda.synchronize()
+        start, end = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        start.record()
+        wall = time.perf_counter()
+        logs = batch.run(sequential=sequential)
+        end.record()
+        torch.cuda.synchronize()
+        wall = time.perf_counter() - wall
+        ms = start.elapsed_time(end)
+        work = sum(math.prod(derive(r).cells) * log.total_steps for r, log in zip(recipes, logs))
+        out[name] = {"value": work / (ms / 1e3) / 1e6, "device_ms": ms, "host_wall_s": wall,
+                     "cell_substeps": work, "substeps": sum(log.total_steps for log in logs)}
+        frames_out = []
+        for recipe, grid in zip(recipes, batch.grids):
+            derived = derive(recipe)
+            view = sheet_domain_view(recipe, derived)
+            renderer = FrameRenderer(view, recipe.render, derived.cells, recipe.output.channels, device)
+            frames_out.append(renderer.render(grid)[..., 1].astype(np.float64))
+        last[name] = frames_out
+        del batch
+        torch.cuda.empty_cache()
+    base = out["one_at_a_time_f32"]["value"]
+    out["ratio_bf16_batched_to_f32_one_at_a_time"] = out["batched_bf16"]["value"] / base
+    out["ratio_f32_batched_to_f32_one_at_a_time"] = out["batched_f32"]["value"] / base
+    out["f32_arms_identical"] = all(np.array_equal(a, b) for a, b in zip(last["one_at_a_time_f32"], last["batched_f32"]))
+    pixel = [float(np.abs(a - b).max()) for a, b in zip(last["batched_bf16"], last["batched_f32"])]
+    total = [abs(float(a.sum()) - float(b.sum())) / max(float(b.sum()), 1e-30)
+             for a, b in zip(last["batched_bf16"], last["batched_f32"])]
+    out["bf16_vs_f32_last_frame"] = {"max_pixel_thickness": max(pixel), "max_relative_total_thickness": max(total)}
+    out["value"] = out["batched_bf16"]["value"]
+    return out
 
 
 def adjoint_variant(device: str) -> dict:
@@ -412,16 +377,21 @@ def operators_variant(device: str) -> dict:
             "march_256x256_ms": render_ms}
 
 
-def large_mixed_variant(device: str, steps: int = 8, frames: int = 2) -> dict:
-    """The large mixed-precision case at 256 x 384 x 256 (dx = 1/128 m, emitter radius 24 cells), seeded on the
-    device: the fields stored as bfloat16 (float arithmetic) against the plain FP32 GPU run of the same state.
-    Mcell-substeps/s of each; the projection of the FP32 state's divergence refined to relative residual 1e-7
-    (defect correction, the pressure as a compensated float pair); a 512 x 512 march; and after `frames`
-    frames of 4 substeps, the largest per-frame thickness and heat difference of the bfloat16 run from the FP32
-    run (heat relative to the FP32 frame's largest heat)."""
-    import numpy as np
+def mixed_variant(device: str, fields=None, steps: int = 8, frames: int = 2, pixels: int = 256) -> dict:
+    """The large mixed-precision case (BASELINE C5) at 256 x 384 x 256 (dx = 1/128 m, emitter radius 24 cells):
+    the seeded state stepped with velocity, smoke and temperature stored as FP32, BF16 and FP16 (FP32
+    arithmetic), each timed over `steps` substeps (CUDA events), then restarted and run `frames` frames of 4
+    substeps, each frame rendered (pixels x pixels, the normal-map layout: thickness and heat depend on smoke
+    and temperature only). The same frames from an FP64 run of the plain method (the oracle in double, on the
+    host cores) are the reference: per frame, the largest pixel difference of thickness and of heat (relative
+    to the frame's largest heat), and the relative difference of the frame's total thickness. Also the
+    projection refined to a relative residual of 1e-7 (FP32 multigrid with defect correction, FP64 norms and
+    coarsest level) and a 512 x 512 march of the FP32 state."""
+    import dataclasses
+
     import torch
 
+    from oracle import oracle as O
     from plume_b200.recipe.derived import derive
     from plume_b200.render.camera import sheet_domain_view
     from plume_b200.render.frame_renderer import FrameRenderer
@@ -429,19 +399,61 @@ def large_mixed_variant(device: str, steps: int = 8, frames: int = 2) -> dict:
     from plume_b200.sim.multigrid import Multigrid
     from plume_b200.sim.pressure import compute_divergence
     from plume_b200.sim.stepper import Stepper
-    from plume_b200.workloads import device_operator_fields, plain_step_recipe
+    from plume_b200.workloads import plain_step_recipe
 
     cells = (256, 384, 256)
     recipe = plain_step_recipe(cells)
     derived = derive(recipe)
     d = recipe.domain
-    fields = device_operator_fields(cells, 20261203, d.ambient_k, device)
-    view = square_view(sheet_domain_view(recipe, derived), 512)
-    out, runs = {"cells": list(cells)}, {}
-    for label, storage in (("f32", torch.float32), ("bf16", torch.bfloat16)):
+    if fields is None or tuple(fields["smoke"].shape) != cells:
+        fields = seeded_state(cells, d.ambient_k)
+    normal_layout = "heat,thickness,normal_x,normal_y"
+    view = square_view(sheet_domain_view(recipe, derived), pixels)
+    dt = derived.dt_s
+    out = {"cells": list(cells), "frames": frames, "substeps_per_frame": 4, "frame_pixels": pixels}
+
+    threads = O.set_threads(os.cpu_count() or 1)
+    start = time.perf_counter()
+    reference = O.make_grid(derived, d.cell_m, d.faces, d.ambient_k, "f64")
+    for name, values in fields.items():
+        getattr(reference, name).data[...] = values
+    stepper64 = O.Stepper(reference, recipe)
+    renderer64 = O.FrameRenderer(view, recipe.render, derived.cells, normal_layout, "f64")
+    frames64 = []
+    for frame in range(frames):
+        for n in range(4):
+            stepper64.step((4 * frame + n) * dt, dt)
+        frames64.append(renderer64.render(reference).astype(np.float64))
+    out["fp64_reference"] = {"kind": "oracle in double", "threads": threads, "seconds": time.perf_counter() - start}
+    del reference, stepper64, renderer64
+
+    for label, storage in (("f32", torch.float32), ("bf16", torch.bfloat16), ("f16", torch.float16)):
         grid = make_grid(derived, d.cell_m, d.faces, d.ambient_k, device, storage=storage)
         for name, values in fields.items():
-            getattr(grid, name).data.copy_(values)
+            getattr(grid, name).data.copy_(torch.from_numpy(values))
+        stepper = Stepper(grid, recipe)
+        for n in range(3):  # warm-up: the solve's graph capture, allocations
+            stepper.step(n * dt, dt)
+        ms = device_ms(lambda: [stepper.step((3 + n) * dt, dt) for n in range(steps)])
+        entry = {"value": math.prod(cells) * steps / (ms / 1e3) / 1e6, "unit": METRIC, "steps": steps}
+        for name, values in fields.items():  # the frames restart from the seeded state
+            getattr(grid, name).data.copy_(torch.from_numpy(values))
+        grid.pressure.zero_()
+        stepper = Stepper(grid, recipe)
+        renderer = FrameRenderer(view, recipe.render, derived.cells, normal_layout, device)
+        thickness_px, heat_px, total = [], [], []
+        for frame in range(frames):
+            for n in range(4):
+                stepper.step((4 * frame + n) * dt, dt)
+            image = renderer.render(grid).astype(np.float64)
+            want = frames64[frame]
+            heat_scale = max(float(np.abs(want[..., 0]).max()), 1e-30)
+            thickness_px.append(float(np.abs(image[..., 1] - want[..., 1]).max()))
+            heat_px.append(float(np.abs(image[..., 0] - want[..., 0]).max()) / heat_scale)
+            total.append(abs(float(image[..., 1].sum()) - float(want[..., 1].sum())) / float(want[..., 1].sum()))
+        entry.update({"thickness_max_pixel_vs_fp64": thickness_px, "heat_max_pixel_vs_fp64": heat_px,
+                      "total_thickness_relative_vs_fp64": total})
+        out[label] = entry
         if label == "f32":
             multigrid = Multigrid(grid, recipe.solver.multigrid_cycles, recipe.solver.multigrid_sweeps)
             compute_divergence(grid)
@@ -453,37 +465,16 @@ def large_mixed_variant(device: str, steps: int = 8, frames: int = 2) -> dict:
             out["projection"] = {"rel_tol": 1e-7, "corrections": refinement.corrections, "ratio": refinement.ratio,
                                  "float_ratio": refinement.float_ratio,
                                  "ms_with_host_syncs": (time.perf_counter() - start) * 1e3}
-            grid.pressure.zero_()
-            renderer = FrameRenderer(view, recipe.render, derived.cells, recipe.output.channels, device)
-            renderer.render(grid)
+            march = FrameRenderer(square_view(sheet_domain_view(recipe, derived), 512), recipe.render, derived.cells,
+                                  recipe.output.channels, device)
+            march.render(grid)
             out["march_512x512_ms"] = device_ms(lambda: (
-                renderer.prepare(grid.smoke.data, grid.info.cell_m),
-                renderer.march(grid.smoke.data, grid.temperature.data, grid.info, renderer.view_params,
-                               renderer.image)))
-        stepper = Stepper(grid, recipe)
-        for n in range(3):  # warm-up: the solve's graph capture, allocations
-            stepper.step(n * derived.dt_s, derived.dt_s)
-        ms = device_ms(lambda: [stepper.step((3 + n) * derived.dt_s, derived.dt_s) for n in range(steps)])
-        out[label] = {"value": math.prod(cells) * steps / (ms / 1e3) / 1e6, "unit": METRIC, "steps": steps}
-        for name, values in fields.items():  # the frames restart from the seeded state
-            getattr(grid, name).data.copy_(values)
-        grid.pressure.zero_()
-        stepper = Stepper(grid, recipe)
-        renderer = FrameRenderer(view, recipe.render, derived.cells, recipe.output.channels, device)
-        rendered = []
-        for frame in range(frames):
-            for n in range(4):
-                stepper.step((4 * frame + n) * derived.dt_s, derived.dt_s)
-            rendered.append(renderer.render(grid))
-        runs[label] = rendered
+                march.prepare(grid.smoke.data, grid.info.cell_m),
+                march.march(grid.smoke.data, grid.temperature.data, grid.info, march.view_params, march.image)))
         del grid, stepper, renderer
         torch.cuda.empty_cache()
-    heat_scale = [max(float(np.abs(f[..., 0]).max()), 1e-30) for f in runs["f32"]]
-    out["bf16"]["thickness_difference_vs_f32"] = [float(np.abs(a[..., 1] - b[..., 1]).max())
-                                                  for a, b in zip(runs["bf16"], runs["f32"])]
-    out["bf16"]["heat_difference_vs_f32"] = [float(np.abs(a[..., 0] - b[..., 0]).max()) / s
-                                             for a, b, s in zip(runs["bf16"], runs["f32"], heat_scale)]
-    out["bf16"]["ratio_to_f32"] = out["bf16"]["value"] / out["f32"]["value"]
+    for label in ("bf16", "f16"):
+        out[label]["ratio_to_f32"] = out[label]["value"] / out["f32"]["value"]
     return out
 
 
@@ -712,10 +703,9 @@ def main():
         "clocks": clocks.summary(),
     }
     if not args.no_variants:
-        line["variants"] = {"storage": storage_variants(recipe, derived, fields, args.steps, device),
-                            "batched": batched_variant(device), "adjoint": adjoint_variant(device),
-                            "operators": operators_variant(device),
-                            "large_mixed": large_mixed_variant(device), "preview_run": preview_run_variant(device)}
+        line["variants"] = {"mixed": mixed_variant(device, fields), "batched": batched_variant(device),
+                            "adjoint": adjoint_variant(device), "operators": operators_variant(device),
+                            "preview_run": preview_run_variant(device)}
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         line["cpu_baseline"] = cpu_baseline(recipe, derived, fields)
     if rank == 0:

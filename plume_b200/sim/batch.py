@@ -72,6 +72,7 @@ class Batch:
         """`initial_state(index, grid)`, when given, fills an instance's fields before its first block (on the
         current stream)."""
         self.device = device
+        self.initial_state = initial_state
         self.instances: list[_Instance] = []
         current = torch.cuda.current_stream(device)
         for index, recipe in enumerate(recipes):
@@ -120,8 +121,40 @@ class Batch:
         inst.next_block += 1
         inst.ready = None
 
-    def run(self, capture: BatchCapture | None = None) -> list[StepLog]:
-        """Runs every instance to its last frame; returns each instance's StepLog (run.py's record)."""
+    def reset(self) -> None:
+        """Puts every instance back at its start (fields and pressure zero, temperature ambient, then
+        `initial_state`), keeping its arrays, so that a second run repeats the first with the allocations and
+        the pressure solves' CUDA graphs already in place."""
+        current = torch.cuda.current_stream(self.device)
+        for inst in self.instances:
+            current.wait_stream(inst.stream)
+        for index, inst in enumerate(self.instances):
+            grid = inst.grid
+            for field in (*grid.velocity_fields(), grid.smoke, grid.temperature):
+                for array in (field.data, field.hat, field.next):
+                    array.zero_()
+            for array in (grid.temperature.data, grid.temperature.hat, grid.temperature.next):
+                array.fill_(inst.recipe.domain.ambient_k)
+            grid.pressure.zero_()
+            grid.divergence.zero_()
+            if self.initial_state is not None:
+                self.initial_state(index, grid)
+            inst.next_block, inst.base_done, inst.warmup_steps, inst.ready = 0, 0, 0, None
+            inst.frame_steps = []
+        for inst in self.instances:
+            inst.stream.wait_stream(current)
+
+    def run(self, capture: BatchCapture | None = None, sequential: bool = False) -> list[StepLog]:
+        """Runs every instance to its last frame; returns each instance's StepLog (run.py's record). With
+        `sequential` the instances run one after another, each to its end before the next starts (the plain
+        one-at-a-time schedule on the same arrays)."""
+        if sequential:
+            for index, inst in enumerate(self.instances):
+                while not inst.done:
+                    self._request_speed(inst)
+                    inst.ready.synchronize()
+                    self._run_block(index, inst, capture)
+            return self._logs()
         for inst in self.instances:
             if not inst.done:
                 self._request_speed(inst)
@@ -137,6 +170,9 @@ class Batch:
             active = [(i, inst) for i, inst in active if not inst.done]
             if not progressed and active:
                 active[0][1].ready.synchronize()  # nothing landed yet: wait for the oldest request
+        return self._logs()
+
+    def _logs(self) -> list[StepLog]:
         for inst in self.instances:
             torch.cuda.current_stream(self.device).wait_stream(inst.stream)
         return [StepLog(inst.warmup_steps, tuple(inst.frame_steps), inst.derived.steps_per_frame,

@@ -70,3 +70,27 @@ def test_batch_waits_for_its_setup_on_a_delayed_stream(cuda_device):
     assert logs == logs_alone
     for key, values in alone.items():
         assert torch.equal(together[key], values), key
+
+
+def test_a_reset_batch_repeats_its_run_in_either_schedule(cuda_device):
+    """Batch.reset puts every instance back at its start: a second run, concurrent or one instance after
+    another, gives the first run's step counts and frames byte for byte."""
+    import torch
+
+    from plume_b200.sim.batch import Batch
+
+    recipes = batched_recipes(count=4, frames=3, seed=11, grids=SMALL_GRIDS)
+    runs = []
+    batch = Batch(recipes, "cuda:0", initial_state=seeded)
+    for sequential in (False, True, False):
+        frames = {}
+        logs = batch.run(capture=lambda i, f, g: frames.__setitem__((i, f), g.smoke.data.clone()),
+                         sequential=sequential)
+        torch.cuda.synchronize()
+        runs.append((logs, frames))
+        batch.reset()
+    for logs, frames in runs[1:]:
+        assert logs == runs[0][0]
+        assert sorted(frames) == sorted(runs[0][1])
+        for key, values in runs[0][1].items():
+            assert torch.equal(frames[key], values), key
