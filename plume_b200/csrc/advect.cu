@@ -544,7 +544,7 @@ __device__ __forceinline__ void march(const Args<T>& A, int seg, float* sm) {
           sum_next += value;
         }
         if (G == 3 && f == 1 && A.dissipate) value = A.ambient + (to_f<T>(from_f<T>(value)) - A.ambient) * A.heat_keep;
-        st_f(A.next[f] + out, value);
+        st_f(A.next[G == 3 ? f : G] + out, value);
       }
     }
 #pragma unroll
