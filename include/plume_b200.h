@@ -476,6 +476,29 @@ int plume_thickness_adjoint(const PlumeGridInfo* info, const PlumeViewParams* vi
                             const float* target, int32_t height, int32_t width, float* thickness, double* loss,
                             float* a_smoke, void* stream);
 
+/* ---- the velocity path of the adjoint (no counterpart in the reference, which has no derivatives) ----------
+ * plume_maccormack_adjoint: for next = MacCormack(data) advected by (u, v, w) (advect.py:59-68) with `hat` the
+ * forward semi-Lagrangian values, adds d loss / d data to a_data given a_next; a_hat is the derivative of hat
+ * (it must hold any derivative known for hat already, e.g. the smoke budget's term). With a_u, a_v, a_w (all or
+ * none) it also adds the derivatives with respect to the advecting velocity, through both traces' endpoints
+ * and midpoints. Any field shape and offset (cells or faces). Atomic adds: last bits vary between runs.
+ * plume_buoyancy_adjoint (forces.py:13-23): a_temperature (and a_smoke with a smoke weight) receive a_v's share;
+ * *grad_heat_buoyancy (device double) += d loss / d heat_buoyancy.
+ * plume_drag_adjoint (forces.py:34-48): *grad_drag += d loss / d drag_per_s (u, v, w: the velocity before drag,
+ * keep = exp(-drag dt)), then a_u, a_v, a_w *= keep.
+ * plume_emit_adjoint (emitters.py:90-121): the temperature and velocity blends scale their derivatives by 1 - b. */
+int plume_maccormack_adjoint(const PlumeGridInfo* info, const int32_t shape[3], const float offset[3], const float* data,
+                             const float* hat, const float* u, const float* v, const float* w, const float* a_next,
+                             float* a_data, float* a_hat, float* a_u, float* a_v, float* a_w, float dt_over_cell,
+                             float outside, int32_t uses_outside, void* stream);
+int plume_buoyancy_adjoint(const PlumeGridInfo* info, const float* a_v, const float* smoke, const float* temperature,
+                           float* a_smoke, float* a_temperature, float gravity, float heat_buoyancy,
+                           float smoke_weight, float ambient_k, float dt, double* grad_heat_buoyancy, void* stream);
+int plume_drag_adjoint(const PlumeGridInfo* info, float* a_u, float* a_v, float* a_w, const float* u, const float* v,
+                       const float* w, const float wind[3], float keep, float dt, double* grad_drag, void* stream);
+int plume_emit_adjoint(const PlumeGridInfo* info, float* a_temperature, float* a_u, float* a_v, float* a_w,
+                       const PlumeEmitter* emitters, int32_t count, int32_t seed, float time_s, float dt, void* stream);
+
 #ifdef __cplusplus
 }
 #endif

@@ -280,6 +280,208 @@ __global__ void k_thickness_adjoint(PlumeGridInfo info, PlumeViewParams view, fl
   }
 }
 
+// ---- the velocity path (no reference counterpart) ------------------------------------------------------------
+// The derivatives with respect to the advecting velocity and the forces, for gradients with respect to the
+// buoyancy and drag scalars. Traces are recomputed with the forward kernels' functions; the linearisation is
+// that of the reference's formulas (trace: advect.py:16-21, samples: sample.py:10-82).
+
+// sample_index_space at g and its gradient with respect to g (index units): along an axis where the clamp holds
+// the coordinate at an end the sample does not move, so that component is 0.
+__device__ __forceinline__ float sample_and_gradient(const float* __restrict__ f, const Dims& d, F3 g, F3& grad) {
+  const Axis1 x = axis_of(g[0], d.n0, d.n1 * d.n2), y = axis_of(g[1], d.n1, d.n2), z = axis_of(g[2], d.n2, 1);
+  const float* p = f + (x.i0 * d.n1 + y.i0) * d.n2 + z.i0;
+  const float a000 = p[0], a100 = p[x.step], a010 = p[y.step], a110 = p[x.step + y.step];
+  const float a001 = p[z.step], a101 = p[x.step + z.step], a011 = p[y.step + z.step];
+  const float a111 = p[x.step + y.step + z.step];
+  const float c00 = lerp_w(a000, a100, x), c10 = lerp_w(a010, a110, x);
+  const float c01 = lerp_w(a001, a101, x), c11 = lerp_w(a011, a111, x);
+  const float e0 = lerp_w(c00, c10, y), e1 = lerp_w(c01, c11, y);
+  const bool free_x = g[0] >= 0.0f && g[0] <= (float)(d.n0 - 1);
+  const bool free_y = g[1] >= 0.0f && g[1] <= (float)(d.n1 - 1);
+  const bool free_z = g[2] >= 0.0f && g[2] <= (float)(d.n2 - 1);
+  grad[0] = free_x ? lerp_w(lerp_w(a100 - a000, a110 - a010, y), lerp_w(a101 - a001, a111 - a011, y), z) : 0.0f;
+  grad[1] = free_y ? lerp_w(c10 - c00, c11 - c01, z) : 0.0f;
+  grad[2] = free_z ? e1 - e0 : 0.0f;
+  return lerp_w(e0, e1, z);
+}
+
+__device__ __forceinline__ F3 component_offset(int c) {
+  return f3(c == 0 ? 0.0f : 0.5f, c == 1 ? 0.0f : 0.5f, c == 2 ? 0.0f : 0.5f);
+}
+
+// Scatters a velocity derivative w (one value per component) at point m to the components' trilinear corners.
+__device__ __forceinline__ void scatter_velocity(float* const a_vel[3], const Vel& vel, F3 m, F3 w) {
+  const Dims dims[3] = {vel.du, vel.dv, vel.dw};
+#pragma unroll
+  for (int c = 0; c < 3; ++c)
+    if (w[c] != 0.0f) scatter(a_vel[c], corners_of(dims[c], sub3(m, component_offset(c))), w[c]);
+}
+
+// The adjoint of end = p - tau V(mid), mid = p - tau/2 V(p) (trace, advect.py:16-21) for d loss / d end = lambda:
+// the velocity's derivative at mid, and through mid's own dependence on V(p), at p.
+__device__ __forceinline__ void trace_adjoint(const Vel& vel, F3 p, float tau, F3 lambda, float* const a_vel[3]) {
+  if (lambda[0] == 0.0f && lambda[1] == 0.0f && lambda[2] == 0.0f) return;
+  const F3 vp = velocity_at_node(vel, p);
+  const F3 mid = sub3(p, mul3(vp, 0.5f * tau));
+  const float* arrays[3] = {vel.u, vel.v, vel.w};
+  const Dims dims[3] = {vel.du, vel.dv, vel.dw};
+  F3 jac[3];  // jac[c][a] = d V_c / d x_a at mid
+#pragma unroll
+  for (int c = 0; c < 3; ++c) sample_and_gradient(arrays[c], dims[c], sub3(mid, component_offset(c)), jac[c]);
+  const F3 a_vm = mul3(lambda, -tau);
+  scatter_velocity(a_vel, vel, mid, a_vm);
+  F3 a_mid = f3(0.0f, 0.0f, 0.0f);
+#pragma unroll
+  for (int c = 0; c < 3; ++c) a_mid = add3(a_mid, mul3(jac[c], a_vm[c]));
+  scatter_velocity(a_vel, vel, p, mul3(a_mid, -0.5f * tau));
+}
+
+struct AdjField {
+  const float* data;   // the field before advection
+  const float* hat;    // its forward semi-Lagrangian values
+  Dims d;
+  F3 offset;
+  float outside;
+  int uses_outside;
+};
+
+// MacCormack adjoint, part 1 for any field (cells or faces): the clamp's branch, the correction's own terms, the
+// backward sample's transpose into a_hat and, with a_vel, the backward trace's velocity derivative.
+__global__ void k_mac_adj_correct(PlumeGridInfo info, Vel vel, AdjField fd, const float* __restrict__ a_next,
+                                  float* __restrict__ a_data, float* __restrict__ a_hat, float* a_u, float* a_v,
+                                  float* a_w, float dt_over_cell) {
+  const int i = blockIdx.z, j = blockIdx.y * blockDim.y + threadIdx.y, k = blockIdx.x * blockDim.x + threadIdx.x;
+  const Dims d = fd.d;
+  if (j >= d.n1 || k >= d.n2) return;
+  const int c = at(d, i, j, k);
+  const float g_next = a_next[c];
+  if (g_next == 0.0f) return;
+  const F3 p = add3(f3((float)i, (float)j, (float)k), fd.offset);
+  const F3 vp = velocity_at_node(vel, p);
+  const F3 src = trace_from(vel, p, vp, dt_over_cell);
+  const F3 back_src = trace_from(vel, p, vp, -dt_over_cell);
+  const bool src_outside = fd.uses_outside == 1 && is_outside_open_face(src, info);
+  const bool back_outside = fd.uses_outside == 1 && is_outside_open_face(back_src, info);
+  const F3 gb = sub3(back_src, fd.offset);
+  const float back = back_outside ? fd.outside : sample_index_space(fd.hat, d, gb);
+  const float corrected = __ldg(fd.hat + c) + 0.5f * (__ldg(fd.data + c) - back);
+  float lo = fd.outside, hi = fd.outside;
+  int lo_idx = -1, hi_idx = -1;
+  if (!src_outside) range_corners(fd.data, d, sub3(src, fd.offset), lo_idx, hi_idx, lo, hi);
+  if (corrected < lo) {
+    if (lo_idx >= 0) atomicAdd(a_data + lo_idx, g_next);
+    return;
+  }
+  if (corrected > hi) {
+    if (hi_idx >= 0) atomicAdd(a_data + hi_idx, g_next);
+    return;
+  }
+  atomicAdd(a_hat + c, g_next);
+  atomicAdd(a_data + c, 0.5f * g_next);
+  if (back_outside) return;
+  const float a_back = -0.5f * g_next;
+  scatter(a_hat, corners_of(d, gb), a_back);
+  if (!a_u) return;
+  F3 grad;
+  sample_and_gradient(fd.hat, d, gb, grad);
+  float* a_vel[3] = {a_u, a_v, a_w};
+  trace_adjoint(vel, p, -dt_over_cell, mul3(grad, a_back), a_vel);
+}
+
+// MacCormack adjoint, part 2: the forward sample's transpose, a_data += sample^T(a_hat), and with a_vel the
+// forward trace's velocity derivative.
+__global__ void k_mac_adj_forward(PlumeGridInfo info, Vel vel, AdjField fd, const float* __restrict__ a_hat,
+                                  float* __restrict__ a_data, float* a_u, float* a_v, float* a_w, float dt_over_cell) {
+  const int i = blockIdx.z, j = blockIdx.y * blockDim.y + threadIdx.y, k = blockIdx.x * blockDim.x + threadIdx.x;
+  const Dims d = fd.d;
+  if (j >= d.n1 || k >= d.n2) return;
+  const float g = a_hat[at(d, i, j, k)];
+  if (g == 0.0f) return;
+  const F3 p = add3(f3((float)i, (float)j, (float)k), fd.offset);
+  const F3 src = trace_from(vel, p, velocity_at_node(vel, p), dt_over_cell);
+  if (fd.uses_outside == 1 && is_outside_open_face(src, info)) return;
+  const F3 gs = sub3(src, fd.offset);
+  scatter(a_data, corners_of(d, gs), g);
+  if (!a_u) return;
+  F3 grad;
+  sample_and_gradient(fd.data, d, gs, grad);
+  float* a_vel[3] = {a_u, a_v, a_w};
+  trace_adjoint(vel, p, dt_over_cell, mul3(grad, g), a_vel);
+}
+
+// Block sums of a per-thread double into *out (one atomic per block).
+__device__ __forceinline__ void block_add(double value, double* out) {
+  __shared__ double slot[ADJ_THREADS];
+  const int t = threadIdx.y * blockDim.x + threadIdx.x;
+  slot[t] = value;
+  __syncthreads();
+  for (int h = ADJ_THREADS / 2; h >= 1; h >>= 1) {
+    if (t < h) slot[t] = slot[t] + slot[t + h];
+    __syncthreads();
+  }
+  if (t == 0 && slot[0] != 0.0) atomicAdd(out, slot[0]);
+}
+
+// buoyancy_kernel's adjoint (forces.py:13-23) for v += g (hb (T - Ta) / Ta - ws s) dt with T, s averaged over
+// the face's two cells: a_T, a_s receive a_v's share; *grad_hb += sum a_v g (T - Ta) / Ta dt. a_v is unchanged.
+__global__ void k_buoyancy_adjoint(PlumeGridInfo info, const float* __restrict__ a_v, const float* __restrict__ smoke,
+                                   const float* __restrict__ temperature, float* __restrict__ a_smoke,
+                                   float* __restrict__ a_temperature, float gravity, float heat_buoyancy,
+                                   float smoke_weight, float ambient, float dt, double* grad_hb) {
+  const int ny = info.dims[1], nz = info.dims[2];
+  const int i = blockIdx.z, j = blockIdx.y * blockDim.y + threadIdx.y, k = blockIdx.x * blockDim.x + threadIdx.x;
+  double part = 0.0;
+  if (j <= ny && k < nz) {
+    const float a = a_v[(i * (ny + 1) + j) * nz + k];
+    if (a != 0.0f) {
+      const int below = imax_(j - 1, 0), above = imin_(j, ny - 1);
+      const int cb = (i * ny + below) * nz + k, ca = (i * ny + above) * nz + k;
+      const float heat = 0.5f * (temperature[cb] + temperature[ca]);
+      const float a_heat = a * gravity * dt * heat_buoyancy / ambient;
+      atomicAdd(a_temperature + cb, 0.5f * a_heat);
+      atomicAdd(a_temperature + ca, 0.5f * a_heat);
+      if (smoke_weight != 0.0f && a_smoke) {
+        const float a_density = -a * gravity * dt * smoke_weight;
+        atomicAdd(a_smoke + cb, 0.5f * a_density);
+        atomicAdd(a_smoke + ca, 0.5f * a_density);
+      }
+      part = (double)a * (double)gravity * (double)dt * ((double)heat - (double)ambient) / (double)ambient;
+    }
+  }
+  block_add(part, grad_hb);
+}
+
+// drag_kernel's adjoint (forces.py:34-48) for f = wind + (f_before - wind) keep over the three face arrays
+// (blockIdx.z segments as the face kernels): *grad_drag += sum a_f (f_before - wind) (-dt keep) (keep =
+// exp(-drag dt)), then a_f *= keep.
+__global__ void k_drag_adjoint(PlumeGridInfo info, float* __restrict__ a_u, float* __restrict__ a_v,
+                               float* __restrict__ a_w, const float* __restrict__ u, const float* __restrict__ v,
+                               const float* __restrict__ w, float3 wind, float keep, float dt, double* grad_drag) {
+  const int nx = info.dims[0], ny = info.dims[1], nz = info.dims[2];
+  int slab = blockIdx.z, axis = 0;
+  if (slab >= nx + 1) {
+    slab -= nx + 1;
+    axis = 1;
+    if (slab >= nx) {
+      slab -= nx;
+      axis = 2;
+    }
+  }
+  const int j = blockIdx.y * blockDim.y + threadIdx.y, k = blockIdx.x * blockDim.x + threadIdx.x;
+  const int n1 = ny + (axis == 1), n2 = nz + (axis == 2);
+  double part = 0.0;
+  if (j < n1 && k < n2) {
+    const long c = ((long)slab * n1 + j) * n2 + k;
+    float* a = axis == 0 ? a_u : (axis == 1 ? a_v : a_w);
+    const float* f = axis == 0 ? u : (axis == 1 ? v : w);
+    const float target = axis == 0 ? wind.x : (axis == 1 ? wind.y : wind.z);
+    const float g = a[c];
+    part = (double)g * ((double)f[c] - (double)target) * (-(double)dt * (double)keep);
+    a[c] = g * keep;
+  }
+  block_add(part, grad_drag);
+}
+
 }  // namespace plume
 
 using namespace plume;
@@ -343,4 +545,50 @@ extern "C" int plume_thickness_adjoint(const PlumeGridInfo* info, const PlumeVie
   k_thickness_adjoint<<<grid, block, 0, as_stream(stream)>>>(*info, *view, opacity, smoke, target, height, width,
                                                              thickness, loss, a_smoke);
   return launch_status("thickness adjoint");
+}
+
+extern "C" int plume_maccormack_adjoint(const PlumeGridInfo* info, const int32_t shape[3], const float offset[3],
+                                       const float* data, const float* hat, const float* u, const float* v,
+                                       const float* w, const float* a_next, float* a_data, float* a_hat, float* a_u,
+                                       float* a_v, float* a_w, float dt_over_cell, float outside, int32_t uses_outside,
+                                       void* stream) {
+  ADJ_CHECK(info && shape && offset && data && hat && u && v && w && a_next && a_data && a_hat,
+            "maccormack_adjoint: null argument");
+  ADJ_CHECK((a_u == nullptr) == (a_v == nullptr) && (a_v == nullptr) == (a_w == nullptr),
+            "maccormack_adjoint: give all three velocity adjoints or none");
+  cudaStream_t st = as_stream(stream);
+  AdjField fd{data, hat, Dims{shape[0], shape[1], shape[2]}, f3(offset[0], offset[1], offset[2]), outside,
+              uses_outside};
+  const Vel vel = make_vel(u, v, w, info->dims);
+  const dim3 grid = cell_grid(fd.d.n0, fd.d.n1, fd.d.n2);
+  k_mac_adj_correct<<<grid, cell_block(), 0, st>>>(*info, vel, fd, a_next, a_data, a_hat, a_u, a_v, a_w, dt_over_cell);
+  int status = launch_status("MacCormack adjoint (correction, velocity)");
+  if (status != PLUME_OK) return status;
+  k_mac_adj_forward<<<grid, cell_block(), 0, st>>>(*info, vel, fd, a_hat, a_data, a_u, a_v, a_w, dt_over_cell);
+  return launch_status("MacCormack adjoint (forward sample, velocity)");
+}
+
+extern "C" int plume_buoyancy_adjoint(const PlumeGridInfo* info, const float* a_v, const float* smoke,
+                                      const float* temperature, float* a_smoke, float* a_temperature, float gravity,
+                                      float heat_buoyancy, float smoke_weight, float ambient_k, float dt,
+                                      double* grad_heat_buoyancy, void* stream) {
+  ADJ_CHECK(info && a_v && smoke && temperature && a_temperature && grad_heat_buoyancy,
+            "buoyancy_adjoint: null argument");
+  const int nx = info->dims[0], ny = info->dims[1], nz = info->dims[2];
+  k_buoyancy_adjoint<<<cell_grid(nx, ny + 1, nz), cell_block(), 0, as_stream(stream)>>>(
+      *info, a_v, smoke, temperature, a_smoke, a_temperature, gravity, heat_buoyancy, smoke_weight, ambient_k, dt,
+      grad_heat_buoyancy);
+  return launch_status("buoyancy adjoint");
+}
+
+extern "C" int plume_drag_adjoint(const PlumeGridInfo* info, float* a_u, float* a_v, float* a_w, const float* u,
+                                  const float* v, const float* w, const float wind[3], float keep, float dt,
+                                  double* grad_drag, void* stream) {
+  ADJ_CHECK(info && a_u && a_v && a_w && u && v && w && wind && grad_drag, "drag_adjoint: null argument");
+  const int nx = info->dims[0], ny = info->dims[1], nz = info->dims[2];
+  const dim3 grid((nz + 1 + TZ - 1) / TZ, (ny + 1 + TY - 1) / TY, (nx + 1) + nx + nx);
+  k_drag_adjoint<<<grid, cell_block(), 0, as_stream(stream)>>>(*info, a_u, a_v, a_w, u, v, w,
+                                                              make_float3(wind[0], wind[1], wind[2]), keep, dt,
+                                                              grad_drag);
+  return launch_status("drag adjoint");
 }

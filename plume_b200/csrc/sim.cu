@@ -160,6 +160,45 @@ __global__ void k_emit(PlumeGridInfo info, T* __restrict__ smoke, T* __restrict_
   }
 }
 
+// The adjoint of k_emit for the temperature and velocity blends (no reference counterpart): each blend
+// T = lerp(T, target, b) passes (1 - b) of the derivative back; the smoke's addition passes it unchanged. Same
+// box and segments as k_emit.
+__global__ void k_emit_adjoint(PlumeGridInfo info, float* __restrict__ a_temperature, float* __restrict__ a_u,
+                               float* __restrict__ a_v, float* __restrict__ a_w, EmitterSet set, int seed, float time_s,
+                               float dt, int3 lo, int3 n) {
+  const int nx = info.dims[0], ny = info.dims[1], nz = info.dims[2];
+  int slab = blockIdx.z;
+  int part = 0;
+  if (slab >= n.x) { slab -= n.x; part = 1; }
+  if (part == 1 && slab >= n.x + 1) { slab -= n.x + 1; part = 2; }
+  if (part == 2 && slab >= n.x) { slab -= n.x; part = 3; }
+  const int i = lo.x + slab;
+  const int j = lo.y + blockIdx.y * blockDim.y + threadIdx.y;
+  const int k = lo.z + blockIdx.x * blockDim.x + threadIdx.x;
+  F3 x;
+  float* target;
+  if (part == 0) {
+    if (i >= nx || j >= ny || k >= nz || j >= lo.y + n.y || k >= lo.z + n.z) return;
+    x = world_position(info, add3(f3((float)i, (float)j, (float)k), f3(0.5f, 0.5f, 0.5f)));
+    target = a_temperature + (i * ny + j) * nz + k;
+  } else {
+    const int axis = part - 1;
+    const int n0 = nx + (axis == 0), n1 = ny + (axis == 1), n2 = nz + (axis == 2);
+    if (i >= n0 || j >= n1 || k >= n2 || j > lo.y + n.y || k > lo.z + n.z) return;
+    const F3 offset = axis == 0 ? f3(0.0f, 0.5f, 0.5f) : (axis == 1 ? f3(0.5f, 0.0f, 0.5f) : f3(0.5f, 0.5f, 0.0f));
+    x = world_position(info, add3(f3((float)i, (float)j, (float)k), offset));
+    target = (axis == 0 ? a_u : (axis == 1 ? a_v : a_w)) + (i * n1 + j) * n2 + k;
+  }
+  float keep = 1.0f;
+  for (int e_index = 0; e_index < set.count; ++e_index) {
+    const PlumeEmitter& e = set.e[e_index];
+    if (!(time_s >= e.start_s && time_s < e.end_s)) continue;
+    const float amount = coverage(e, x, seed);
+    if (amount > 0.0f) keep = keep * (1.0f - blend_factor(amount, dt));
+  }
+  if (keep != 1.0f) *target = *target * keep;
+}
+
 // The cells (inclusive index range per axis) that can lie within reach of the emitters, with a 2-cell margin
 // for rounding; false when none is inside the grid.
 static bool emitter_box(const PlumeGridInfo& info, const PlumeEmitter* e, int count, int lo[3], int hi[3]) {
@@ -1153,6 +1192,32 @@ extern "C" int plume_emit(const PlumeGridInfo* info, float* smoke, float* temper
   CHECK_ARG(count >= 0 && (count == 0 || emitters), "emit: bad emitter list");
   CHECK_ARG(valid_dims(info->dims), "emit: bad dims");
   return launch_emit(*info, smoke, temperature, u, v, w, emitters, count, seed, time_s, dt, as_stream(stream));
+}
+
+extern "C" int plume_emit_adjoint(const PlumeGridInfo* info, float* a_temperature, float* a_u, float* a_v, float* a_w,
+                                  const PlumeEmitter* emitters, int32_t count, int32_t seed, float time_s, float dt,
+                                  void* stream) {
+  CHECK_ARG(info && a_temperature && a_u && a_v && a_w, "emit_adjoint: null argument");
+  CHECK_ARG(count >= 0 && (count == 0 || emitters), "emit_adjoint: bad emitter list");
+  CHECK_ARG(valid_dims(info->dims), "emit_adjoint: bad dims");
+  cudaStream_t st = as_stream(stream);
+  std::vector<PlumeEmitter> active;
+  for (int n = 0; n < count; ++n)
+    if (time_s >= emitters[n].start_s && time_s < emitters[n].end_s) active.push_back(emitters[n]);
+  for (size_t first = 0; first < active.size(); first += PLUME_MAX_EMITTERS) {
+    EmitterSet set;
+    set.count = (int)std::min<size_t>(PLUME_MAX_EMITTERS, active.size() - first);
+    for (int n = 0; n < set.count; ++n) set.e[n] = active[first + n];
+    int lo[3], hi[3];
+    if (!emitter_box(*info, set.e, set.count, lo, hi)) continue;
+    const int3 box_lo = make_int3(lo[0], lo[1], lo[2]);
+    const int3 box_n = make_int3(hi[0] - lo[0] + 1, hi[1] - lo[1] + 1, hi[2] - lo[2] + 1);
+    dim3 grid((box_n.z + 1 + TZ - 1) / TZ, (box_n.y + 1 + TY - 1) / TY, box_n.x + (box_n.x + 1) + box_n.x + box_n.x);
+    k_emit_adjoint<<<grid, cell_block(), 0, st>>>(*info, a_temperature, a_u, a_v, a_w, set, seed, time_s, dt, box_lo,
+                                                   box_n);
+    CHECK_LAUNCH("emit adjoint");
+  }
+  return PLUME_OK;
 }
 
 extern "C" int plume_buoyancy(const PlumeGridInfo* info, float* v, const float* smoke, const float* temperature,
