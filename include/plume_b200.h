@@ -487,6 +487,13 @@ int plume_thickness_adjoint(const PlumeGridInfo* info, const PlumeViewParams* vi
  * plume_drag_adjoint (forces.py:34-48): *grad_drag += d loss / d drag_per_s (u, v, w: the velocity before drag,
  * keep = exp(-drag dt)), then a_u, a_v, a_w *= keep.
  * plume_emit_adjoint (emitters.py:90-121): the temperature and velocity blends scale their derivatives by 1 - b. */
+/* plume_budget_adjoint (conserve.py:45-52 then dissipate.py:10-15 for the smoke): given a_out, the derivative
+ * of the smoke after the budget's rescale and dissipation by `keep`, writes a_next (of next before the rescale)
+ * and starts a_data and a_hat with the rescale factor's uniform terms (from the three totals). `partial` needs
+ * 1024 doubles, `coeffs` 4. */
+int plume_budget_adjoint(const PlumeGridInfo* info, const float* next_pre, const double* totals, float keep,
+                         const float* a_out, float* a_next, float* a_data, float* a_hat, double* partial,
+                         double* coeffs, void* stream);
 int plume_maccormack_adjoint(const PlumeGridInfo* info, const int32_t shape[3], const float offset[3], const float* data,
                              const float* hat, const float* u, const float* v, const float* w, const float* a_next,
                              float* a_data, float* a_hat, float* a_u, float* a_v, float* a_w, float dt_over_cell,

@@ -161,6 +161,7 @@ SIGNATURES = {
     "plume_source_grad": [_P, _SHAPE, _P, _SHAPE, _SHAPE, _F, _P],
     "plume_smoke_adjoint": [_INFO, _P, _P, _P, _P, _P, _P, _P, _F, _F, _P, _P, _P, _P, _P, _P, _P],
     "plume_thickness_adjoint": [_INFO, ctypes.POINTER(PlumeViewParams), _F, _P, _P, _I, _I, _P, _P, _P, _P],
+    "plume_budget_adjoint": [_INFO, _P, _P, _F, _P, _P, _P, _P, _P, _P, _P],
     "plume_maccormack_adjoint": [_INFO, _SHAPE, _F3P, _P, _P, _P, _P, _P, _P, _P, _P, _P, _P, _P, _F, _F, _I, _P],
     "plume_buoyancy_adjoint": [_INFO, _P, _P, _P, _P, _P, _F, _F, _F, _F, _F, _P, _P],
     "plume_drag_adjoint": [_INFO, _P, _P, _P, _P, _P, _P, _F3P, _F, _F, _P, _P],

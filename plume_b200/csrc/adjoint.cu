@@ -592,3 +592,21 @@ extern "C" int plume_drag_adjoint(const PlumeGridInfo* info, float* a_u, float* 
                                                               grad_drag);
   return launch_status("drag adjoint");
 }
+
+extern "C" int plume_budget_adjoint(const PlumeGridInfo* info, const float* next_pre, const double* totals, float keep,
+                                   const float* a_out, float* a_next, float* a_data, float* a_hat, double* partial,
+                                   double* coeffs, void* stream) {
+  ADJ_CHECK(info && next_pre && totals && a_out && a_next && a_data && a_hat && partial && coeffs,
+            "budget_adjoint: null argument");
+  cudaStream_t st = as_stream(stream);
+  const Dims d = dims_of(*info);
+  const long n = (long)d.n0 * d.n1 * d.n2;
+  const int blocks = (int)std::min<long>(adj_blocks(n), 1024);
+  k_dot_partials<<<blocks, ADJ_THREADS, 0, st>>>(a_out, next_pre, n, partial);
+  int status = launch_status("adjoint dot");
+  if (status != PLUME_OK) return status;
+  k_budget_adjoint_coeffs<<<1, 32, 0, st>>>(totals, partial, blocks, coeffs);
+  if ((status = launch_status("budget adjoint coefficients")) != PLUME_OK) return status;
+  k_budget_adjoint_apply<<<blocks, ADJ_THREADS, 0, st>>>(a_out, n, coeffs, keep, a_next, a_data, a_hat);
+  return launch_status("budget adjoint");
+}

@@ -1,0 +1,134 @@
+"""The adjoint through the velocity path (FlowFit): the gradient of the rendered-thickness loss with respect to
+heat_buoyancy and drag_per_s, whose effect reaches the smoke only through the velocity (buoyancy, drag,
+self-advection, projection, scalar advection), and with respect to the source field, with a smoke weight so
+that the smoke also pushes the velocity.
+
+Checks: each scalar's gradient against central differences of the same float32 model's loss, and of the FP64
+oracle's loss; the source gradient against central differences on the voxels with the largest gradient; and,
+without smoke weight, the source gradient equals SourceFit's (the smoke-only adjoint) where the velocity path
+adds nothing."""
+
+import dataclasses
+
+import numpy as np
+import pytest
+
+from oracle import oracle as O
+from plume_b200.recipe.derived import derive
+from plume_b200.workloads import plain_step_recipe
+
+pytestmark = pytest.mark.gpu
+
+CELLS = (20, 28, 20)
+SOURCE = (5, 5, 5)
+CORNER = (7, 2, 7)
+SUBSTEPS = 10
+CYCLES = 8  # forward V-cycles: the forward projection close to exact, as the adjoint's is
+SCALAR_RTOL = 1e-2      # against float32 central differences
+SCALAR_RTOL_FP64 = 2e-2
+SOURCE_RTOL = 2e-2
+
+
+def flow_recipe(smoke_weight=0.05, **forces):
+    recipe = plain_step_recipe(CELLS, cycles=CYCLES, frames=4, substeps=3)
+    f = dataclasses.replace(recipe.forces, vorticity_confinement=0.0, smoke_weight=smoke_weight, **forces)
+    return dataclasses.replace(recipe, forces=f, dissipation=dataclasses.replace(
+        recipe.dissipation, smoke_per_s=0.3, cooling_per_s=0.2))
+
+
+def oracle_loss(recipe, source, target, precision="f64"):
+    derived = derive(recipe)
+    d = recipe.domain
+
+    def add(grid, time_s, dt):
+        grid.smoke.data[CORNER[0]:CORNER[0] + SOURCE[0], CORNER[1]:CORNER[1] + SOURCE[1],
+                        CORNER[2]:CORNER[2] + SOURCE[2]] += source * dt
+
+    grid = O.make_grid(derived, d.cell_m, d.faces, d.ambient_k, precision)
+    stepper = O.Stepper(grid, recipe, before_step=add)
+    for n in range(SUBSTEPS):
+        stepper.step(n * derived.dt_s, derived.dt_s)
+    from plume_b200.render.camera import sheet_domain_view
+
+    view = sheet_domain_view(recipe, derived)
+    thickness = O.FrameRenderer(view, recipe.render, derived.cells, recipe.output.channels,
+                                precision).render(grid)[..., 1]
+    return float(((thickness - target) ** 2).sum()), thickness
+
+
+@pytest.fixture(scope="module")
+def case():
+    import torch
+
+    from plume_b200.adjoint import FlowFit
+
+    recipe = flow_recipe()
+    rng = np.random.default_rng(4)
+    source = rng.uniform(0.0, 1.0, SOURCE) * 20.0
+    target_recipe = dataclasses.replace(recipe, forces=dataclasses.replace(recipe.forces, heat_buoyancy=1.2))
+    _, target = oracle_loss(target_recipe, np.clip(source + rng.normal(0.0, 4.0, SOURCE), 0.0, None), 0.0)
+    fit = FlowFit(recipe, SOURCE, CORNER, SUBSTEPS, "cuda:0", checkpoint_every=4, adjoint_cycles=12)
+    src = torch.from_numpy(source.astype(np.float32))
+    tgt = torch.from_numpy(target.astype(np.float32))
+    loss, grad, scalars, _ = fit.loss_and_grad(src, tgt)
+    return recipe, source, target, fit, src, tgt, loss, grad.cpu().numpy().astype(np.float64), scalars
+
+
+@pytest.mark.parametrize("name,h", [("heat_buoyancy", 1e-2), ("drag_per_s", 1e-2)])
+def test_scalar_gradients_match_central_differences(cuda_device, case, name, h):
+    recipe, source, target, fit, src, tgt, loss, _, scalars = case
+    value = getattr(recipe.forces, name)
+    up = fit.with_forces(**{name: value + h}).loss(src, tgt)
+    down = fit.with_forces(**{name: value - h}).loss(src, tgt)
+    fd = (up - down) / (2.0 * h)
+    target_recipe = recipe
+    up64, _ = oracle_loss(dataclasses.replace(recipe, forces=dataclasses.replace(recipe.forces, **{name: value + 1e-3})),
+                          source, target)
+    down64, _ = oracle_loss(dataclasses.replace(recipe, forces=dataclasses.replace(recipe.forces, **{name: value - 1e-3})),
+                            source, target)
+    fd64 = (up64 - down64) / 2e-3
+    print(f"{name}: adjoint {scalars[name]:.6g}  float32 FD {fd:.6g}  FP64 FD {fd64:.6g}")
+    assert abs(scalars[name] - fd) <= SCALAR_RTOL * abs(fd)
+    assert abs(scalars[name] - fd64) <= SCALAR_RTOL_FP64 * abs(fd64)
+
+
+def test_source_gradient_matches_central_differences(cuda_device, case):
+    import torch
+
+    _, source, target, fit, src, tgt, _, grad, _ = case
+    scale = float(np.abs(grad).max())
+    picks = list(np.argsort(np.abs(grad).ravel())[-4:])
+    h = 2e-2 * float(source.max())
+    errors = []
+    for flat in picks:
+        index = np.unravel_index(flat, SOURCE)
+        up, down = source.copy(), source.copy()
+        up[index] += h
+        down[index] -= h
+        fd = (fit.loss(torch.from_numpy(up.astype(np.float32)), tgt) -
+              fit.loss(torch.from_numpy(down.astype(np.float32)), tgt)) / (2.0 * h)
+        errors.append(abs(grad[index] - fd) / scale)
+    print("source gradient errors (of the gradient's scale):", [f"{e:.2e}" for e in errors])
+    assert max(errors) <= SOURCE_RTOL
+
+
+def test_without_smoke_weight_the_source_gradient_is_the_smoke_adjoints(cuda_device):
+    import torch
+
+    from plume_b200.adjoint import FlowFit, SourceFit
+
+    recipe = flow_recipe(smoke_weight=0.0)
+    rng = np.random.default_rng(6)
+    source = torch.from_numpy((rng.uniform(0.0, 1.0, SOURCE) * 20.0).astype(np.float32))
+    derived = derive(recipe)
+    from plume_b200.render.camera import sheet_domain_view
+
+    view = sheet_domain_view(recipe, derived)
+    target = torch.full((view.height_px, view.width_px), 0.1, dtype=torch.float32)
+    _, flow_grad, scalars, _ = FlowFit(recipe, SOURCE, CORNER, SUBSTEPS, "cuda:0", checkpoint_every=4).loss_and_grad(
+        source, target)
+    _, smoke_grad, _ = SourceFit(recipe, SOURCE, CORNER, SUBSTEPS, "cuda:0", checkpoint_every=4).loss_and_grad(
+        source, target)
+    a, b = flow_grad.cpu().numpy(), smoke_grad.cpu().numpy()
+    assert np.abs(a - b).max() <= 1e-3 * np.abs(b).max()
+    assert all(np.isfinite(v) for v in scalars.values())
