@@ -37,15 +37,24 @@
 namespace plume {
 namespace mac {
 
-constexpr int TY = 16, TZ = 32, NT = TY * TZ;             // tile of one block: 512 elements per plane
-constexpr int RZ = TZ + 4, RY = TY + 4, RP = RY * RZ;     // staged plane: rows j0-2..j0+TY+1, cols k0-2..k0+TZ+1
-constexpr int HZ = TZ + 2, HY = TY + 2, HP = HY * HZ;     // hat plane: rows j0-1..j0+TY, cols k0-1..k0+TZ
-constexpr int HALO = HP - NT;                             // the hat plane's one-cell ring: 100 elements
+#ifndef PLUME_MAC_TY
+#define PLUME_MAC_TY 16
+#endif
+constexpr int TY = PLUME_MAC_TY, TZ = 32, NT = TY * TZ;   // tile of one block: TY x 32 elements per plane
+constexpr int BLOCKS_PER_SM = 1024 / NT;                // 512 threads: 2 blocks per SM, 256: 4
+// Plane strides are padded to a multiple of 32 floats, so that samples in neighbouring planes of the same row
+// and column fall in the same bank only for the same lane position (planes 720 floats apart would put lanes 16
+// columns apart in one bank).
+constexpr int pad32(int n) { return (n + 31) / 32 * 32; }
+constexpr int RZ = TZ + 4, RY = TY + 4, RP = pad32(RY * RZ);  // staged plane: rows j0-2..j0+TY+1, cols k0-2..k0+TZ+1
+constexpr int HZ = TZ + 2, HY = TY + 2, HP = pad32(HY * HZ);  // hat plane: rows j0-1..j0+TY, cols k0-1..k0+TZ
+constexpr int HALO = HY * HZ - NT;                        // the hat plane's one-cell ring (100 elements at TY 16)
 constexpr int VR = 8;                                     // velocity ring: planes i-1..i+2 in use, i+3 landing
 constexpr int SR = 4;                                     // smoke/temperature ring: planes i..i+2, i+3 landing
 constexpr int HR = 4;                                     // hat ring: planes i-1..i+1 read, i+2 written next
 constexpr float REACH = 0.98f;                            // trace reach (cells) served from shared memory
-constexpr int STAGE_PER_THREAD = (RP + NT - 1) / NT;      // 2
+constexpr int RPN = RY * RZ;                              // staged elements per plane
+constexpr int STAGE_PER_THREAD = (RPN + NT - 1) / NT;
 
 __device__ __forceinline__ float lerpm(float a, float b, float t) { return __fmaf_rn(t, b - a, a); }
 
@@ -73,10 +82,10 @@ __device__ __forceinline__ void range8(const float* a, float& lo, float& hi) {
 }
 
 // Corners from a ring of R staged planes; `inplane` = y * RZ + z - rowbase (the staged row and column).
-template <int R>
+template <int R, int S>
 __device__ __forceinline__ void ring_corners(const float* ring, int x, int inplane, float* a) {
-  const float* p0 = ring + (x & (R - 1)) * RP + inplane;
-  const float* p1 = ring + ((x + 1) & (R - 1)) * RP + inplane;
+  const float* p0 = ring + (x & (R - 1)) * S + inplane;
+  const float* p1 = ring + ((x + 1) & (R - 1)) * S + inplane;
   a[0] = p0[0];
   a[1] = p1[0];
   a[2] = p0[RZ];
@@ -134,16 +143,17 @@ __device__ __forceinline__ float maxabs3(F3 v) { return fmaxf(fmaxf(fabsf(v[0]),
 // ---- velocity at a point (sample.py:74-82), from the staged ring or from global memory --------------------
 // The three components' axes are split once: x of v and w, y of u and w, z of u and v are the same
 // coordinate minus 1/2.
+template <int S>
 __device__ __forceinline__ F3 ring_velocity(const float* vring, int rowbase, F3 m) {
   const Ax x0 = split(m[0]), x1 = split(m[0] - 0.5f);
   const Ax y0 = split(m[1]), y1 = split(m[1] - 0.5f);
   const Ax z0 = split(m[2]), z1 = split(m[2] - 0.5f);
   float a[8];
-  ring_corners<VR>(vring, x0.i, y1.i * RZ + z1.i - rowbase, a);
+  ring_corners<VR, S>(vring, x0.i, y1.i * RZ + z1.i - rowbase, a);
   const float u = blend8(a, x0.t, y1.t, z1.t);
-  ring_corners<VR>(vring + VR * RP, x1.i, y0.i * RZ + z1.i - rowbase, a);
+  ring_corners<VR, S>(vring + VR * S, x1.i, y0.i * RZ + z1.i - rowbase, a);
   const float v = blend8(a, x1.t, y0.t, z1.t);
-  ring_corners<VR>(vring + 2 * VR * RP, x1.i, y1.i * RZ + z0.i - rowbase, a);
+  ring_corners<VR, S>(vring + 2 * VR * S, x1.i, y1.i * RZ + z0.i - rowbase, a);
   const float w = blend8(a, x1.t, y1.t, z0.t);
   return f3(u, v, w);
 }
@@ -201,13 +211,21 @@ __device__ __forceinline__ float node_component(Load load) {
   else return lerpm(y0, along_y(az1), 0.5f);
 }
 
+// The velocity ring's plane stride: padded to a multiple of 32 floats in the velocity march; the scalar march
+// keeps it unpadded so that two blocks still fit in one SM's shared memory.
+template <int G>
+struct Stride {
+  static constexpr int value = G == 3 ? RPN : RP;
+};
+
 template <int G>
 __device__ __forceinline__ F3 ring_node(const float* vring, int x, int inplane) {
+  constexpr int S = Stride<G>::value;
   auto ring = [&](const float* r) {
-    return [=](int dx, int dy, int dz) { return r[((x + dx) & (VR - 1)) * RP + inplane + dy * RZ + dz]; };
+    return [=](int dx, int dy, int dz) { return r[((x + dx) & (VR - 1)) * S + inplane + dy * RZ + dz]; };
   };
-  return f3(node_component<G, 0>(ring(vring)), node_component<G, 1>(ring(vring + VR * RP)),
-            node_component<G, 2>(ring(vring + 2 * VR * RP)));
+  return f3(node_component<G, 0>(ring(vring)), node_component<G, 1>(ring(vring + VR * S)),
+            node_component<G, 2>(ring(vring + 2 * VR * S)));
 }
 
 template <int G, class T>
@@ -269,7 +287,7 @@ __device__ __forceinline__ void hat_at(const Args<T>& A, const float* vring, con
   F3 src = p;
   if (fast) {
     const F3 mid = sub3(p, mul3(vp, 0.5f * A.dt));
-    const F3 vm = ring_velocity(vring, rowbase, mid);
+    const F3 vm = ring_velocity<Stride<G>::value>(vring, rowbase, mid);
     fast = maxabs3(vm) * fabsf(A.dt) < REACH;
     src = sub3(p, mul3(vm, A.dt));
   }
@@ -288,8 +306,8 @@ __device__ __forceinline__ void hat_at(const Args<T>& A, const float* vring, con
       continue;
     }
     float a[8];
-    if constexpr (G == 3) ring_corners<SR>(sring + f * SR * RP, gx.i, gin, a);
-    else ring_corners<VR>(vring + G * VR * RP, gx.i, gin, a);
+    if constexpr (G == 3) ring_corners<SR, RPN>(sring + f * SR * RPN, gx.i, gin, a);
+    else ring_corners<VR, RP>(vring + G * VR * RP, gx.i, gin, a);
     hat[f] = blend8(a, gx.t, gy.t, gz.t);
     range8(a, lo[f], hi[f]);
   }
@@ -332,7 +350,7 @@ __device__ __noinline__ void back_global(const Args<T>& A, const float* hring, i
 }
 
 // ---- staging ------------------------------------------------------------------------------------------------
-// Each thread stages the plane elements e = t and t + NT (while e < RP); its offsets inside a plane of each
+// Each thread stages the plane elements e = t, t + NT, ... (while e < RPN); its offsets inside a plane of each
 // array shape are fixed for the whole march.
 struct StageOffsets {
   int off[3][STAGE_PER_THREAD];  // per array shape: u and the cells share (ny, nz); v (ny+1, nz); w (ny, nz+1)
@@ -346,7 +364,7 @@ __device__ __forceinline__ void stage_plane(const T* __restrict__ src, const Dim
 #pragma unroll
   for (int n = 0; n < STAGE_PER_THREAD; ++n) {
     const int e = threadIdx.x + n * NT;
-    if (e < RP) {
+    if (e < RPN) {
       if constexpr (sizeof(T) == 4) {
         const unsigned dst = (unsigned)__cvta_generic_to_shared(ring_plane + e);
         const size_t from = __cvta_generic_to_global(base + so.off[shape][n]);
@@ -373,9 +391,10 @@ __device__ __forceinline__ void march(const Args<T>& A, int seg, float* sm) {
   if (s >= gd.n0) return;
   const int e = imin_(s + A.seg_len, gd.n0);
 
-  float* vring = sm;                                  // [3][VR][RP]
-  float* sring = vring + 3 * VR * RP;                 // [2][SR][RP] (scalar march)
-  float* hring = sring + (G == 3 ? 2 * SR * RP : 0);  // [F][HR][HP]
+  constexpr int VS = Stride<G>::value;                 // velocity ring plane stride
+  float* vring = sm;                                  // [3][VR][VS]
+  float* sring = vring + 3 * VR * VS;                 // [2][SR][RPN] (scalar march)
+  float* hring = sring + (G == 3 ? 2 * SR * RPN : 0);  // [F][HR][HP]
   const int t = threadIdx.x, ty = t / TZ, tz = t % TZ;
   const int rowbase = (j0 - 2) * RZ + (k0 - 2), hbase = (j0 - 1) * HZ + (k0 - 1);
 
@@ -387,7 +406,7 @@ __device__ __forceinline__ void march(const Args<T>& A, int seg, float* sm) {
     for (int sh = 0; sh < 3; ++sh)
 #pragma unroll
       for (int n = 0; n < STAGE_PER_THREAD; ++n) {
-        const int el = imin_(t + n * NT, RP - 1), r = el / RZ, q = el % RZ;
+        const int el = imin_(t + n * NT, RPN - 1), r = el / RZ, q = el % RZ;
         const int y = imin_(imax_(j0 - 2 + r, 0), shapes[sh].n1 - 1);
         const int z = imin_(imax_(k0 - 2 + q, 0), shapes[sh].n2 - 1);
         so.off[sh][n] = y * shapes[sh].n2 + z;
@@ -397,12 +416,12 @@ __device__ __forceinline__ void march(const Args<T>& A, int seg, float* sm) {
   const Dims cd{nx, ny, nz};
   auto stage_velocity = [&](int plane) {
 #pragma unroll
-    for (int c = 0; c < 3; ++c) stage_plane(A.vel[c], vd[c], c, plane, vring + (c * VR + (plane & (VR - 1))) * RP, so);
+    for (int c = 0; c < 3; ++c) stage_plane(A.vel[c], vd[c], c, plane, vring + (c * VR + (plane & (VR - 1))) * VS, so);
   };
   auto stage_scalars = [&](int plane) {
     if constexpr (G == 3) {
 #pragma unroll
-      for (int f = 0; f < 2; ++f) stage_plane(A.field[f], cd, 0, plane, sring + (f * SR + (plane & (SR - 1))) * RP, so);
+      for (int f = 0; f < 2; ++f) stage_plane(A.field[f], cd, 0, plane, sring + (f * SR + (plane & (SR - 1))) * RPN, so);
     }
   };
 
@@ -511,7 +530,7 @@ __device__ __forceinline__ void march(const Args<T>& A, int seg, float* sm) {
       float back[F];
       if (fast) {
         const F3 mid = sub3(p, mul3(vp, 0.5f * -A.dt));
-        const F3 vm = ring_velocity(vring, rowbase, mid);
+        const F3 vm = ring_velocity<VS>(vring, rowbase, mid);
         fast = maxabs3(vm) * fabsf(A.dt) < REACH;
         if (fast) {
           const F3 bsrc = sub3(p, mul3(vm, -A.dt));
@@ -536,7 +555,7 @@ __device__ __forceinline__ void march(const Args<T>& A, int seg, float* sm) {
       const size_t out = (size_t)i * plane_stride + (size_t)tj * gd.n2 + tk;
 #pragma unroll
       for (int f = 0; f < F; ++f) {
-        const float data = G == 3 ? ldg_f(A.field[f] + out) : vring[(G * VR + (i & (VR - 1))) * RP + inplane];
+        const float data = G == 3 ? ldg_f(A.field[f] + out) : vring[(G * VR + (i & (VR - 1))) * VS + inplane];
         const float corrected = own_hat[f] + 0.5f * (data - back[f]);
         float value = clampf_(corrected, range_lo[f], range_hi[f]);
         if (G == 3 && f == 0) {
@@ -565,7 +584,7 @@ __device__ __forceinline__ void march(const Args<T>& A, int seg, float* sm) {
 
 // MINB: blocks per SM the kernel is compiled for (2: at most 64 registers a thread; 1: up to 128).
 template <class T, int MINB>
-__global__ void __launch_bounds__(NT, MINB) k_mac_velocity(Args<T> A) {
+__global__ void __launch_bounds__(NT, MINB * BLOCKS_PER_SM / 2) k_mac_velocity(Args<T> A) {
   extern __shared__ float sm[];
   int z = blockIdx.z;
   if (z < A.segs[0]) return march<T, 0>(A, z, sm);
@@ -575,7 +594,7 @@ __global__ void __launch_bounds__(NT, MINB) k_mac_velocity(Args<T> A) {
 }
 
 template <class T, int MINB>
-__global__ void __launch_bounds__(NT, MINB) k_mac_scalars(Args<T> A) {
+__global__ void __launch_bounds__(NT, MINB * BLOCKS_PER_SM / 2) k_mac_scalars(Args<T> A) {
   extern __shared__ float sm[];
   march<T, 3>(A, blockIdx.z, sm);
 }
@@ -604,11 +623,11 @@ __global__ void k_segment_lines(const float* __restrict__ seg_sums, int segs, lo
 }
 
 constexpr size_t VELOCITY_SMEM = sizeof(float) * (3 * VR * RP + HR * HP);
-constexpr size_t SCALAR_SMEM = sizeof(float) * (3 * VR * RP + 2 * SR * RP + 2 * HR * HP);
+constexpr size_t SCALAR_SMEM = sizeof(float) * (3 * VR * RPN + 2 * SR * RPN + 2 * HR * HP);
 
-// Segments along x: enough blocks for about six waves of two blocks per SM, each segment at least 8 planes.
+// Segments along x: enough blocks for about six waves of the resident blocks, each segment at least 8 planes.
 static int segments(int n0, long tiles, int groups) {
-  const long target = 6L * 2 * 148;
+  const long target = 6L * BLOCKS_PER_SM * 148;
   long segs = (target + tiles * groups - 1) / (tiles * groups);
   segs = std::max(1L, std::min(segs, (long)std::max(1, n0 / 8)));
   return (int)segs;
