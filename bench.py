@@ -261,38 +261,47 @@ def batched_variant(device: str, count: int = 64, frames: int = 48) -> dict:
 
 
 def adjoint_variant(device: str) -> dict:
-    """The differentiable step's cost: a 96 x 144 x 96 smoke puff (forces.smoke_weight 0), a 16^3 source field
-    with its corner at cell (40, 0, 40) (centred on (48, 8, 48)), 64 substeps with a checkpoint every 8; the
-    forward run (recording the tape) against the backward pass (recomputing each segment's smoke path, then
-    the adjoint), per substep, timed on the host around device-synchronised runs."""
+    """The differentiable step (BASELINE C3): 96 x 144 x 96 cells, 64 substeps (32 frames of 2), a 16^3 source
+    field centred on cell (48, 8, 48), buoyancy 1.0 and drag 0.2 (no vorticity confinement), a checkpoint every 8
+    substeps. FlowFit's gradient with respect to the source field, heat_buoyancy and drag_per_s (the velocity
+    path included) against the forward substep it differentiates: the forward is timed as plume_step substeps
+    (the production step) and as FlowFit's taped forward; the adjoint is the backward pass (recomputing each
+    segment, then every substep's adjoint). CUDA events around device-synchronised runs."""
     import dataclasses
 
-    import numpy as np
     import torch
 
-    from plume_b200.adjoint import SourceFit
+    from plume_b200.adjoint import FlowFit
+    from plume_b200.recipe.derived import derive
+    from plume_b200.sim.grid import make_grid
+    from plume_b200.sim.stepper import Stepper
     from plume_b200.workloads import plain_step_recipe
 
     recipe = plain_step_recipe((96, 144, 96), cycles=4, frames=32, substeps=2)
-    recipe = dataclasses.replace(recipe, forces=dataclasses.replace(recipe.forces, smoke_weight=0.0))
+    recipe = dataclasses.replace(recipe, forces=dataclasses.replace(recipe.forces, vorticity_confinement=0.0))
+    derived = derive(recipe)
     substeps = 64
-    fit = SourceFit(recipe, (16, 16, 16), (40, 0, 40), substeps, device, checkpoint_every=8)
+    fit = FlowFit(recipe, (16, 16, 16), (40, 0, 40), substeps, device, checkpoint_every=8)
     source = torch.from_numpy(np.random.default_rng(3).uniform(0.0, 1.0, (16, 16, 16)).astype(np.float32)).to(device)
     target = torch.zeros((fit.view.height_px, fit.view.width_px), dtype=torch.float32, device=device)
     fit.loss_and_grad(source, target)  # warm-up: graph captures, allocations
-    torch.cuda.synchronize()
-    start = time.perf_counter()
-    fit.forward(source)
-    torch.cuda.synchronize()
-    forward = time.perf_counter() - start
-    start = time.perf_counter()
-    fit.loss_and_grad(source, target)
-    torch.cuda.synchronize()
-    total = time.perf_counter() - start
-    backward = total - forward
+    taped_ms = device_ms(lambda: fit.forward(source))
+    total_ms = device_ms(lambda: fit.loss_and_grad(source, target))
+    d = recipe.domain
+    grid = make_grid(derived, d.cell_m, d.faces, d.ambient_k, device)
+    stepper = Stepper(grid, recipe)
+    stepper.step(0.0, derived.dt_s)
+    step_ms = device_ms(lambda: [stepper.step(n * derived.dt_s, derived.dt_s) for n in range(substeps)])
+    adjoint_ms = total_ms - taped_ms
+    _, _, scalars, _ = fit.loss_and_grad(source, target)
     return {"cells": [96, 144, 96], "substeps": substeps, "checkpoint_every": 8,
-            "forward_ms_per_substep": forward * 1e3 / substeps, "adjoint_ms_per_substep": backward * 1e3 / substeps,
-            "adjoint_over_forward": backward / forward}
+            "parameters": ["source field 16^3", "heat_buoyancy", "drag_per_s"],
+            "forward_step_ms_per_substep": step_ms / substeps,
+            "forward_taped_ms_per_substep": taped_ms / substeps,
+            "adjoint_ms_per_substep": adjoint_ms / substeps,
+            "adjoint_over_forward": adjoint_ms / step_ms,
+            "adjoint_over_taped_forward": adjoint_ms / taped_ms,
+            "scalar_gradients": scalars}
 
 
 def square_view(view, pixels: int):

@@ -220,9 +220,10 @@ int plume_use_graphs(int32_t enable);
 
 /* No counterpart in the reference (the same solve, another storage). plume_multigrid with caller scratch of
  * plume_split_scratch_floats(&levels[0].info) floats: when the top level has at least the plume_tune_split
- * threshold of cells (default 1 << 23, the levels larger than L2), it is swept in colour-split storage (red and
- * black cells in separate arrays, converted in and out around the cycles), which halves the sectors a colour
- * pass moves. Every value equals plume_multigrid's. plume_step does the same with its advect_scratch. */
+ * threshold of cells, it is swept in colour-split storage (red and black cells in separate arrays, converted in
+ * and out around the cycles), so that a colour pass moves only the sectors of the cells it needs. Every value
+ * equals plume_multigrid's. plume_step does the same with its advect_scratch. The threshold is off by default
+ * (1 << 40 cells): the split kernels measured slower on B200. */
 long long plume_split_scratch_floats(const PlumeGridInfo* info);
 int plume_tune_split(long long min_cells);
 int plume_multigrid_split(const PlumeLevel* levels, int32_t level_count, int32_t cycles, int32_t sweeps,
@@ -272,10 +273,11 @@ int plume_smoke_budget(const PlumeGridInfo* info, const float* data, const float
 int plume_smoke_budget_static(const PlumeGridInfo* info, const float* data, const float* hat, float* next,
                               double* totals_out, void* stream);
 
-/* No counterpart in the reference. plume_step advects velocity, smoke and temperature with the fused passes
- * below (the default, enable = 1) or with the two-pass kernels of plume_advect_maccormack (enable = 0), whose
- * blends keep the reference's a*(1-t) + b*t. A process-wide switch, for comparison and tests. */
-int plume_use_fused_advection(int32_t enable);
+/* No counterpart in the reference. Which of plume_step's advections use the fused passes below: bit 0 the
+ * velocity (plume_maccormack_velocity), bit 1 smoke and temperature (plume_maccormack_scalars); the others use
+ * the two-pass kernels of plume_advect_maccormack, whose blends keep the reference's a*(1-t) + b*t. Default 1
+ * (fused velocity, two-pass scalars: the fastest measured on B200). A process-wide switch. */
+int plume_use_fused_advection(int32_t mask);
 
 /* advect.py:59-68 advect_maccormack of u, v and w by themselves (the step's velocity advection,
  * stepper.py:46-52), in one fused pass: the forward semi-Lagrangian value is kept in on-chip memory and never

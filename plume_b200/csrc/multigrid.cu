@@ -42,9 +42,12 @@ static long g_tiled_min_cells = 1L << 40;  // measured: per-colour sweeps win wh
 // 2048 cells (rather than 8192) saves 9% of the solve: a 16x24x16 level sweeps faster as per-colour launches
 // across the GPU than inside one block on one SM.
 static long g_bottom_max_cells = 2048;
-// The top level runs in colour-split storage (given caller scratch) when it has at least this many cells:
-// the levels that do not fit in L2, where the colour passes are bound by DRAM traffic.
-static long g_split_min_cells = 1L << 23;
+// The top level runs in colour-split storage (given caller scratch) when it has at least this many cells
+// (plume_tune_split). Off by default: measured on B200 at 256x384x256, every split kernel ran about 1.8x slower
+// than its natural-layout counterpart although it moves fewer sectors (colour pass 109 vs 59 us, residual and
+// restriction 165 vs about 95 us, prolongation 133 vs about 80 us), and the 4-cycle solve took 5.46 ms
+// against 3.53 ms.
+static long g_split_min_cells = 1L << 40;
 static int g_bottom_kind = 0;  // 0: the one-block solve, 1: the cluster solve
 constexpr size_t BOTTOM_MAX_SMEM = 200 * 1024;
 

@@ -3,10 +3,11 @@ heat_buoyancy and drag_per_s, whose effect reaches the smoke only through the ve
 self-advection, projection, scalar advection), and with respect to the source field, with a smoke weight so
 that the smoke also pushes the velocity.
 
-Checks: each scalar's gradient against central differences of the same float32 model's loss, and of the FP64
-oracle's loss; the source gradient against central differences on the voxels with the largest gradient; and,
-without smoke weight, the source gradient equals SourceFit's (the smoke-only adjoint) where the velocity path
-adds nothing."""
+Checks: each scalar's gradient against central differences of the FP64 oracle's loss (h = 1e-3; measured
+agreement 3e-3 and 4e-3) and, more loosely, of the float32 model's own loss (h = 1e-2, whose rounding and
+curvature put it a few percent off); the source gradient against central differences on the voxels with the
+largest gradient; and, without smoke weight, the source gradient equals SourceFit's (the smoke-only adjoint)
+where the velocity path adds nothing."""
 
 import dataclasses
 
@@ -24,8 +25,8 @@ SOURCE = (5, 5, 5)
 CORNER = (7, 2, 7)
 SUBSTEPS = 10
 CYCLES = 8  # forward V-cycles: the forward projection close to exact, as the adjoint's is
-SCALAR_RTOL = 1e-2      # against float32 central differences
-SCALAR_RTOL_FP64 = 2e-2
+SCALAR_RTOL_FP64 = 1e-2  # against FP64 central differences
+SCALAR_RTOL = 6e-2       # against float32 central differences
 SOURCE_RTOL = 2e-2
 
 
@@ -81,7 +82,6 @@ def test_scalar_gradients_match_central_differences(cuda_device, case, name, h):
     up = fit.with_forces(**{name: value + h}).loss(src, tgt)
     down = fit.with_forces(**{name: value - h}).loss(src, tgt)
     fd = (up - down) / (2.0 * h)
-    target_recipe = recipe
     up64, _ = oracle_loss(dataclasses.replace(recipe, forces=dataclasses.replace(recipe.forces, **{name: value + 1e-3})),
                           source, target)
     down64, _ = oracle_loss(dataclasses.replace(recipe, forces=dataclasses.replace(recipe.forces, **{name: value - 1e-3})),
