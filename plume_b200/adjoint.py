@@ -202,15 +202,23 @@ class FlowFit:
       dissipation; the smoke budget (uniform terms from its totals); MacCormack of smoke and temperature, with
       respect to the fields and to the advecting velocity (both traces' endpoints and midpoints); the
       projection, whose adjoint is the projection itself (walls zeroed, divergence, solve, gradient: the
-      operator is symmetric), solved by `adjoint_cycles` V-cycles from zero (or refined to `solve_tol`); MacCormack of the velocity by itself (as field and as
-      advector); drag (d/d drag_per_s); buoyancy (to temperature and smoke, d/d heat_buoyancy); the emitter's
-      blends; the source add (d/d source).
-    The forward solve runs the recipe's V-cycles from its warm start; the adjoint solves the projection more
-    accurately, so the gradient is that of the exact projection (the forward solve's residual bounds the
-    difference)."""
+      operator is symmetric), solved by `adjoint_cycles` V-cycles (the recipe's count by default) or refined
+      to `solve_tol`; MacCormack of the velocity by itself (as field and as advector); drag (d/d drag_per_s);
+      buoyancy (to temperature and smoke, d/d heat_buoyancy); the emitter's blends; the source add (d/d source).
+    The forward solve runs the recipe's V-cycles from the previous substep's pressure. The adjoint's solve
+    starts, with `warm_start`, from the adjoint pressure of the substep after it (the one solved just before
+    in the backward walk), else from zero. Either way the gradient is that of the exact projection, to within
+    the residual the solves leave.
+
+    Tape: a substep's record is 12 face arrays and 5 cell arrays. The forward pass of loss_and_grad keeps the
+    records of the last segments whole while they fit `tape_bytes` (by default half the device memory free when
+    the gradient is asked for), and the backward pass recomputes only the segments it did not keep. The forward
+    is deterministic, so a kept record and a recomputed one are the same floats, and the budget changes the
+    time, not the gradient."""
 
     def __init__(self, recipe, source_shape, corner, substeps: int, device: str = "cuda:0", window=(0.0, math.inf),
-                 checkpoint_every: int = 8, adjoint_cycles: int = 8, solve_tol: float | None = None):
+                 checkpoint_every: int = 8, adjoint_cycles: int | None = None, solve_tol: float | None = None,
+                 warm_start: bool = True, tape_bytes: int | None = None):
         from plume_b200.sim.multigrid import Multigrid
 
         f = recipe.forces
@@ -222,7 +230,10 @@ class FlowFit:
         self.device = device
         self.source_shape, self.corner = tuple(source_shape), tuple(corner)
         self.substeps, self.window, self.every = substeps, window, checkpoint_every
-        self.adjoint_cycles, self.solve_tol = adjoint_cycles, solve_tol
+        if adjoint_cycles is None:
+            adjoint_cycles = recipe.solver.multigrid_cycles
+        self.adjoint_cycles, self.solve_tol, self.warm_start = adjoint_cycles, solve_tol, warm_start
+        self.tape_bytes = tape_bytes
         self.view = sheet_domain_view(recipe, self.derived)
         self.view_params = domain_view_params(self.view)
         self.emitters = emitter_params(recipe.emitter, device)
@@ -313,20 +324,42 @@ class FlowFit:
                    ambient, N.stream())
         return rec
 
-    def forward(self, source: torch.Tensor):
+    def forward(self, source: torch.Tensor, taped_from: int | None = None):
         """The run from rest with the source; returns the checkpoints (one full state every checkpoint_every
-        substeps) and leaves the final state in the work grid."""
+        substeps) and leaves the final state in the work grid. With `taped_from`, also returns the records of
+        substeps taped_from.. (a dict by substep)."""
         g = self.grid
         for x in (*g.velocity_fields(), g.smoke):
             x.data.zero_()
         g.temperature.data.fill_(self.recipe.domain.ambient_k)
         g.pressure.zero_()
-        checkpoints = []
+        checkpoints, records = [], {}
         for n in range(self.substeps):
             if n % self.every == 0:
                 checkpoints.append(self._state())
-            self._substep(n, source)
-        return checkpoints
+            taped = taped_from is not None and n >= taped_from
+            rec = self._substep(n, source, record=taped)
+            if taped:
+                records[n] = rec
+        return (checkpoints, records) if taped_from is not None else checkpoints
+
+    def record_bytes(self) -> int:
+        """Device bytes of one substep's record."""
+        g = self.grid
+        faces = sum(x.data.numel() for x in g.velocity_fields())
+        return 4 * (4 * faces + 5 * g.smoke.data.numel()) + 8 * 3
+
+    def _taped_from(self) -> int:
+        """The first substep whose record the forward keeps: whole segments from the end, within the budget."""
+        budget = self.tape_bytes
+        if budget is None:
+            free, _ = torch.cuda.mem_get_info(torch.device(self.device))
+            budget = free // 2
+        keep = int(budget // self.record_bytes())
+        first = self.substeps - keep
+        if first <= 0:
+            return 0
+        return min(self.substeps, -(-first // self.every) * self.every)
 
     def _thickness(self, target):
         g = self.grid
@@ -348,17 +381,19 @@ class FlowFit:
     def with_forces(self, **forces) -> "FlowFit":
         recipe = dataclasses.replace(self.recipe, forces=dataclasses.replace(self.recipe.forces, **forces))
         return FlowFit(recipe, self.source_shape, self.corner, self.substeps, self.device, self.window, self.every,
-                       self.adjoint_cycles, self.solve_tol)
+                       self.adjoint_cycles, self.solve_tol, self.warm_start, self.tape_bytes)
 
     # ---- backward ----------------------------------------------------------------------------------------
     def _project_adjoint(self, a_vel):
-        """a_vel <- P a_vel: the projection, its solve adjoint_cycles V-cycles from zero (or refined)."""
+        """a_vel <- P a_vel: the projection, its solve adjoint_cycles V-cycles (or refined) from the last
+        adjoint pressure (warm_start) or from zero."""
         from plume_b200.sim.pressure import project, project_refined
 
         adj = self.adjoint_grid
         for x, a in zip(adj.velocity_fields(), a_vel):
             x.data.copy_(a)
-        adj.pressure.zero_()
+        if not self.warm_start:
+            adj.pressure.zero_()
         if self.solve_tol is None:
             project(adj, self.adjoint_multigrid)
         else:
@@ -420,9 +455,11 @@ class FlowFit:
         """(loss, d loss / d source, {"heat_buoyancy": ..., "drag_per_s": ...}, final thickness)."""
         source = source.to(self.device, torch.float32).contiguous()
         target = target.to(self.device, torch.float32).contiguous()
-        checkpoints = self.forward(source)
+        taped_from = self._taped_from()
+        checkpoints, taped = self.forward(source, taped_from)
         loss, thickness, a_smoke = self._thickness(target)
         g = self.grid
+        self.adjoint_grid.pressure.zero_()
         a_heat = torch.zeros_like(g.temperature.data)
         a_vel = [torch.zeros_like(x.data) for x in g.velocity_fields()]
         grads = torch.zeros(2, dtype=torch.float64, device=self.device)
@@ -430,8 +467,11 @@ class FlowFit:
         for segment in reversed(range(len(checkpoints))):
             first = segment * self.every
             last = min(first + self.every, self.substeps)
-            self._load(checkpoints[segment])
-            records = [self._substep(n, source, record=True) for n in range(first, last)]
+            if first >= taped_from:
+                records = [taped.pop(n) for n in range(first, last)]
+            else:
+                self._load(checkpoints[segment])
+                records = [self._substep(n, source, record=True) for n in range(first, last)]
             for n in reversed(range(first, last)):
                 a_smoke, a_heat, a_vel = self._substep_adjoint(n, records[n - first], a_smoke, a_heat, a_vel, grads,
                                                                grad_source)

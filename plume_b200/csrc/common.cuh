@@ -34,6 +34,24 @@ __device__ __forceinline__ F3 add3(F3 a, F3 b) { return f3(a[0] + b[0], a[1] + b
 __device__ __forceinline__ F3 sub3(F3 a, F3 b) { return f3(a[0] - b[0], a[1] - b[1], a[2] - b[2]); }
 __device__ __forceinline__ F3 mul3(F3 a, float s) { return f3(a[0] * s, a[1] * s, a[2] * s); }
 __device__ __forceinline__ F3 div3(F3 a, float s) { return f3(a[0] / s, a[1] / s, a[2] / s); }
+
+// x / d where d is often a power of two (a grid spacing such as 1/64 m, its square, a child count). When d is
+// a positive power of two whose reciprocal is a normal float, x * (1/d) multiplies by an exact 2^-e, so the
+// product is the correctly rounded quotient: the same float as the IEEE division (this library never flushes
+// subnormals), without the division's instruction sequence. Any other d divides.
+struct Divisor {
+  float d, inv;
+  bool pow2;
+};
+__device__ __forceinline__ Divisor divisor(float d) {
+  const unsigned bits = __float_as_uint(d), e = bits >> 23;  // sign bit 0 checked below, so e is the exponent
+  const bool pow2 = (bits & 0x807fffffu) == 0u && e >= 1u && e <= 253u;
+  return Divisor{d, __uint_as_float((254u - (pow2 ? e : 127u)) << 23), pow2};
+}
+__device__ __forceinline__ float divide(float x, const Divisor& q) { return q.pow2 ? x * q.inv : x / q.d; }
+__device__ __forceinline__ F3 divide3(F3 a, const Divisor& q) {
+  return f3(divide(a[0], q), divide(a[1], q), divide(a[2], q));
+}
 __device__ __forceinline__ float dot3(F3 a, F3 b) { return a[0] * b[0] + a[1] * b[1] + a[2] * b[2]; }
 __device__ __forceinline__ float len3(F3 a) { return sqrtf(dot3(a, a)); }
 __device__ __forceinline__ F3 normalize3(F3 a) { return div3(a, len3(a)); }

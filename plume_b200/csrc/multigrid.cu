@@ -206,7 +206,7 @@ __global__ void k_residual_restrict(PlumeGridInfo fine, const float* __restrict_
         }
       }
   const int out = at(coarse, i, j, k);
-  coarse_rhs[out] = total / count;
+  coarse_rhs[out] = divide(total, divisor(count));  // count is 1, 2, 4 or 8
   coarse_q[out] = 0.0f;
 }
 
@@ -241,7 +241,23 @@ __global__ void k_split_layout(Dims d, int H, const float* __restrict__ in, floa
 }
 
 // One colour pass over the split arrays, PLANES x-planes per thread: every update is computed before any is
-// stored (a colour reads only the other colour).
+// stored (a colour reads only the other colour). A cell's six face neighbours all sit in the other colour's
+// array: its x and y neighbours at the same half index m, one plane (ny * H) or one row (H) away; its z
+// neighbours at m - 1 + p and m + p, p = k & 1. `face_load` turns the stencil's (i, j, k) neighbour
+// coordinates into those offsets, so every load is one add from the cell's own index.
+struct SplitCell {
+  long other;  // the index of (i, j, k >> 1) in the other colour's array
+  int i, j, k, par, plane, row;
+  __device__ __forceinline__ long face(int a, int b, int c) const {
+    return other + (long)((a - i) * plane + (b - j) * row + (c < k ? par - 1 : (c > k ? par : 0)));
+  }
+};
+
+__device__ __forceinline__ SplitCell split_cell(const Dims& d, int H, int i, int j, int k) {
+  const int c = (i + j + k) & 1;
+  return SplitCell{((long)((1 - c) * d.n0 + i) * d.n1 + j) * H + (k >> 1), i, j, k, k & 1, d.n1 * H, H};
+}
+
 template <int PLANES>
 __global__ void k_rb_split(PlumeGridInfo info, int H, float* __restrict__ qs, const float* __restrict__ rs, int color,
                            float relaxation) {
@@ -252,7 +268,6 @@ __global__ void k_rb_split(PlumeGridInfo info, int H, float* __restrict__ qs, co
   if (j >= ny || m >= H) return;
   const Dims d = dims_of(info);
   const float ghost = ghost_coupling(info);
-  auto load = [&](int a, int b, int c) { return qs[split_at(d, H, a, b, c)]; };
   float out[PLANES];
   bool write[PLANES];
 #pragma unroll
@@ -261,6 +276,8 @@ __global__ void k_rb_split(PlumeGridInfo info, int H, float* __restrict__ qs, co
     write[p] = false;
     if (i < nx && k < nz) {
       const long idx = ((long)(color * nx + i) * ny + j) * H + m;
+      const SplitCell cell = split_cell(d, H, i, j, k);
+      auto load = [&](int a, int b, int c) { return qs[cell.face(a, b, c)]; };
       write[p] = relax_cell(true, info, ghost, i, j, k, qs[idx], __ldg(rs + idx), relaxation, load, out[p]);
     }
   }
@@ -277,7 +294,6 @@ __global__ void k_residual_restrict_split(PlumeGridInfo fine, int H, const float
   const int i = blockIdx.z, j = blockIdx.y * blockDim.y + threadIdx.y, k = blockIdx.x * blockDim.x + threadIdx.x;
   if (j >= coarse.n1 || k >= coarse.n2) return;
   const Dims fd = dims_of(fine);
-  auto load = [&](int a, int b, int c) { return __ldg(qs + split_at(fd, H, a, b, c)); };
   const bool uniform = is_uniform(fine);
   const float ghost = ghost_coupling(fine);
   float total = 0.0f, count = 0.0f;
@@ -290,12 +306,14 @@ __global__ void k_residual_restrict_split(PlumeGridInfo fine, int H, const float
         const int fi = 2 * i + di, fj = 2 * j + dj, fk = 2 * k + dk;
         if (fi < fd.n0 && fj < fd.n1 && fk < fd.n2) {
           const long idx = split_at(fd, H, fi, fj, fk);
+          const SplitCell cell = split_cell(fd, H, fi, fj, fk);
+          auto load = [&](int a, int b, int c) { return __ldg(qs + cell.face(a, b, c)); };
           total = total + residual_cell(uniform, fine, ghost, fi, fj, fk, __ldg(qs + idx), __ldg(rs + idx), load);
           count = count + 1.0f;
         }
       }
   const int out = at(coarse, i, j, k);
-  coarse_rhs[out] = total / count;
+  coarse_rhs[out] = divide(total, divisor(count));  // count is 1, 2, 4 or 8
   coarse_q[out] = 0.0f;
 }
 

@@ -76,7 +76,7 @@ __device__ __forceinline__ float residual_at(const PlumeGridInfo& info, int i, i
   float sq, sc;
   neighbor_sum(info, i, j, k, load, sq, sc);
   float scale = cell_volume(info, i, j, k) * info.cell_m * info.cell_m;
-  return rhs - (sq - sc * q) / scale;
+  return rhs - divide(sq - sc * q, divisor(scale));
 }
 
 // ---- the uniform-coefficient case ---------------------------------------------------------------------------
@@ -140,7 +140,7 @@ __device__ __forceinline__ float residual_uniform(const PlumeGridInfo& info, flo
                                                   float rhs, Load load) {
   float sq, sc;
   neighbor_sum_uniform(info, ghost, i, j, k, load, sq, sc);
-  return rhs - (sq - sc * q) / (info.cell_m * info.cell_m);
+  return rhs - divide(sq - sc * q, divisor(info.cell_m * info.cell_m));
 }
 
 // Either path, chosen per level.

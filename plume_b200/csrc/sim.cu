@@ -324,9 +324,13 @@ __device__ __forceinline__ F3 center_velocity(const VelT<T>& vel, int i, int j, 
 }
 
 // curl_kernel (vorticity.py:38-45) with the centre velocities of center_velocity_kernel computed in place.
+// With `spin` (the step's scratch), |curl| of the cell is stored as well, computed as push_at would compute it
+// from the stored components (the same floats), so the push reads one value per neighbour instead of three and
+// a square root.
 template <class T>
 __device__ __forceinline__ void curl_at(const PlumeGridInfo& info, const VelT<T>& vel, float* __restrict__ cx,
-                                        float* __restrict__ cy, float* __restrict__ cz, int i, int j, int k) {
+                                        float* __restrict__ cy, float* __restrict__ cz, float* __restrict__ spin,
+                                        int i, int j, int k) {
   const int nx = info.dims[0], ny = info.dims[1], nz = info.dims[2];
   const int cell[3] = {i, j, k};
   const int n[3] = {nx, ny, nz};
@@ -340,25 +344,27 @@ __device__ __forceinline__ void curl_at(const PlumeGridInfo& info, const VelT<T>
     if (span == 0.0f) {
       d[axis] = f3(0.0f, 0.0f, 0.0f);
     } else {
-      d[axis] = div3(sub3(center_velocity(vel, hi[0], hi[1], hi[2]), center_velocity(vel, lo[0], lo[1], lo[2])),
-                     span * info.cell_m);
+      d[axis] = divide3(sub3(center_velocity(vel, hi[0], hi[1], hi[2]), center_velocity(vel, lo[0], lo[1], lo[2])),
+                        divisor(span * info.cell_m));
     }
   }
   const int c = (i * ny + j) * nz + k;
-  cx[c] = d[1][2] - d[2][1];
-  cy[c] = d[2][0] - d[0][2];
-  cz[c] = d[0][1] - d[1][0];
+  const F3 curl = f3(d[1][2] - d[2][1], d[2][0] - d[0][2], d[0][1] - d[1][0]);
+  cx[c] = curl[0];
+  cy[c] = curl[1];
+  cz[c] = curl[2];
+  if (spin) spin[c] = len3(curl);
 }
 
 template <class T, int PLANES>
 __global__ void k_curl(PlumeGridInfo info, VelT<T> vel, float* __restrict__ cx, float* __restrict__ cy,
-                       float* __restrict__ cz) {
+                       float* __restrict__ cz, float* __restrict__ spin) {
   const int nx = info.dims[0], ny = info.dims[1], nz = info.dims[2];
   const int i0 = blockIdx.z * PLANES, j = blockIdx.y * blockDim.y + threadIdx.y, k = blockIdx.x * blockDim.x + threadIdx.x;
   if (j >= ny || k >= nz) return;
 #pragma unroll
   for (int p = 0; p < PLANES; ++p)
-    if (i0 + p < nx) curl_at(info, vel, cx, cy, cz, i0 + p, j, k);
+    if (i0 + p < nx) curl_at(info, vel, cx, cy, cz, spin, i0 + p, j, k);
 }
 
 __device__ __forceinline__ F3 load3(const float* __restrict__ x, const float* __restrict__ y,
@@ -366,11 +372,13 @@ __device__ __forceinline__ F3 load3(const float* __restrict__ x, const float* __
   return f3(__ldg(x + c), __ldg(y + c), __ldg(z + c));
 }
 
-// confinement_push_kernel (vorticity.py:53-71).
+// confinement_push_kernel (vorticity.py:53-71); SPIN: |curl| read from k_curl's `spin` array.
+template <bool SPIN>
 __device__ __forceinline__ void push_at(const PlumeGridInfo& info, const float* __restrict__ cx,
                                         const float* __restrict__ cy, const float* __restrict__ cz,
-                                        float* __restrict__ px, float* __restrict__ py, float* __restrict__ pz,
-                                        float strength, int i, int j, int k) {
+                                        const float* __restrict__ spin, float* __restrict__ px,
+                                        float* __restrict__ py, float* __restrict__ pz, float strength, int i, int j,
+                                        int k) {
   const int nx = info.dims[0], ny = info.dims[1], nz = info.dims[2];
   const Dims d{nx, ny, nz};
   const int cell[3] = {i, j, k};
@@ -383,9 +391,10 @@ __device__ __forceinline__ void push_at(const PlumeGridInfo& info, const float* 
     hi[axis] = imin_(cell[axis] + 1, n[axis] - 1);
     float span = (float)(hi[axis] - lo[axis]);
     if (span > 0.0f) {
-      float spin_hi = len3(load3(cx, cy, cz, at(d, hi[0], hi[1], hi[2])));
-      float spin_lo = len3(load3(cx, cy, cz, at(d, lo[0], lo[1], lo[2])));
-      toward[axis] = (spin_hi - spin_lo) / (span * info.cell_m);
+      const int at_hi = at(d, hi[0], hi[1], hi[2]), at_lo = at(d, lo[0], lo[1], lo[2]);
+      float spin_hi = SPIN ? __ldg(spin + at_hi) : len3(load3(cx, cy, cz, at_hi));
+      float spin_lo = SPIN ? __ldg(spin + at_lo) : len3(load3(cx, cy, cz, at_lo));
+      toward[axis] = divide(spin_hi - spin_lo, divisor(span * info.cell_m));
     }
   }
   const int c = at(d, i, j, k);
@@ -402,16 +411,16 @@ __device__ __forceinline__ void push_at(const PlumeGridInfo& info, const float* 
   pz[c] = push[2];
 }
 
-template <int PLANES>
+template <int PLANES, bool SPIN>
 __global__ void k_push(PlumeGridInfo info, const float* __restrict__ cx, const float* __restrict__ cy,
-                       const float* __restrict__ cz, float* __restrict__ px, float* __restrict__ py,
-                       float* __restrict__ pz, float strength) {
+                       const float* __restrict__ cz, const float* __restrict__ spin, float* __restrict__ px,
+                       float* __restrict__ py, float* __restrict__ pz, float strength) {
   const int nx = info.dims[0], ny = info.dims[1], nz = info.dims[2];
   const int i0 = blockIdx.z * PLANES, j = blockIdx.y * blockDim.y + threadIdx.y, k = blockIdx.x * blockDim.x + threadIdx.x;
   if (j >= ny || k >= nz) return;
 #pragma unroll
   for (int p = 0; p < PLANES; ++p)
-    if (i0 + p < nx) push_at(info, cx, cy, cz, px, py, pz, strength, i0 + p, j, k);
+    if (i0 + p < nx) push_at<SPIN>(info, cx, cy, cz, spin, px, py, pz, strength, i0 + p, j, k);
 }
 
 // ---- turbulence: turbulence.py:26-53 -----------------------------------------------------------------------
@@ -531,19 +540,27 @@ static int launch_face_forces(const PlumeGridInfo& info, T* u, T* v, T* w, const
   });
 }
 
+// `spin`, when given, is nx*ny*nz floats of scratch for |curl| (the step passes its divergence array, which
+// the projection overwrites later).
 template <class T>
 static int launch_confinement_push(const PlumeGridInfo& info, const T* u, const T* v, const T* w,
                                    float* const curl[3], float* const push[3], float strength, int apply,
-                                   cudaStream_t st) {
+                                   cudaStream_t st, float* spin = nullptr) {
   const int nx = info.dims[0], ny = info.dims[1], nz = info.dims[2];
   VelT<T> vel = make_vel(u, v, w, info.dims);
+  if (!apply) spin = nullptr;
   return with_planes([&](auto P) {
     constexpr int PL = decltype(P)::value;
-    k_curl<T, PL><<<cell_grid_planes(nx, ny, nz, PL), cell_block(), 0, st>>>(info, vel, curl[0], curl[1], curl[2]);
+    const dim3 grid = cell_grid_planes(nx, ny, nz, PL);
+    k_curl<T, PL><<<grid, cell_block(), 0, st>>>(info, vel, curl[0], curl[1], curl[2], spin);
     CHECK_LAUNCH("curl");
     if (!apply) return PLUME_OK;
-    k_push<PL><<<cell_grid_planes(nx, ny, nz, PL), cell_block(), 0, st>>>(info, curl[0], curl[1], curl[2], push[0],
-                                                                          push[1], push[2], strength);
+    if (spin)
+      k_push<PL, true><<<grid, cell_block(), 0, st>>>(info, curl[0], curl[1], curl[2], spin, push[0], push[1],
+                                                      push[2], strength);
+    else
+      k_push<PL, false><<<grid, cell_block(), 0, st>>>(info, curl[0], curl[1], curl[2], nullptr, push[0], push[1],
+                                                       push[2], strength);
     return launch_status("confinement push");
   });
 }
@@ -846,7 +863,7 @@ __global__ void k_divergence(PlumeGridInfo info, const T* __restrict__ u, const 
     float flux = (ldg_f(u + ((i + 1) * ny + j) * nz + k) - ldg_f(u + (i * ny + j) * nz + k)) +
                  (ldg_f(v + (i * (ny + 1) + j + 1) * nz + k) - ldg_f(v + (i * (ny + 1) + j) * nz + k)) +
                  (ldg_f(w + (i * ny + j) * (nz + 1) + k + 1) - ldg_f(w + (i * ny + j) * (nz + 1) + k));
-    div[(i * ny + j) * nz + k] = flux / info.cell_m;
+    div[(i * ny + j) * nz + k] = divide(flux, divisor(info.cell_m));
   }
 }
 
@@ -888,7 +905,7 @@ __device__ __forceinline__ void subtract_gradient_planes(const PlumeGridInfo& in
   }
 #pragma unroll
   for (int p = 0; p < PLANES; ++p)
-    if (apply[p]) st_f(f + (i0 + p) * plane + at_jk, value[p] - (above[p] - below[p]) / info.cell_m);
+    if (apply[p]) st_f(f + (i0 + p) * plane + at_jk, value[p] - divide(above[p] - below[p], divisor(info.cell_m)));
 }
 
 template <class T, int PLANES>
@@ -1519,7 +1536,8 @@ static int step(const PlumeStepState* s, const PlumeStepParams* p, void* stream)
   if (p->confinement != 0.0f) {
     float* curl[3] = {s->curl[0], s->curl[1], s->curl[2]};
     float* push[3] = {s->push[0], s->push[1], s->push[2]};
-    if ((status = launch_confinement_push<T>(info, ud, vd, wd, curl, push, p->confinement, 1, st)) != PLUME_OK)
+    if ((status = launch_confinement_push<T>(info, ud, vd, wd, curl, push, p->confinement, 1, st, s->divergence)) !=
+        PLUME_OK)
       return status;
     ff.confinement = 1;
     ff.push[0] = s->push[0];

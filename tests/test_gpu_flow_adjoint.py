@@ -132,3 +132,43 @@ def test_without_smoke_weight_the_source_gradient_is_the_smoke_adjoints(cuda_dev
     a, b = flow_grad.cpu().numpy(), smoke_grad.cpu().numpy()
     assert np.abs(a - b).max() <= 1e-3 * np.abs(b).max()
     assert all(np.isfinite(v) for v in scalars.values())
+
+
+WARM_RTOL = 1e-5  # the warm-started 4-cycle adjoint solve against 12 cycles, on each gradient (measured 3e-7)
+
+
+def test_a_warm_started_adjoint_solve_of_four_cycles_gives_the_same_gradients(cuda_device, case):
+    """The adjoint projection solved by 4 V-cycles from the adjoint pressure of the substep after (the default
+    for a recipe of 4 cycles) against the case's 12 cycles: the gradients agree within WARM_RTOL, so the
+    cheaper solve keeps the finite-difference agreement above."""
+    from plume_b200.adjoint import FlowFit
+
+    recipe, _, _, _, src, tgt, loss, grad, scalars = case
+    fit = FlowFit(recipe, SOURCE, CORNER, SUBSTEPS, "cuda:0", checkpoint_every=4, adjoint_cycles=4)
+    assert fit.warm_start
+    warm_loss, warm_grad, warm_scalars, _ = fit.loss_and_grad(src, tgt)
+    assert warm_loss == loss
+    warm_grad = warm_grad.cpu().numpy().astype(np.float64)
+    source_err = float(np.abs(warm_grad - grad).max()) / float(np.abs(grad).max())
+    print("warm start: source", f"{source_err:.2e}",
+          {name: f"{abs(warm_scalars[name] - scalars[name]) / abs(scalars[name]):.2e}" for name in scalars})
+    assert source_err <= WARM_RTOL
+    for name in scalars:
+        assert abs(warm_scalars[name] - scalars[name]) <= WARM_RTOL * abs(scalars[name])
+
+
+def test_the_tape_budget_changes_the_time_not_the_gradient(cuda_device, case):
+    """With no tape budget every segment is recomputed from its checkpoint; the case's run (the default budget)
+    kept every record from its forward pass. The gradients agree to the atomics' run-to-run rounding."""
+    from plume_b200.adjoint import FlowFit
+
+    recipe, _, _, fit, src, tgt, loss, grad, scalars = case
+    assert fit._taped_from() == 0  # the default budget holds this run's whole tape
+    lean = FlowFit(recipe, SOURCE, CORNER, SUBSTEPS, "cuda:0", checkpoint_every=4, adjoint_cycles=12, tape_bytes=0)
+    assert lean._taped_from() == SUBSTEPS
+    lean_loss, lean_grad, lean_scalars, _ = lean.loss_and_grad(src, tgt)
+    assert lean_loss == loss
+    lean_grad = lean_grad.cpu().numpy().astype(np.float64)
+    assert float(np.abs(lean_grad - grad).max()) <= 1e-6 * float(np.abs(grad).max())
+    for name in scalars:
+        assert abs(lean_scalars[name] - scalars[name]) <= 1e-6 * abs(scalars[name])

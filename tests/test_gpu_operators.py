@@ -80,13 +80,20 @@ def test_emit_matches_the_oracle(cuda_device):
         assert max_rel(host(getattr(c, name).data), getattr(o, name).data, floor=1e-3) < EXP_POW_RTOL, name
 
 
-def test_forces_match_the_oracle(cuda_device):
+# Spacings: a power of two, where the kernels multiply by the exact reciprocal of a spacing in place of dividing
+# by it, and one that is not, where they divide; both must give the oracle's floats.
+CELL_MS = [1.0 / 64.0, 0.1]
+CELL_M_IDS = ["dx-1/64", "dx-0.1"]
+
+
+@pytest.mark.parametrize("cell_m", CELL_MS, ids=CELL_M_IDS)
+def test_forces_match_the_oracle(cuda_device, cell_m):
     from plume_b200.sim.forces import apply_buoyancy, apply_drag
     from plume_b200.sim.turbulence import apply_turbulence
     from plume_b200.sim.vorticity import VorticityConfinement
 
     for cells, faces in CASES:
-        o, c = pair(cells, faces)
+        o, c = pair(cells, faces, cell_m=cell_m)
         O.apply_buoyancy(o, 1.0, 1.0, 0.05, 1.0, 0.02)
         apply_buoyancy(c, 1.0, 1.0, 0.05, 1.0, 0.02)
         assert_same(host(c.v.data), o.v.data, f"buoyancy {cells}")
@@ -103,13 +110,14 @@ def test_forces_match_the_oracle(cuda_device):
             assert_same(host(getattr(c, name).data), getattr(o, name).data, f"{name} after forces {cells}")
 
 
+@pytest.mark.parametrize("cell_m", CELL_MS, ids=CELL_M_IDS)
 @pytest.mark.parametrize("cells,faces", CASES, ids=IDS)
-def test_projection_matches_the_oracle(cuda_device, cells, faces):
+def test_projection_matches_the_oracle(cuda_device, cells, faces, cell_m):
     from plume_b200.sim.multigrid import Multigrid
     from plume_b200.sim.pressure import GaussSeidel, compute_divergence, project
 
     for solver in ("gauss_seidel", "multigrid"):
-        o, c = pair(cells, faces)
+        o, c = pair(cells, faces, cell_m=cell_m)
         if solver == "gauss_seidel":
             os_, cs = O.GaussSeidel(20), GaussSeidel(20)
         else:
@@ -142,11 +150,12 @@ def test_projection_on_a_level_beyond_l2_matches_the_oracle(cuda_device, cells):
         assert_same(host(c.pressure), o.pressure, f"{solver} pressure")
 
 
-def test_multigrid_residual_matches_the_oracle(cuda_device):
+@pytest.mark.parametrize("cell_m", CELL_MS, ids=CELL_M_IDS)
+def test_multigrid_residual_matches_the_oracle(cuda_device, cell_m):
     from plume_b200.sim.multigrid import Multigrid
     from plume_b200.sim.pressure import compute_divergence
 
-    o, c = pair((15, 17, 13), OPEN)
+    o, c = pair((15, 17, 13), OPEN, cell_m=cell_m)
     O.compute_divergence(o)
     compute_divergence(c)
     om, cm = O.Multigrid(o, 1, 2), Multigrid(c, 1, 2)
