@@ -226,6 +226,7 @@ int plume_use_graphs(int32_t enable);
  * (1 << 40 cells): the split kernels measured slower on B200. */
 long long plume_split_scratch_floats(const PlumeGridInfo* info);
 int plume_tune_split(long long min_cells);
+long long plume_split_min_cells(void); /* the current threshold */
 int plume_multigrid_split(const PlumeLevel* levels, int32_t level_count, int32_t cycles, int32_t sweeps,
                           float* scratch, void* stream);
 

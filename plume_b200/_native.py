@@ -119,6 +119,7 @@ SIGNATURES = {
     "plume_use_graphs": [_I],
     "plume_split_scratch_floats": [_INFO],
     "plume_tune_split": [ctypes.c_longlong],
+    "plume_split_min_cells": [],
     "plume_multigrid_split": [ctypes.POINTER(PlumeLevel), _I, _I, _I, _P, _P],
     "plume_smoke_scratch_doubles": [_INFO],
     "plume_advect_scratch_floats": [_INFO],
@@ -186,7 +187,8 @@ def lib() -> ctypes.CDLL:
             fn = getattr(loaded, name)
             fn.argtypes = argtypes
             wide = name in ("plume_advect_scratch_floats", "plume_brick_floats", "plume_norm_scratch_doubles",
-                            "plume_maccormack_scratch_floats", "plume_split_scratch_floats")
+                            "plume_maccormack_scratch_floats", "plume_split_scratch_floats",
+                            "plume_split_min_cells")
             fn.restype = ctypes.c_longlong if wide else ctypes.c_int
         _lib = loaded
     return _lib

@@ -15,6 +15,7 @@
 #include <cooperative_groups.h>
 
 #include <algorithm>
+#include <cstdint>
 #include <cstdlib>
 #include <cstring>
 #include <mutex>
@@ -240,11 +241,9 @@ __global__ void k_split_layout(Dims d, int H, const float* __restrict__ in, floa
   }
 }
 
-// One colour pass over the split arrays, PLANES x-planes per thread: every update is computed before any is
-// stored (a colour reads only the other colour). A cell's six face neighbours all sit in the other colour's
-// array: its x and y neighbours at the same half index m, one plane (ny * H) or one row (H) away; its z
-// neighbours at m - 1 + p and m + p, p = k & 1. `face_load` turns the stencil's (i, j, k) neighbour
-// coordinates into those offsets, so every load is one add from the cell's own index.
+// A split cell's six face neighbours all sit in the other colour's array: its x and y neighbours at the same
+// half index m, one plane (ny * H) or one row (H) away; its z neighbours at m - 1 + p and m + p, p = k & 1.
+// `face` turns the stencil's (i, j, k) neighbour coordinates into those offsets, one add from the cell's index.
 struct SplitCell {
   long other;  // the index of (i, j, k >> 1) in the other colour's array
   int i, j, k, par, plane, row;
@@ -258,32 +257,49 @@ __device__ __forceinline__ SplitCell split_cell(const Dims& d, int H, int i, int
   return SplitCell{((long)((1 - c) * d.n0 + i) * d.n1 + j) * H + (k >> 1), i, j, k, k & 1, d.n1 * H, H};
 }
 
-template <int PLANES>
-__global__ void k_rb_split(PlumeGridInfo info, int H, float* __restrict__ qs, const float* __restrict__ rs, int color,
-                           float relaxation) {
+// The same colour pass with four cells of a row per thread and 16-byte loads: the thread's own q and rhs, the
+// other colour's rows one plane and one row away (x and y neighbours, at the same half indices), and the other
+// colour's own row (z neighbours) plus the one value beyond the four that the row's parity needs. Rows are
+// padded to a multiple of four. Every cell's update is relax_cell's, its neighbours taken from those values.
+__device__ __forceinline__ float4 ld4(const float* p) { return *reinterpret_cast<const float4*>(p); }
+__device__ __forceinline__ float4 ldg4(const float* p) { return __ldg(reinterpret_cast<const float4*>(p)); }
+
+__global__ void k_rb_split4(PlumeGridInfo info, int H, float* __restrict__ qs, const float* __restrict__ rs, int color,
+                            float relaxation) {
   wait_for_previous_grid();
   const int nx = info.dims[0], ny = info.dims[1], nz = info.dims[2];
-  const int i0 = blockIdx.z * PLANES, j = blockIdx.y * blockDim.y + threadIdx.y;
-  const int m = blockIdx.x * blockDim.x + threadIdx.x;
-  if (j >= ny || m >= H) return;
-  const Dims d = dims_of(info);
+  const int i = blockIdx.z, j = blockIdx.y * blockDim.y + threadIdx.y;
+  const int m0 = 4 * (blockIdx.x * blockDim.x + threadIdx.x);
+  if (j >= ny || m0 >= H) return;
+  const int p = (i + j + color) & 1;  // cell k = 2 m + p
+  const long plane = (long)ny * H;
+  const long own = ((long)(color * nx + i) * ny + j) * H + m0;
+  const long oth = ((long)((1 - color) * nx + i) * ny + j) * H + m0;
+  // the other colour is not written by this pass
+  const float4 q4 = ld4(qs + own), r4 = ldg4(rs + own);
+  const float4 x0 = ldg4(qs + (i > 0 ? oth - plane : oth)), x1 = ldg4(qs + (i < nx - 1 ? oth + plane : oth));
+  const float4 y0 = ldg4(qs + (j > 0 ? oth - H : oth)), y1 = ldg4(qs + (j < ny - 1 ? oth + H : oth));
+  const float4 zc = ldg4(qs + oth);
+  const int mz = p == 0 ? m0 - 1 : m0 + 4;
+  const float zx = mz >= 0 && mz < H ? __ldg(qs + oth - m0 + mz) : 0.0f;
+  const float qv[4] = {q4.x, q4.y, q4.z, q4.w}, rv[4] = {r4.x, r4.y, r4.z, r4.w};
+  const float xa[4] = {x0.x, x0.y, x0.z, x0.w}, xb[4] = {x1.x, x1.y, x1.z, x1.w};
+  const float ya[4] = {y0.x, y0.y, y0.z, y0.w}, yb[4] = {y1.x, y1.y, y1.z, y1.w};
+  const float zs[6] = {zx, zc.x, zc.y, zc.z, zc.w, zx};  // the other colour's row at m0 - 1 .. m0 + 4
   const float ghost = ghost_coupling(info);
-  float out[PLANES];
-  bool write[PLANES];
+  float out[4] = {qv[0], qv[1], qv[2], qv[3]};
 #pragma unroll
-  for (int p = 0; p < PLANES; ++p) {
-    const int i = i0 + p, k = 2 * m + ((i + j + color) & 1);
-    write[p] = false;
-    if (i < nx && k < nz) {
-      const long idx = ((long)(color * nx + i) * ny + j) * H + m;
-      const SplitCell cell = split_cell(d, H, i, j, k);
-      auto load = [&](int a, int b, int c) { return qs[cell.face(a, b, c)]; };
-      write[p] = relax_cell(true, info, ghost, i, j, k, qs[idx], __ldg(rs + idx), relaxation, load, out[p]);
-    }
+  for (int n = 0; n < 4; ++n) {
+    const int k = 2 * (m0 + n) + p;
+    if (k >= nz) continue;
+    const float zm = zs[n + p], zp = zs[n + 1 + p];  // at m - 1 + p and m + p
+    auto load = [&](int a, int b, int c) {
+      return a < i ? xa[n] : (a > i ? xb[n] : (b < j ? ya[n] : (b > j ? yb[n] : (c < k ? zm : zp))));
+    };
+    float value;
+    if (relax_cell(true, info, ghost, i, j, k, qv[n], rv[n], relaxation, load, value)) out[n] = value;
   }
-#pragma unroll
-  for (int p = 0; p < PLANES; ++p)
-    if (write[p]) qs[((long)(color * nx + i0 + p) * ny + j) * H + m] = out[p];
+  *reinterpret_cast<float4*>(qs + own) = make_float4(out[0], out[1], out[2], out[3]);
 }
 
 // k_residual_restrict with the fine level in split storage.
@@ -992,8 +1008,11 @@ struct SplitTop {
   int H;
 };
 
+// Half-row length of the split arrays: (nz + 1) / 2 cells, padded to a multiple of four for 16-byte loads.
+static int split_H(const PlumeGridInfo& info) { return ((info.dims[2] + 1) / 2 + 3) / 4 * 4; }
+
 static long split_floats(const PlumeGridInfo& info) {
-  return 2L * info.dims[0] * info.dims[1] * ((info.dims[2] + 1) / 2);
+  return 2L * info.dims[0] * info.dims[1] * split_H(info);
 }
 
 static int split_sweeps(const PlumeGridInfo& info, const SplitTop& sp, int sweeps, const float* coarse_q,
@@ -1005,10 +1024,10 @@ static int split_sweeps(const PlumeGridInfo& info, const SplitTop& sp, int sweep
                                      cell_block(), 0, st, "prolong (split)", cd, d, sp.H, coarse_q, sp.q);
     if (status != PLUME_OK) return status;
   }
-  const dim3 grid((sp.H + TZ - 1) / TZ, (d.n1 + TY - 1) / TY, (d.n0 + 1) / 2);
+  const dim3 grid((sp.H / 4 + TZ - 1) / TZ, (d.n1 + TY - 1) / TY, d.n0);
   for (int s = 0; s < sweeps; ++s)
     for (int color = 0; color < 2; ++color) {
-      int status = launch_solve_kernel(k_rb_split<2>, grid, cell_block(), 0, st, "red-black colour (split)", info,
+      int status = launch_solve_kernel(k_rb_split4, grid, cell_block(), 0, st, "red-black colour (split)", info,
                                        sp.H, sp.q, (const float*)sp.rhs, color, 1.0f);
       if (status != PLUME_OK) return status;
     }
@@ -1231,8 +1250,8 @@ static int v_cycle(const PlumeLevel* levels, int count, int index, Pressure& q, 
 // uniform couplings, swept by colour (not tiled) and at least g_split_min_cells cells.
 static bool use_split(const PlumeLevel* levels, int count, int bottom, const float* scratch) {
   const PlumeGridInfo& info = levels[0].info;
-  return scratch && count >= 2 && bottom > 0 && uniform_level(info) && cells_of(info) >= g_split_min_cells &&
-         cells_of(info) < g_tiled_min_cells;
+  return scratch && ((uintptr_t)scratch & 15) == 0 && count >= 2 && bottom > 0 && uniform_level(info) &&
+         cells_of(info) >= g_split_min_cells && cells_of(info) < g_tiled_min_cells;
 }
 
 static int multigrid_direct(const PlumeLevel* levels, int count, int cycles, int sweeps, cudaStream_t st,
@@ -1242,7 +1261,7 @@ static int multigrid_direct(const PlumeLevel* levels, int count, int cycles, int
   if (use_split(levels, count, bottom, split_scratch)) {
     const PlumeGridInfo& info = levels[0].info;
     const Dims d = dims_of(info);
-    SplitTop sp{split_scratch, split_scratch + split_floats(info), (d.n2 + 1) / 2};
+    SplitTop sp{split_scratch, split_scratch + split_floats(info), split_H(info)};
     const dim3 grid((sp.H + TZ - 1) / TZ, (d.n1 + TY - 1) / TY, d.n0);
     int status = launch_solve_kernel(k_split_layout<true>, grid, cell_block(), 0, st, "pressure to split storage", d,
                                      sp.H, (const float*)levels[0].q, sp.q);
@@ -1410,6 +1429,8 @@ extern "C" int plume_tune_split(long long min_cells) {
   plume::g_split_min_cells = (long)min_cells;
   return PLUME_OK;
 }
+
+extern "C" long long plume_split_min_cells(void) { return plume::g_split_min_cells; }
 
 extern "C" long long plume_split_scratch_floats(const PlumeGridInfo* info) {
   if (!info || info->dims[0] < 1 || info->dims[1] < 1 || info->dims[2] < 1)

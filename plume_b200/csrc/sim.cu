@@ -1399,7 +1399,10 @@ extern "C" int plume_multigrid_correct(const PlumeLevel* levels, int32_t level_c
 extern "C" long long plume_advect_scratch_floats(const PlumeGridInfo* info) {
   if (!info || !valid_dims(info->dims)) return fail(PLUME_ERR_INVALID, "advect_scratch_floats: bad dims");
   const long long nx = info->dims[0], ny = info->dims[1], nz = info->dims[2];
-  return 2 * ((nx + 1) * ny * nz + nx * (ny + 1) * nz + nx * ny * (nz + 1));
+  // the clamp ranges of the two-pass advection, or the colour-split solve's q and rhs (rows padded to 4)
+  const long long ranges = 2 * ((nx + 1) * ny * nz + nx * (ny + 1) * nz + nx * ny * (nz + 1));
+  const long long split = 4 * nx * ny * (((nz + 1) / 2 + 3) / 4 * 4);
+  return ranges > split ? ranges : split;
 }
 
 extern "C" int plume_smoke_scratch_doubles(const PlumeGridInfo* info) {

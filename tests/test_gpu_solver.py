@@ -118,9 +118,10 @@ def test_the_autotuner_picks_the_fastest_candidate_and_restores_the_pressure(tun
 def split_threshold(cuda_device):
     from plume_b200 import _native as N
 
+    default = N.lib().plume_split_min_cells()
     N.call("plume_tune_split", 1)  # every top level runs split, whatever its size
     yield
-    N.call("plume_tune_split", 1 << 23)
+    N.call("plume_tune_split", default)
 
 
 @pytest.mark.parametrize("cells,faces", CASES + [((24, 20, 33), OPEN), ((31, 17, 9), ALL_CLOSED)],

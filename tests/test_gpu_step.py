@@ -166,13 +166,14 @@ def test_a_substep_with_the_split_top_level_gives_the_oracles_floats(cuda_device
         dissipation=dataclasses.replace(recipe.dissipation, smoke_per_s=0.0, cooling_per_s=0.0))
     o, c, os_, cs, derived = stepper_pair(recipe)
     os_.step(1.0, derived.dt_s)
+    default = N.lib().plume_split_min_cells()
     N.call("plume_use_fused_advection", 0)
     N.call("plume_tune_split", 1)
     try:
         cs.step(1.0, derived.dt_s)
     finally:
         N.call("plume_use_fused_advection", 1)
-        N.call("plume_tune_split", 1 << 23)
+        N.call("plume_tune_split", default)
     for name in FIELDS:
         assert_same(host(getattr(c, name).data), getattr(o, name).data, name)
     assert_same(host(c.pressure), o.pressure, "pressure")
