@@ -222,8 +222,9 @@ int plume_use_graphs(int32_t enable);
  * plume_split_scratch_floats(&levels[0].info) floats: when the top level has at least the plume_tune_split
  * threshold of cells, it is swept in colour-split storage (red and black cells in separate arrays, converted in
  * and out around the cycles), so that a colour pass moves only the sectors of the cells it needs. Every value
- * equals plume_multigrid's. plume_step does the same with its advect_scratch. The threshold is off by default
- * (1 << 40 cells): the split kernels measured slower on B200. */
+ * equals plume_multigrid's. plume_step does the same with its advect_scratch. The threshold is 1 << 23 cells
+ * by default (levels whose q and rhs exceed L2, where the split passes measured faster on B200); the scratch
+ * must be 16-byte aligned, or the natural layout runs. */
 long long plume_split_scratch_floats(const PlumeGridInfo* info);
 int plume_tune_split(long long min_cells);
 long long plume_split_min_cells(void); /* the current threshold */

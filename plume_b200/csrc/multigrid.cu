@@ -44,11 +44,11 @@ static long g_tiled_min_cells = 1L << 40;  // measured: per-colour sweeps win wh
 // across the GPU than inside one block on one SM.
 static long g_bottom_max_cells = 2048;
 // The top level runs in colour-split storage (given caller scratch) when it has at least this many cells
-// (plume_tune_split). Off by default: measured on B200 at 256x384x256, every split kernel ran about 1.8x slower
-// than its natural-layout counterpart although it moves fewer sectors (colour pass 109 vs 59 us, residual and
-// restriction 165 vs about 95 us, prolongation 133 vs about 80 us), and the 4-cycle solve took 5.46 ms
-// against 3.53 ms.
-static long g_split_min_cells = 1L << 40;
+// (plume_tune_split): levels whose q and rhs do not fit in L2. Measured on B200 at 256x384x256, 4 V-cycles: the
+// solve takes 3.14 ms split against 3.52 ms natural (colour pass 45.5 against 59.9 us, prolongation 91 against
+// 109 us, residual and restriction about 110 against 107 us, plus 0.15 ms of layout conversions per solve); at
+// 128x192x128, whose levels fit in L2, split is slower (0.97 against 0.78 ms).
+static long g_split_min_cells = 1L << 23;
 static int g_bottom_kind = 0;  // 0: the one-block solve, 1: the cluster solve
 constexpr size_t BOTTOM_MAX_SMEM = 200 * 1024;
 
@@ -213,14 +213,13 @@ __global__ void k_residual_restrict(PlumeGridInfo fine, const float* __restrict_
 
 // ---- the top level in colour-split storage -----------------------------------------------------------------
 // A level larger than L2 is swept from two arrays per quantity, one per colour: cell (i, j, k) of colour
-// c = (i + j + k) & 1 sits at ((c * nx + i) * ny + j) * H + (k >> 1), H = (nz + 1) / 2. A colour pass then
-// reads and writes whole sectors of the cells it needs (its own q and rhs, the other colour's q) instead of
-// sectors shared by both colours. The updates, residuals and prolongation are the natural-layout kernels'
-// functions fed through a loader that maps (i, j, k) to the split index, so every value is the same.
-__device__ __forceinline__ long split_at(const Dims& d, int H, int i, int j, int k) {
-  return ((long)(((i + j + k) & 1) * d.n0 + i) * d.n1 + j) * H + (k >> 1);
-}
-
+// c = (i + j + k) & 1 sits at ((c * nx + i) * ny + j) * H + (k >> 1), H = (nz + 1) / 2 rounded up to a multiple
+// of four. A colour pass then reads and writes whole sectors of the cells it needs (its own q and rhs, the other
+// colour's q) instead of sectors shared by both colours. A cell's six face neighbours all sit in the other
+// colour's array: its x and y neighbours at the same half index m, one plane (ny * H) or one row (H) away; its
+// z neighbours at m - 1 + p and m + p, p = k & 1. The split kernels load whole rows of four half indices and
+// hand the natural-layout stencil functions (relax_cell, residual_cell) those values through a loader, so every
+// value is the same as in the natural layout.
 // natural -> split (to_split) or split -> natural: thread (i, j, m) moves the cells k = 2m and 2m + 1
 template <bool TO_SPLIT>
 __global__ void k_split_layout(Dims d, int H, const float* __restrict__ in, float* __restrict__ out) {
@@ -239,22 +238,6 @@ __global__ void k_split_layout(Dims d, int H, const float* __restrict__ in, floa
       out[s] = 0.0f;  // the padding slot of an odd row
     }
   }
-}
-
-// A split cell's six face neighbours all sit in the other colour's array: its x and y neighbours at the same
-// half index m, one plane (ny * H) or one row (H) away; its z neighbours at m - 1 + p and m + p, p = k & 1.
-// `face` turns the stencil's (i, j, k) neighbour coordinates into those offsets, one add from the cell's index.
-struct SplitCell {
-  long other;  // the index of (i, j, k >> 1) in the other colour's array
-  int i, j, k, par, plane, row;
-  __device__ __forceinline__ long face(int a, int b, int c) const {
-    return other + (long)((a - i) * plane + (b - j) * row + (c < k ? par - 1 : (c > k ? par : 0)));
-  }
-};
-
-__device__ __forceinline__ SplitCell split_cell(const Dims& d, int H, int i, int j, int k) {
-  const int c = (i + j + k) & 1;
-  return SplitCell{((long)((1 - c) * d.n0 + i) * d.n1 + j) * H + (k >> 1), i, j, k, k & 1, d.n1 * H, H};
 }
 
 // The same colour pass with four cells of a row per thread and 16-byte loads: the thread's own q and rhs, the
@@ -302,46 +285,143 @@ __global__ void k_rb_split4(PlumeGridInfo info, int H, float* __restrict__ qs, c
   *reinterpret_cast<float4*>(qs + own) = make_float4(out[0], out[1], out[2], out[3]);
 }
 
-// k_residual_restrict with the fine level in split storage.
-__global__ void k_residual_restrict_split(PlumeGridInfo fine, int H, const float* __restrict__ qs,
-                                          const float* __restrict__ rs, Dims coarse, float* __restrict__ coarse_rhs,
-                                          float* __restrict__ coarse_q) {
+// k_residual_restrict with the fine level in split storage, V (2 or 4) coarse cells kc0 .. kc0 + V - 1 per
+// thread. The children of coarse cell kc sit at half index m = kc in both colours' rows (fk = 2 kc and
+// 2 kc + 1 are one of each colour), so for each child (di, dj, dk) of the V cells the thread loads, as 8- or
+// 16-byte rows at m = kc0 .., the child's own row and rhs, the other colour's row (its z neighbours) and the
+// other colour's four neighbouring rows, plus the value beyond the V that an end's z neighbour needs. Every
+// child's residual is residual_cell's on those values, and each coarse cell adds its children in the
+// reference's order (di, dj, dk).
+template <int V>
+struct Row {
+  float v[V];
+};
+template <int V>
+__device__ __forceinline__ Row<V> ldg_row(const float* p) {
+  Row<V> r;
+  if constexpr (V == 4) {
+    const float4 a = ldg4(p);
+    r.v[0] = a.x, r.v[1] = a.y, r.v[2] = a.z, r.v[3] = a.w;
+  } else {
+    const float2 a = __ldg(reinterpret_cast<const float2*>(p));
+    r.v[0] = a.x, r.v[1] = a.y;
+  }
+  return r;
+}
+
+#ifndef PLUME_RESTRICT_MINB
+#define PLUME_RESTRICT_MINB 3
+#endif
+#ifndef PLUME_RESTRICT_CELLS
+#define PLUME_RESTRICT_CELLS 4
+#endif
+template <int V>
+__global__ void __launch_bounds__(256, PLUME_RESTRICT_MINB)
+    k_residual_restrict_split(PlumeGridInfo fine, int H, const float* __restrict__ qs, const float* __restrict__ rs,
+                              Dims coarse, float* __restrict__ coarse_rhs, float* __restrict__ coarse_q) {
   wait_for_previous_grid();
-  const int i = blockIdx.z, j = blockIdx.y * blockDim.y + threadIdx.y, k = blockIdx.x * blockDim.x + threadIdx.x;
-  if (j >= coarse.n1 || k >= coarse.n2) return;
+  const int i = blockIdx.z, j = blockIdx.y * blockDim.y + threadIdx.y;
+  const int kc0 = V * (blockIdx.x * blockDim.x + threadIdx.x);
+  if (j >= coarse.n1 || kc0 >= coarse.n2) return;
   const Dims fd = dims_of(fine);
   const bool uniform = is_uniform(fine);
   const float ghost = ghost_coupling(fine);
-  float total = 0.0f, count = 0.0f;
+  const long colour_floats = (long)fd.n0 * fd.n1 * H;
+  auto row = [&](int c, int a, int b) {  // (a, b)'s row of colour c at m = kc0, a and b clamped into the level
+    a = imin_(imax_(a, 0), fd.n0 - 1);
+    b = imin_(imax_(b, 0), fd.n1 - 1);
+    return c * colour_floats + ((long)a * fd.n1 + b) * H + kc0;
+  };
+  float total[V], count[V];
+#pragma unroll
+  for (int n = 0; n < V; ++n) total[n] = count[n] = 0.0f;
 #pragma unroll
   for (int di = 0; di < 2; ++di)
 #pragma unroll
-    for (int dj = 0; dj < 2; ++dj)
+    for (int dj = 0; dj < 2; ++dj) {
+      const int fi = 2 * i + di, fj = 2 * j + dj;
+      if (fi >= fd.n0 || fj >= fd.n1) continue;
+      const int c0 = (fi + fj) & 1;  // the colour of child dk = 0; child dk = 1 has the other
 #pragma unroll
       for (int dk = 0; dk < 2; ++dk) {
-        const int fi = 2 * i + di, fj = 2 * j + dj, fk = 2 * k + dk;
-        if (fi < fd.n0 && fj < fd.n1 && fk < fd.n2) {
-          const long idx = split_at(fd, H, fi, fj, fk);
-          const SplitCell cell = split_cell(fd, H, fi, fj, fk);
-          auto load = [&](int a, int b, int c) { return __ldg(qs + cell.face(a, b, c)); };
-          total = total + residual_cell(uniform, fine, ghost, fi, fj, fk, __ldg(qs + idx), __ldg(rs + idx), load);
-          count = count + 1.0f;
+        const int cc = dk == 0 ? c0 : 1 - c0, oc = 1 - cc;
+        const Row<V> own = ldg_row<V>(qs + row(cc, fi, fj)), rhs = ldg_row<V>(rs + row(cc, fi, fj));
+        const Row<V> other = ldg_row<V>(qs + row(oc, fi, fj));
+        const Row<V> xm = ldg_row<V>(qs + row(oc, fi - 1, fj)), xp = ldg_row<V>(qs + row(oc, fi + 1, fj));
+        const Row<V> ym = ldg_row<V>(qs + row(oc, fi, fj - 1)), yp = ldg_row<V>(qs + row(oc, fi, fj + 1));
+        // z neighbours in the other colour's row: child dk = 0 (fk = 2 kc) at m = kc - 1 and kc, child dk = 1
+        // (fk = 2 kc + 1) at m = kc and kc + 1; the first needs m = kc0 - 1, the second m = kc0 + V
+        const float beyond = dk == 0 ? (kc0 >= 1 ? __ldg(qs + row(oc, fi, fj) - 1) : 0.0f)
+                                     : (kc0 + V < H ? __ldg(qs + row(oc, fi, fj) + V) : 0.0f);
+#pragma unroll
+        for (int n = 0; n < V; ++n) {
+          const int fk = 2 * (kc0 + n) + dk;
+          if (fk >= fd.n2) continue;
+          const float zm = dk == 0 ? (n == 0 ? beyond : other.v[n > 0 ? n - 1 : 0]) : other.v[n];
+          const float zp = dk == 0 ? other.v[n] : (n == V - 1 ? beyond : other.v[n < V - 1 ? n + 1 : V - 1]);
+          auto load = [&](int a, int b, int c) {
+            return a < fi ? xm.v[n]
+                          : (a > fi ? xp.v[n] : (b < fj ? ym.v[n] : (b > fj ? yp.v[n] : (c < fk ? zm : zp))));
+          };
+          total[n] = total[n] + residual_cell(uniform, fine, ghost, fi, fj, fk, own.v[n], rhs.v[n], load);
+          count[n] = count[n] + 1.0f;
         }
       }
-  const int out = at(coarse, i, j, k);
-  coarse_rhs[out] = divide(total, divisor(count));  // count is 1, 2, 4 or 8
-  coarse_q[out] = 0.0f;
+    }
+#pragma unroll
+  for (int n = 0; n < V; ++n) {
+    if (kc0 + n >= coarse.n2) break;
+    const int out = at(coarse, i, j, kc0 + n);
+    coarse_rhs[out] = divide(total[n], divisor(count[n]));  // count is 1, 2, 4 or 8
+    coarse_q[out] = 0.0f;
+  }
 }
 
-// k_prolong_add with the fine level in split storage: thread (c, i, j, m) adds to its cell of colour c.
-__global__ void k_prolong_add_split(Dims coarse, Dims fine, int H, const float* __restrict__ cq, float* __restrict__ qs) {
+// k_prolong_add with the fine level in split storage, four cells of a row per thread: thread (c, i, j, m0)
+// adds to its cells m0 .. m0 + 3 of colour c. The four share the coarse sample's x and y axes; along z they
+// read six consecutive coarse columns (m0 - 1 + p .. m0 + 4 + p, clamped), each blended in x then y once
+// (sample_index_space's first lerps, which run per column in that order), and each cell blends its two
+// columns in z: the same float operations as sample_index_space at prolong_point, with fewer loads and less
+// index arithmetic.
+__global__ void k_prolong_add_split4(Dims coarse, Dims fine, int H, const float* __restrict__ cq,
+                                     float* __restrict__ qs) {
   wait_for_previous_grid();
   const int c = blockIdx.z / fine.n0, i = blockIdx.z - c * fine.n0;
-  const int j = blockIdx.y * blockDim.y + threadIdx.y, m = blockIdx.x * blockDim.x + threadIdx.x;
-  const int k = 2 * m + ((i + j + c) & 1);
-  if (j >= fine.n1 || m >= H || k >= fine.n2) return;
-  const long idx = ((long)(c * fine.n0 + i) * fine.n1 + j) * H + m;
-  qs[idx] = qs[idx] + sample_index_space(cq, coarse, prolong_point(i, j, k));
+  const int j = blockIdx.y * blockDim.y + threadIdx.y, m0 = 4 * (blockIdx.x * blockDim.x + threadIdx.x);
+  if (j >= fine.n1 || m0 >= H) return;
+  const int p = (i + j + c) & 1;  // cell k = 2 m + p
+  const F3 g = prolong_point(i, j, 2 * m0 + p);
+  const Axis1 x = axis_of(g[0], coarse.n0, coarse.n1 * coarse.n2), y = axis_of(g[1], coarse.n1, coarse.n2);
+  const float* base = cq + (x.i0 * coarse.n1 + y.i0) * coarse.n2;
+  const int zbase = m0 - 1 + p;
+  float e[6];
+#pragma unroll
+  for (int o = 0; o < 6; ++o) {
+    const float* col = base + imin_(imax_(zbase + o, 0), coarse.n2 - 1);
+    e[o] = lerp_w(lerp_w(__ldg(col), __ldg(col + x.step), x), lerp_w(__ldg(col + y.step), __ldg(col + x.step + y.step), x),
+                  y);
+  }
+  const long own = ((long)(c * fine.n0 + i) * fine.n1 + j) * H + m0;
+  const float4 q4 = ld4(qs + own);
+  float out[4] = {q4.x, q4.y, q4.z, q4.w};
+#pragma unroll
+  for (int n = 0; n < 4; ++n) {
+    const int k = 2 * (m0 + n) + p;
+    if (k >= fine.n2) continue;
+    const F3 gk = prolong_point(i, j, k);
+    const Axis1 z = axis_of(gk[2], coarse.n2, 1);
+    const int off = z.i0 - zbase;  // n, or n + 1 where the lower clamp holds the first cell at column 0
+    float value;
+    if (off == n || off == n + 1) {
+      const float lo = off == n ? e[n] : e[n + 1];
+      const float hi = z.step == 0 ? lo : (off == n ? e[n + 1] : e[n + 2]);
+      value = lerp_w(lo, hi, z);
+    } else {
+      value = sample_index_space(cq, coarse, gk);
+    }
+    out[n] = out[n] + value;
+  }
+  *reinterpret_cast<float4*>(qs + own) = make_float4(out[0], out[1], out[2], out[3]);
 }
 
 // ---- the cluster coarse solve --------------------------------------------------------------------------------
@@ -1020,7 +1100,7 @@ static int split_sweeps(const PlumeGridInfo& info, const SplitTop& sp, int sweep
   const Dims d = dims_of(info);
   if (coarse) {
     const Dims cd = dims_of(*coarse);
-    int status = launch_solve_kernel(k_prolong_add_split, dim3((sp.H + TZ - 1) / TZ, (d.n1 + TY - 1) / TY, 2 * d.n0),
+    int status = launch_solve_kernel(k_prolong_add_split4, dim3((sp.H / 4 + TZ - 1) / TZ, (d.n1 + TY - 1) / TY, 2 * d.n0),
                                      cell_block(), 0, st, "prolong (split)", cd, d, sp.H, coarse_q, sp.q);
     if (status != PLUME_OK) return status;
   }
@@ -1194,7 +1274,9 @@ static int v_cycle(const PlumeLevel* levels, int count, int index, Pressure& q, 
     if (status != PLUME_OK) return status;
     const PlumeLevel& coarse = levels[1];
     const Dims cd = dims_of(coarse.info);
-    if ((status = launch_solve_kernel(k_residual_restrict_split, cell_grid(cd.n0, cd.n1, cd.n2), cell_block(), 0, st,
+    constexpr int V = PLUME_RESTRICT_CELLS;
+    const dim3 grid(((cd.n2 + V - 1) / V + TZ - 1) / TZ, (cd.n1 + TY - 1) / TY, cd.n0);
+    if ((status = launch_solve_kernel(k_residual_restrict_split<V>, grid, cell_block(), 0, st,
                                       "residual and restriction (split)", lv.info, split->H, (const float*)split->q,
                                       (const float*)split->rhs, cd, coarse.rhs, coarse.q)) != PLUME_OK)
       return status;
