@@ -41,8 +41,27 @@ PHASE_BYTES = {"forces": 32.0, "velocity advection": 24.0, "divergence": 16.0, "
                "gradient": 28.0, "scalar advection": 44.0}
 MG_BYTES_PER_CYCLE = 74.0
 # DRAM bytes (read + write) per top-level cell per V-cycle that ncu counted for the pressure-solve kernels of
-# the 128x192x128 step (965.7 MB per substep at 4 cycles); the solve's traffic scales with the level cells.
+# the 128x192x128 step (965.7 MB per substep at 4 cycles, every level in the natural layout); the solve's
+# traffic scales with the level cells.
 MG_TRAFFIC_PER_CYCLE = 965.7e6 / (128 * 192 * 128) / 4
+# A top level in colour-split storage (levels of at least plume_split_min_cells cells), per top-level cell,
+# from one ncu capture of each kernel at 256x384x256 (dram__bytes_read.sum + dram__bytes_write.sum): a colour
+# pass 175.9 MB, the residual and restriction 219.3 MB, the prolongation 158.1 MB per V-cycle (8 passes per
+# cycle at 2 + 2 sweeps); the three layout conversions 461.5 MB per solve. The levels below it are a natural
+# hierarchy of one eighth the cells.
+SPLIT_PASS_TRAFFIC = 175.9e6 / (256 * 384 * 256)
+SPLIT_CYCLE_TRAFFIC = (219.3e6 + 158.1e6) / (256 * 384 * 256)
+SPLIT_SOLVE_TRAFFIC = 461.5e6 / (256 * 384 * 256)
+
+
+def solve_traffic(ncells: int, cycles: int, sweeps: int) -> float:
+    """DRAM bytes of one multigrid solve per substep, from the measured per-cell figures above."""
+    from plume_b200 import _native as N
+
+    if ncells >= N.lib().plume_split_min_cells():
+        top = cycles * (4 * sweeps * SPLIT_PASS_TRAFFIC + SPLIT_CYCLE_TRAFFIC) + SPLIT_SOLVE_TRAFFIC
+        return ncells * (top + cycles * MG_TRAFFIC_PER_CYCLE / 8)
+    return MG_TRAFFIC_PER_CYCLE * cycles * ncells
 
 
 def parse_args():
@@ -700,7 +719,8 @@ def main():
         "resident_gb_per_grid": resident_gb,
         "roofline": {"bound": "hbm", "kernel": f"{dominant} phase of plume_step", "achieved": achieved, "peak": peak,
                      "unit": "GB/s", "frac": achieved / peak if achieved else None,
-                     "traffic": (MG_TRAFFIC_PER_CYCLE * cycles * ncells if dominant == "pressure solve" else None),
+                     "traffic": (solve_traffic(ncells, cycles, recipe.solver.multigrid_sweeps)
+                                 if dominant == "pressure solve" else None),
                      "peak_kind": peak_kind},
         "step_roofline": {"bytes_per_cell_substep": step_bytes,
                           "achieved": step_bytes * ncells * args.steps / (max_ms / 1e3) / 1e9,
