@@ -285,6 +285,48 @@ __global__ void k_rb_split4(PlumeGridInfo info, int H, float* __restrict__ qs, c
   *reinterpret_cast<float4*>(qs + own) = make_float4(out[0], out[1], out[2], out[3]);
 }
 
+// The natural-layout colour pass (k_rb_colour) with four consecutive cells of a row per thread, two of them of
+// the colour: 16-byte loads of the row, of its four neighbouring rows and of rhs, and the one value beyond the
+// four that the row's parity needs. The other colour's two values are stored back unchanged: this pass never
+// writes them, so any thread reading them sees the same floats. Every update is relax_cell's. Rows of a
+// multiple of four cells, 16-byte-aligned arrays.
+template <bool UNIFORM>
+__global__ void k_rb_colour4(PlumeGridInfo info, float* __restrict__ q, const float* __restrict__ rhs, int color,
+                             float relaxation) {
+  wait_for_previous_grid();
+  const int nx = info.dims[0], ny = info.dims[1], nz = info.dims[2];
+  const int i = blockIdx.z, j = blockIdx.y * blockDim.y + threadIdx.y;
+  const int k0 = 4 * (blockIdx.x * blockDim.x + threadIdx.x);
+  if (j >= ny || k0 >= nz) return;
+  const int p = (i + j + color) & 1;  // this colour's cells: k0 + p and k0 + p + 2
+  const long plane = (long)ny * nz, row = ((long)i * ny + j) * nz + k0;
+  const float4 c4 = ld4(q + row), r4 = ldg4(rhs + row);
+  const float4 x0 = ld4(q + (i > 0 ? row - plane : row)), x1 = ld4(q + (i < nx - 1 ? row + plane : row));
+  const float4 y0 = ld4(q + (j > 0 ? row - nz : row)), y1 = ld4(q + (j < ny - 1 ? row + nz : row));
+  const int ze = p == 0 ? k0 - 1 : k0 + 4;
+  const float zx = ze >= 0 && ze < nz ? q[row - k0 + ze] : 0.0f;
+  const float cv[4] = {c4.x, c4.y, c4.z, c4.w}, rv[4] = {r4.x, r4.y, r4.z, r4.w};
+  const float xa[4] = {x0.x, x0.y, x0.z, x0.w}, xb[4] = {x1.x, x1.y, x1.z, x1.w};
+  const float ya[4] = {y0.x, y0.y, y0.z, y0.w}, yb[4] = {y1.x, y1.y, y1.z, y1.w};
+  const float ghost = ghost_coupling(info);
+  float out[4] = {cv[0], cv[1], cv[2], cv[3]};
+#pragma unroll
+  for (int n = 0; n < 2; ++n) {
+#pragma unroll
+    for (int pp = 0; pp < 2; ++pp) {  // a = p + 2 n with p known per thread: both cases unrolled
+      if (pp != p) continue;
+      const int a = pp + 2 * n, k = k0 + a;
+      const float zm = a == 0 ? zx : cv[a > 0 ? a - 1 : 0], zp = a == 3 ? zx : cv[a < 3 ? a + 1 : 3];
+      auto load = [&](int aa, int b, int c) {
+        return aa < i ? xa[a] : (aa > i ? xb[a] : (b < j ? ya[a] : (b > j ? yb[a] : (c < k ? zm : zp))));
+      };
+      float value;
+      if (relax_cell(UNIFORM, info, ghost, i, j, k, cv[a], rv[a], relaxation, load, value)) out[a] = value;
+    }
+  }
+  *reinterpret_cast<float4*>(q + row) = make_float4(out[0], out[1], out[2], out[3]);
+}
+
 // k_residual_restrict with the fine level in split storage, V (2 or 4) coarse cells kc0 .. kc0 + V - 1 per
 // thread. The children of coarse cell kc sit at half index m = kc in both colours' rows (fk = 2 kc and
 // 2 kc + 1 are one of each colour), so for each child (di, dj, dk) of the V cells the thread loads, as 8- or
@@ -1054,6 +1096,12 @@ static void launch_tiled(const PlumeGridInfo& info, Pressure& q, const float* rh
 
 // Levels of at least this many cells (q and rhs over 64 MB) sweep two planes per thread (k_rb_colour_pair).
 constexpr long RB_PAIR_MIN_CELLS = 1L << 23;
+// Smaller levels with rows of a multiple of four cells sweep four cells of a row per thread (k_rb_colour4);
+// PLUME_COLOUR4=0 keeps one cell per thread.
+static const bool g_colour4 = [] {
+  const char* v = getenv("PLUME_COLOUR4");
+  return !(v && v[0] == '0');
+}();
 
 static int colour_sweep(const PlumeGridInfo& info, float* q, const float* rhs, float relaxation, cudaStream_t st) {
   const Dims d = dims_of(info);
@@ -1063,6 +1111,17 @@ static int colour_sweep(const PlumeGridInfo& info, float* q, const float* rhs, f
       int status = uniform_level(info) ? launch_solve_kernel(k_rb_colour_pair<true>, grid, cell_block(), 0, st,
                                                              "red-black colour", info, q, rhs, color, relaxation)
                                        : launch_solve_kernel(k_rb_colour_pair<false>, grid, cell_block(), 0, st,
+                                                             "red-black colour", info, q, rhs, color, relaxation);
+      if (status != PLUME_OK) return status;
+    }
+    return PLUME_OK;
+  }
+  if (g_colour4 && d.n2 % 4 == 0 && (((uintptr_t)q | (uintptr_t)rhs) & 15) == 0) {
+    const dim3 grid((d.n2 / 4 + TZ - 1) / TZ, (d.n1 + TY - 1) / TY, d.n0);
+    for (int color = 0; color < 2; ++color) {
+      int status = uniform_level(info) ? launch_solve_kernel(k_rb_colour4<true>, grid, cell_block(), 0, st,
+                                                             "red-black colour", info, q, rhs, color, relaxation)
+                                       : launch_solve_kernel(k_rb_colour4<false>, grid, cell_block(), 0, st,
                                                              "red-black colour", info, q, rhs, color, relaxation);
       if (status != PLUME_OK) return status;
     }
