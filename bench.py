@@ -281,13 +281,11 @@ def batched_variant(device: str, count: int = 64, frames: int = 48) -> dict:
 
 def adjoint_variant(device: str) -> dict:
     """The differentiable step (BASELINE C3): 96 x 144 x 96 cells, 64 substeps (32 frames of 2), a 16^3 source
-    field centred on cell (48, 8, 48), buoyancy 1.0 and drag 0.2 (no vorticity confinement), a checkpoint every 8
-    substeps. FlowFit's gradient with respect to the source field, heat_buoyancy and drag_per_s (the velocity
-    path included) against the forward substep it differentiates: the forward is timed as plume_step substeps
+    field centred on cell (48, 8, 48), buoyancy 1.0, drag 0.2 and vorticity confinement 0.3, a checkpoint every 8
+    substeps. FlowFit's gradient with respect to the source field, heat_buoyancy, drag_per_s and the confinement
+    strength (the velocity path included) against the forward substep it differentiates: the forward is timed as plume_step substeps
     (the production step) and as FlowFit's taped forward; the adjoint is the backward pass (recomputing each
     segment, then every substep's adjoint). CUDA events around device-synchronised runs."""
-    import dataclasses
-
     import torch
 
     from plume_b200.adjoint import FlowFit
@@ -297,7 +295,6 @@ def adjoint_variant(device: str) -> dict:
     from plume_b200.workloads import plain_step_recipe
 
     recipe = plain_step_recipe((96, 144, 96), cycles=4, frames=32, substeps=2)
-    recipe = dataclasses.replace(recipe, forces=dataclasses.replace(recipe.forces, vorticity_confinement=0.0))
     derived = derive(recipe)
     substeps = 64
     fit = FlowFit(recipe, (16, 16, 16), (40, 0, 40), substeps, device, checkpoint_every=8)
@@ -314,7 +311,7 @@ def adjoint_variant(device: str) -> dict:
     adjoint_ms = total_ms - taped_ms
     _, _, scalars, _ = fit.loss_and_grad(source, target)
     return {"cells": [96, 144, 96], "substeps": substeps, "checkpoint_every": 8,
-            "parameters": ["source field 16^3", "heat_buoyancy", "drag_per_s"],
+            "parameters": ["source field 16^3", "heat_buoyancy", "drag_per_s", "vorticity_confinement"],
             "forward_step_ms_per_substep": step_ms / substeps,
             "forward_taped_ms_per_substep": taped_ms / substeps,
             "adjoint_ms_per_substep": adjoint_ms / substeps,

@@ -507,6 +507,15 @@ int plume_buoyancy_adjoint(const PlumeGridInfo* info, const float* a_v, const fl
                            float smoke_weight, float ambient_k, float dt, double* grad_heat_buoyancy, void* stream);
 int plume_drag_adjoint(const PlumeGridInfo* info, float* a_u, float* a_v, float* a_w, const float* u, const float* v,
                        const float* w, const float wind[3], float keep, float dt, double* grad_drag, void* stream);
+/* plume_confinement_adjoint (vorticity.py:17-84, VorticityConfinement.apply): given a_u, a_v, a_w, the derivative
+ * of the velocity after confinement, adds the confinement's transposed Jacobian so that they become the
+ * derivative of the velocity before it (u, v, w: that velocity, recorded by the caller), and adds
+ * d loss / d strength to *grad_strength (device double). `scratch` holds
+ * plume_confinement_adjoint_scratch_floats(info) floats (10 per cell). No atomics on the face arrays. */
+int plume_confinement_adjoint(const PlumeGridInfo* info, const float* u, const float* v, const float* w, float* a_u,
+                              float* a_v, float* a_w, float strength, float dt, float* scratch, double* grad_strength,
+                              void* stream);
+long plume_confinement_adjoint_scratch_floats(const PlumeGridInfo* info);
 int plume_emit_adjoint(const PlumeGridInfo* info, float* a_temperature, float* a_u, float* a_v, float* a_w,
                        const PlumeEmitter* emitters, int32_t count, int32_t seed, float time_s, float dt, void* stream);
 

@@ -167,6 +167,8 @@ SIGNATURES = {
     "plume_buoyancy_adjoint": [_INFO, _P, _P, _P, _P, _P, _F, _F, _F, _F, _F, _P, _P],
     "plume_drag_adjoint": [_INFO, _P, _P, _P, _P, _P, _P, _F3P, _F, _F, _P, _P],
     "plume_emit_adjoint": [_INFO, _P, _P, _P, _P, ctypes.POINTER(PlumeEmitter), _I, _I, _F, _F, _P],
+    "plume_confinement_adjoint": [_INFO, _P, _P, _P, _P, _P, _P, _F, _F, _P, _P, _P],
+    "plume_confinement_adjoint_scratch_floats": [_INFO],
 }
 
 _lib = None
@@ -188,7 +190,7 @@ def lib() -> ctypes.CDLL:
             fn.argtypes = argtypes
             wide = name in ("plume_advect_scratch_floats", "plume_brick_floats", "plume_norm_scratch_doubles",
                             "plume_maccormack_scratch_floats", "plume_split_scratch_floats",
-                            "plume_split_min_cells")
+                            "plume_split_min_cells", "plume_confinement_adjoint_scratch_floats")
             fn.restype = ctypes.c_longlong if wide else ctypes.c_int
         _lib = loaded
     return _lib

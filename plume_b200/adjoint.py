@@ -194,7 +194,7 @@ class FlowFit:
     through the velocity. No reference counterpart.
 
     Model: SourceFit's (a source field added to the smoke at the start of every substep in its window, then the
-    recipe's step), for recipes without vorticity confinement or turbulence; any smoke weight. The forward run
+    recipe's step); any smoke weight, vorticity confinement and turbulence. The forward run
     steps operator by operator (stepper.py:28-44, the two-pass advection) and keeps the full state (velocity,
     smoke, temperature and the pressure the next solve starts from) every `checkpoint_every` substeps. The
     backward pass walks the segments from the last, recomputes each segment's substeps keeping what the
@@ -204,13 +204,16 @@ class FlowFit:
       projection, whose adjoint is the projection itself (walls zeroed, divergence, solve, gradient: the
       operator is symmetric), solved by `adjoint_cycles` V-cycles (the recipe's count by default) or refined
       to `solve_tol`; MacCormack of the velocity by itself (as field and as advector); drag (d/d drag_per_s);
-      buoyancy (to temperature and smoke, d/d heat_buoyancy); the emitter's blends; the source add (d/d source).
+      turbulence, whose push does not depend on the velocity (its adjoint passes the derivative through);
+      vorticity confinement (through the push, the normalised spin gradient, the spin and the curl; d/d
+      vorticity_confinement); buoyancy (to temperature and smoke, d/d heat_buoyancy); the emitter's blends; the
+      source add (d/d source).
     The forward solve runs the recipe's V-cycles from the previous substep's pressure. The adjoint's solve
     starts, with `warm_start`, from the adjoint pressure of the substep after it (the one solved just before
     in the backward walk), else from zero. Either way the gradient is that of the exact projection, to within
     the residual the solves leave.
 
-    Tape: a substep's record is 12 face arrays and 5 cell arrays. The forward pass of loss_and_grad keeps the
+    Tape: a substep's record is 12 face arrays (15 with confinement) and 5 cell arrays. The forward pass of loss_and_grad keeps the
     records of the last segments whole while they fit `tape_bytes` (by default half the device memory free when
     the gradient is asked for), and the backward pass recomputes only the segments it did not keep. The forward
     is deterministic, so a kept record and a recomputed one are the same floats, and the budget changes the
@@ -222,8 +225,6 @@ class FlowFit:
         from plume_b200.sim.multigrid import Multigrid
 
         f = recipe.forces
-        if f.vorticity_confinement != 0.0 or f.turbulence.strength_mps2 != 0.0:
-            raise ValueError("FlowFit differentiates steps without vorticity confinement or turbulence")
         if recipe.solver.pressure_solver != "multigrid":
             raise ValueError("FlowFit needs the multigrid pressure solve")
         self.recipe, self.derived = recipe, derive(recipe)
@@ -247,6 +248,13 @@ class FlowFit:
         self.factor = torch.empty(1, dtype=torch.float32, device=device)
         self.partial = torch.empty(1024, dtype=torch.float64, device=device)
         self.coeffs = torch.empty(4, dtype=torch.float64, device=device)
+        self.confined = f.vorticity_confinement > 0.0  # the step applies confinement only for a positive strength
+        if self.confined:
+            cells = self.grid.smoke.data.shape
+            self.curl = [torch.empty(cells, dtype=torch.float32, device=device) for _ in range(3)]
+            self.push = [torch.empty(cells, dtype=torch.float32, device=device) for _ in range(3)]
+            self.confinement_scratch = torch.empty(N.lib().plume_confinement_adjoint_scratch_floats(info),
+                                                   dtype=torch.float32, device=device)
 
     # ---- forward -----------------------------------------------------------------------------------------
     def _active(self, time_s: float) -> bool:
@@ -282,6 +290,16 @@ class FlowFit:
         N.call("plume_buoyancy", info, N.ptr(g.v.data), N.ptr(g.smoke.data), N.ptr(g.temperature.data),
                f.gravity_mps2, f.heat_buoyancy, f.smoke_weight, ambient, dt, N.stream())
         rec = {}
+        if self.confined:
+            if record:
+                rec["velocity_before_confinement"] = tuple(x.data.clone() for x in g.velocity_fields())
+            N.call("plume_confinement", info, N.ptr(g.u.data), N.ptr(g.v.data), N.ptr(g.w.data), N.ptrs(*self.curl),
+                   N.ptrs(*self.push), f.vorticity_confinement, dt, 1, N.stream())
+        turbulence = f.turbulence
+        if turbulence.strength_mps2 != 0.0:
+            N.call("plume_turbulence", info, N.ptr(g.u.data), N.ptr(g.v.data), N.ptr(g.w.data), recipe.seed,
+                   turbulence.scale_m, turbulence.strength_mps2, time_s * turbulence.speed_mps / turbulence.scale_m,
+                   dt, N.stream())
         if record:
             rec["velocity_before_drag"] = tuple(x.data.clone() for x in g.velocity_fields())
         if f.drag_per_s != 0.0:
@@ -347,7 +365,7 @@ class FlowFit:
         """Device bytes of one substep's record."""
         g = self.grid
         faces = sum(x.data.numel() for x in g.velocity_fields())
-        return 4 * (4 * faces + 5 * g.smoke.data.numel()) + 8 * 3
+        return 4 * ((5 if self.confined else 4) * faces + 5 * g.smoke.data.numel()) + 8 * 3
 
     def _taped_from(self) -> int:
         """The first substep whose record the forward keeps: whole segments from the end, within the budget."""
@@ -441,6 +459,11 @@ class FlowFit:
             N.call("plume_drag_adjoint", info, *(N.ptr(x) for x in a_vd),
                    *(N.ptr(x) for x in rec["velocity_before_drag"]), N.f3(f.wind_mps), math.exp(-f.drag_per_s * dt),
                    dt, N.ptr(grads[1:2], torch.float64), N.stream())
+        # turbulence's push does not depend on the velocity: its adjoint is the identity
+        if self.confined:
+            N.call("plume_confinement_adjoint", info, *(N.ptr(x) for x in rec["velocity_before_confinement"]),
+                   *(N.ptr(x) for x in a_vd), f.vorticity_confinement, dt, N.ptr(self.confinement_scratch),
+                   N.ptr(grads[2:3], torch.float64), N.stream())
         N.call("plume_buoyancy_adjoint", info, N.ptr(a_vd[1]), N.ptr(rec["smoke"]), N.ptr(rec["temperature"]),
                N.ptr(a_smoke_in), N.ptr(a_heat_in), f.gravity_mps2, f.heat_buoyancy, f.smoke_weight, ambient, dt,
                N.ptr(grads[0:1], torch.float64), N.stream())
@@ -452,7 +475,8 @@ class FlowFit:
         return a_smoke_in, a_heat_in, list(a_vd)
 
     def loss_and_grad(self, source: torch.Tensor, target: torch.Tensor):
-        """(loss, d loss / d source, {"heat_buoyancy": ..., "drag_per_s": ...}, final thickness)."""
+        """(loss, d loss / d source, {"heat_buoyancy": ..., "drag_per_s": ...[, "vorticity_confinement": ...]},
+        final thickness); the confinement strength's derivative when the recipe applies confinement."""
         source = source.to(self.device, torch.float32).contiguous()
         target = target.to(self.device, torch.float32).contiguous()
         taped_from = self._taped_from()
@@ -462,7 +486,7 @@ class FlowFit:
         self.adjoint_grid.pressure.zero_()
         a_heat = torch.zeros_like(g.temperature.data)
         a_vel = [torch.zeros_like(x.data) for x in g.velocity_fields()]
-        grads = torch.zeros(2, dtype=torch.float64, device=self.device)
+        grads = torch.zeros(3, dtype=torch.float64, device=self.device)
         grad_source = torch.zeros(self.source_shape, dtype=torch.float32, device=self.device)
         for segment in reversed(range(len(checkpoints))):
             first = segment * self.every
@@ -476,5 +500,8 @@ class FlowFit:
                 a_smoke, a_heat, a_vel = self._substep_adjoint(n, records[n - first], a_smoke, a_heat, a_vel, grads,
                                                                grad_source)
             del records
-        hb, drag = (float(x) for x in grads.cpu())
-        return loss, grad_source, {"heat_buoyancy": hb, "drag_per_s": drag}, thickness
+        hb, drag, eps = (float(x) for x in grads.cpu())
+        scalars = {"heat_buoyancy": hb, "drag_per_s": drag}
+        if self.confined:
+            scalars["vorticity_confinement"] = eps
+        return loss, grad_source, scalars, thickness

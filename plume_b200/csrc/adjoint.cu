@@ -482,6 +482,194 @@ __global__ void k_drag_adjoint(PlumeGridInfo info, float* __restrict__ a_u, floa
   block_add(part, grad_drag);
 }
 
+// ---- vorticity confinement's adjoint (vorticity.py:17-84) ----------------------------------------------------
+// Forward, per cell: centre velocity c = face averages; curl w = central differences of c (one-sided at the
+// edges); spin s = |w|; g = central differences of s; N = g / |g|; push = sigma (N x w) with sigma =
+// strength * cell_m (zero where |g| < 1e-12); each face adds dt/2 (push of the cell below + of the cell above),
+// the cells clamped into the grid. The adjoint runs those steps backwards, each difference's transpose as a
+// gather over the cells whose stencil holds this one, so no atomics are needed.
+
+// The transpose of one axis's central difference D(c') = (x[hi(c')] - x[lo(c')]) / (span(c') h), hi/lo
+// clamped into 0..n-1 (vorticity.py:25-35): d/dx[t] of sum over c' of e[c'] D(c').
+__device__ __forceinline__ float difference_adjoint(const float* __restrict__ e, long at_t, long stride, int t, int n,
+                                                    float h) {
+  if (n < 2) return 0.0f;
+  auto span = [&](int c) { return (float)(imin_(c + 1, n - 1) - imax_(c - 1, 0)) * h; };
+  float total = 0.0f;
+  if (t >= 1) total += __ldg(e + at_t - stride) / span(t - 1);  // t is the upper point of cell t - 1
+  if (t <= n - 2) total -= __ldg(e + at_t + stride) / span(t + 1);  // the lower point of cell t + 1
+  if (t == n - 1) total += __ldg(e + at_t) / span(t);  // an edge cell is its own upper (or lower) point
+  if (t == 0) total -= __ldg(e + at_t) / span(t);
+  return total;
+}
+
+// Curl and spin of the velocity before confinement (the forward's values, recomputed).
+__global__ void k_conf_adj_curl(PlumeGridInfo info, Vel vel, float* __restrict__ wx, float* __restrict__ wy,
+                                float* __restrict__ wz, float* __restrict__ spin) {
+  const int n[3] = {info.dims[0], info.dims[1], info.dims[2]};
+  const int i = blockIdx.z, j = blockIdx.y * blockDim.y + threadIdx.y, k = blockIdx.x * blockDim.x + threadIdx.x;
+  if (j >= n[1] || k >= n[2]) return;
+  auto centre = [&](int a, int b, int c) {
+    return f3(0.5f * (__ldg(vel.u + at(vel.du, a, b, c)) + __ldg(vel.u + at(vel.du, a + 1, b, c))),
+              0.5f * (__ldg(vel.v + at(vel.dv, a, b, c)) + __ldg(vel.v + at(vel.dv, a, b + 1, c))),
+              0.5f * (__ldg(vel.w + at(vel.dw, a, b, c)) + __ldg(vel.w + at(vel.dw, a, b, c + 1))));
+  };
+  const int cell[3] = {i, j, k};
+  F3 d[3];
+#pragma unroll
+  for (int axis = 0; axis < 3; ++axis) {
+    int lo[3] = {i, j, k}, hi[3] = {i, j, k};
+    lo[axis] = imax_(cell[axis] - 1, 0);
+    hi[axis] = imin_(cell[axis] + 1, n[axis] - 1);
+    const float span = (float)(hi[axis] - lo[axis]);
+    d[axis] = span == 0.0f ? f3(0.0f, 0.0f, 0.0f)
+                           : div3(sub3(centre(hi[0], hi[1], hi[2]), centre(lo[0], lo[1], lo[2])), span * info.cell_m);
+  }
+  const long c = ((long)i * n[1] + j) * n[2] + k;
+  const F3 w = f3(d[1][2] - d[2][1], d[2][0] - d[0][2], d[0][1] - d[1][0]);
+  wx[c] = w[0];
+  wy[c] = w[1];
+  wz[c] = w[2];
+  spin[c] = len3(w);
+}
+
+// The push's adjoint at each cell: the push derivative gathered from the faces beside the cell, then through
+// push = sigma (N x w) and N = g / |g|: writes d/dg (ga) and the direct part of d/dw (wa), and adds
+// d loss / d strength = sum over cells of pbar . cell_m (N x w).
+__global__ void k_conf_adj_push(PlumeGridInfo info, const float* __restrict__ a_u, const float* __restrict__ a_v,
+                                const float* __restrict__ a_w, const float* __restrict__ wx,
+                                const float* __restrict__ wy, const float* __restrict__ wz,
+                                const float* __restrict__ spin, float* __restrict__ gax, float* __restrict__ gay,
+                                float* __restrict__ gaz, float* __restrict__ wax, float* __restrict__ way,
+                                float* __restrict__ waz, float strength, float dt, double* grad_strength) {
+  const int n[3] = {info.dims[0], info.dims[1], info.dims[2]};
+  const int i = blockIdx.z, j = blockIdx.y * blockDim.y + threadIdx.y, k = blockIdx.x * blockDim.x + threadIdx.x;
+  double part = 0.0;
+  if (j < n[1] && k < n[2]) {
+    const int cell[3] = {i, j, k};
+    const Dims cd{n[0], n[1], n[2]};
+    const long c = ((long)i * n[1] + j) * n[2] + k;
+    // pbar: face t of the axis feeds cells max(t-1, 0) and min(t, n-1) with weight dt/2 each
+    const float* a_face[3] = {a_u, a_v, a_w};
+    F3 pbar;
+#pragma unroll
+    for (int axis = 0; axis < 3; ++axis) {
+      const Dims fd{n[0] + (axis == 0), n[1] + (axis == 1), n[2] + (axis == 2)};
+      int up[3] = {i, j, k};
+      up[axis] += 1;
+      const float lo_face = __ldg(a_face[axis] + at(fd, i, j, k));
+      const float hi_face = __ldg(a_face[axis] + at(fd, up[0], up[1], up[2]));
+      float total = lo_face + hi_face;
+      if (cell[axis] == 0) total += lo_face;
+      if (cell[axis] == n[axis] - 1) total += hi_face;
+      pbar[axis] = 0.5f * dt * total;
+    }
+    F3 g = f3(0.0f, 0.0f, 0.0f);
+#pragma unroll
+    for (int axis = 0; axis < 3; ++axis) {
+      int lo[3] = {i, j, k}, hi[3] = {i, j, k};
+      lo[axis] = imax_(cell[axis] - 1, 0);
+      hi[axis] = imin_(cell[axis] + 1, n[axis] - 1);
+      const float span = (float)(hi[axis] - lo[axis]);
+      if (span > 0.0f)
+        g[axis] = (__ldg(spin + at(cd, hi[0], hi[1], hi[2])) - __ldg(spin + at(cd, lo[0], lo[1], lo[2]))) /
+                  (span * info.cell_m);
+    }
+    const float length = len3(g);
+    F3 ga = f3(0.0f, 0.0f, 0.0f), wa = f3(0.0f, 0.0f, 0.0f);
+    if (length >= 1.0e-12f) {
+      const F3 w = f3(__ldg(wx + c), __ldg(wy + c), __ldg(wz + c));
+      const F3 nrm = div3(g, length);
+      const float sigma = strength * info.cell_m;
+      const F3 nbar = mul3(cross3(w, pbar), sigma);
+      wa = mul3(cross3(pbar, nrm), sigma);
+      ga = div3(sub3(nbar, mul3(nrm, dot3(nrm, nbar))), length);
+      const F3 nw = cross3(nrm, w);
+      part = (double)info.cell_m * ((double)pbar[0] * nw[0] + (double)pbar[1] * nw[1] + (double)pbar[2] * nw[2]);
+    }
+    gax[c] = ga[0];
+    gay[c] = ga[1];
+    gaz[c] = ga[2];
+    wax[c] = wa[0];
+    way[c] = wa[1];
+    waz[c] = wa[2];
+  }
+  block_add(part, grad_strength);
+}
+
+// The spin's adjoint: sbar = the transposed differences of ga; w's derivative += sbar w / s (s > 0).
+__global__ void k_conf_adj_spin(PlumeGridInfo info, const float* __restrict__ gax, const float* __restrict__ gay,
+                                const float* __restrict__ gaz, const float* __restrict__ wx,
+                                const float* __restrict__ wy, const float* __restrict__ wz,
+                                const float* __restrict__ spin, float* __restrict__ wax, float* __restrict__ way,
+                                float* __restrict__ waz) {
+  const int n[3] = {info.dims[0], info.dims[1], info.dims[2]};
+  const int i = blockIdx.z, j = blockIdx.y * blockDim.y + threadIdx.y, k = blockIdx.x * blockDim.x + threadIdx.x;
+  if (j >= n[1] || k >= n[2]) return;
+  const long plane = (long)n[1] * n[2], c = i * plane + (long)j * n[2] + k;
+  const float h = info.cell_m;
+  const float sbar = difference_adjoint(gax, c, plane, i, n[0], h) + difference_adjoint(gay, c, n[2], j, n[1], h) +
+                     difference_adjoint(gaz, c, 1, k, n[2], h);
+  const float s = __ldg(spin + c);
+  if (s > 0.0f && sbar != 0.0f) {
+    const float scale = sbar / s;
+    wax[c] += scale * __ldg(wx + c);
+    way[c] += scale * __ldg(wy + c);
+    waz[c] += scale * __ldg(wz + c);
+  }
+}
+
+// The curl's adjoint: the centre velocity's derivative from w's (wa) through the transposed differences:
+// cbar_x = D_z^T(wa_y) - D_y^T(wa_z), cbar_y = D_x^T(wa_z) - D_z^T(wa_x), cbar_z = D_y^T(wa_x) - D_x^T(wa_y).
+__global__ void k_conf_adj_curlT(PlumeGridInfo info, const float* __restrict__ wax, const float* __restrict__ way,
+                                 const float* __restrict__ waz, float* __restrict__ cbx, float* __restrict__ cby,
+                                 float* __restrict__ cbz) {
+  const int n[3] = {info.dims[0], info.dims[1], info.dims[2]};
+  const int i = blockIdx.z, j = blockIdx.y * blockDim.y + threadIdx.y, k = blockIdx.x * blockDim.x + threadIdx.x;
+  if (j >= n[1] || k >= n[2]) return;
+  const long plane = (long)n[1] * n[2], c = i * plane + (long)j * n[2] + k;
+  const float h = info.cell_m;
+  auto dx = [&](const float* e) { return difference_adjoint(e, c, plane, i, n[0], h); };
+  auto dy = [&](const float* e) { return difference_adjoint(e, c, n[2], j, n[1], h); };
+  auto dz = [&](const float* e) { return difference_adjoint(e, c, 1, k, n[2], h); };
+  cbx[c] = dz(way) - dy(waz);
+  cby[c] = dx(waz) - dz(wax);
+  cbz[c] = dy(wax) - dx(way);
+}
+
+// The centre velocity's adjoint onto the faces: face t of an axis averages into cells t - 1 and t.
+__global__ void k_conf_adj_faces(PlumeGridInfo info, float* __restrict__ a_u, float* __restrict__ a_v,
+                                 float* __restrict__ a_w, const float* __restrict__ cbx, const float* __restrict__ cby,
+                                 const float* __restrict__ cbz) {
+  const int nx = info.dims[0], ny = info.dims[1], nz = info.dims[2];
+  int slab = blockIdx.z, axis = 0;
+  if (slab >= nx + 1) {
+    slab -= nx + 1;
+    axis = 1;
+    if (slab >= nx) {
+      slab -= nx;
+      axis = 2;
+    }
+  }
+  const int j = blockIdx.y * blockDim.y + threadIdx.y, k = blockIdx.x * blockDim.x + threadIdx.x;
+  const int n1 = ny + (axis == 1), n2 = nz + (axis == 2);
+  if (j >= n1 || k >= n2) return;
+  const int face[3] = {slab, j, k};
+  const int n[3] = {nx, ny, nz};
+  const Dims cd{nx, ny, nz};
+  const float* cb = axis == 0 ? cbx : (axis == 1 ? cby : cbz);
+  float* a = axis == 0 ? a_u : (axis == 1 ? a_v : a_w);
+  const int t = face[axis];
+  float total = 0.0f;
+  if (t >= 1) {
+    int b[3] = {slab, j, k};
+    b[axis] -= 1;
+    total += __ldg(cb + at(cd, b[0], b[1], b[2]));
+  }
+  if (t <= n[axis] - 1) total += __ldg(cb + at(cd, slab, j, k));
+  a[((long)slab * n1 + j) * n2 + k] += 0.5f * total;
+}
+
 }  // namespace plume
 
 using namespace plume;
@@ -609,4 +797,36 @@ extern "C" int plume_budget_adjoint(const PlumeGridInfo* info, const float* next
   if ((status = launch_status("budget adjoint coefficients")) != PLUME_OK) return status;
   k_budget_adjoint_apply<<<blocks, ADJ_THREADS, 0, st>>>(a_out, n, coeffs, keep, a_next, a_data, a_hat);
   return launch_status("budget adjoint");
+}
+
+extern "C" int plume_confinement_adjoint(const PlumeGridInfo* info, const float* u, const float* v, const float* w,
+                                         float* a_u, float* a_v, float* a_w, float strength, float dt, float* scratch,
+                                         double* grad_strength, void* stream) {
+  ADJ_CHECK(info && u && v && w && a_u && a_v && a_w && scratch && grad_strength,
+            "confinement_adjoint: null argument");
+  ADJ_CHECK(info->dims[0] >= 1 && info->dims[1] >= 1 && info->dims[2] >= 1, "confinement_adjoint: bad dims");
+  cudaStream_t st = as_stream(stream);
+  const Dims d = dims_of(*info);
+  const long n = (long)d.n0 * d.n1 * d.n2;
+  float* wx = scratch;  // curl (3), spin, d/dg (3), d/dw (3); d/dg's arrays then hold d/d centre velocity
+  float *wy = wx + n, *wz = wy + n, *spin = wz + n, *gax = spin + n, *gay = gax + n, *gaz = gay + n;
+  float *wax = gaz + n, *way = wax + n, *waz = way + n;
+  const dim3 grid = cell_grid(d.n0, d.n1, d.n2);
+  k_conf_adj_curl<<<grid, cell_block(), 0, st>>>(*info, make_vel(u, v, w, info->dims), wx, wy, wz, spin);
+  int status = launch_status("confinement adjoint (curl)");
+  if (status != PLUME_OK) return status;
+  k_conf_adj_push<<<grid, cell_block(), 0, st>>>(*info, a_u, a_v, a_w, wx, wy, wz, spin, gax, gay, gaz, wax, way, waz,
+                                                 strength, dt, grad_strength);
+  if ((status = launch_status("confinement adjoint (push)")) != PLUME_OK) return status;
+  k_conf_adj_spin<<<grid, cell_block(), 0, st>>>(*info, gax, gay, gaz, wx, wy, wz, spin, wax, way, waz);
+  if ((status = launch_status("confinement adjoint (spin)")) != PLUME_OK) return status;
+  k_conf_adj_curlT<<<grid, cell_block(), 0, st>>>(*info, wax, way, waz, gax, gay, gaz);
+  if ((status = launch_status("confinement adjoint (curl transpose)")) != PLUME_OK) return status;
+  const dim3 faces((d.n2 + 1 + TZ - 1) / TZ, (d.n1 + 1 + TY - 1) / TY, (d.n0 + 1) + d.n0 + d.n0);
+  k_conf_adj_faces<<<faces, cell_block(), 0, st>>>(*info, a_u, a_v, a_w, gax, gay, gaz);
+  return launch_status("confinement adjoint (faces)");
+}
+
+extern "C" long plume_confinement_adjoint_scratch_floats(const PlumeGridInfo* info) {
+  return info ? 10L * info->dims[0] * info->dims[1] * info->dims[2] : -1;
 }

@@ -84,3 +84,7 @@ def test_newer_entry_points_reject_bad_arguments_without_a_gpu():
     level[0].q = level[0].rhs = level[0].residual = 0x1000  # q aliases the residual array
     assert lib.plume_multigrid_correct(level, 1, 2, ctypes.c_void_p(0x2000), None, None) == -1
     assert b"multigrid_correct" in lib.plume_last_error()
+    assert lib.plume_confinement_adjoint(ctypes.byref(info), None, None, None, None, None, None, 0.3, 0.1, None,
+                                         None, None) == -1
+    assert b"confinement_adjoint" in lib.plume_last_error()
+    assert lib.plume_confinement_adjoint_scratch_floats(ctypes.byref(info)) == 10 * 8 * 8 * 8
