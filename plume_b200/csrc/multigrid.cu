@@ -757,8 +757,63 @@ struct BlockArgs {
   int sweeps;
   PlumeLevel lv[BOTTOM_MAX_LEVELS];
   int offset[BOTTOM_MAX_LEVELS];
-  int f64_offset;  // k_block_solve<true>: the coarsest level's double copy, from this float offset
+  int coef_offset[BOTTOM_MAX_LEVELS];  // a level with overhanging cells: its CellCoef table's float offset (else -1)
+  int f64_offset;  // k_block_solve<true, ...>: the coarsest level's double copy, from this float offset
 };
+
+// The stencil of one cell of a level with overhanging cells (fill_hi < 1), as neighbor_sum and relaxed compute
+// it: the six couplings in neighbor_sum's order (x-, x+, y-, y+, z-, z+; a ghost's coupling, or 0 for a closed
+// face, where the neighbour is outside the level), their sum sc added in that order, and the source scale
+// vc = (cell_volume * cell_m) * cell_m. The one-block solve builds these once per launch for its non-uniform
+// levels, so each sweep's update is loads, products and sums, without neighbor_sum's seven divisions.
+struct CellCoef {
+  float c[6];
+  float sc, vc;
+};
+
+__device__ __forceinline__ CellCoef cell_coef(const PlumeGridInfo& info, int i, int j, int k) {
+  const int c[3] = {i, j, k};
+  CellCoef out;
+  float sc = 0.0f;
+#pragma unroll
+  for (int axis = 0; axis < 3; ++axis) {
+    float area = 1.0f;
+#pragma unroll
+    for (int other = 0; other < 3; ++other)
+      if (other != axis) area = area * cell_fill(info, other, c[other]);
+    const float own = cell_fill(info, axis, c[axis]);
+    float tc[2];
+#pragma unroll
+    for (int side = 0; side < 2; ++side) {
+      const int step = side == 0 ? -1 : 1;
+      const int n = c[axis] + step;
+      if (n >= 0 && n < info.dims[axis]) tc[side] = area / (0.5f * (own + cell_fill(info, axis, n)));
+      else if ((step < 0 && info.open_lo[axis] == 1) || (step > 0 && info.open_hi[axis] == 1))
+        tc[side] = area / (0.5f * own + info.ghost_gap);
+      else tc[side] = 0.0f;
+      out.c[2 * axis + side] = tc[side];
+    }
+    sc = (sc + tc[0]) + tc[1];
+  }
+  out.sc = sc;
+  out.vc = cell_volume(info, i, j, k) * info.cell_m * info.cell_m;
+  return out;
+}
+
+// neighbor_sum's sq from a cell's table entry: the in-level neighbours' coupling * pressure, 0 for the rest,
+// added in its order.
+__device__ __forceinline__ float coef_sum(const CellCoef& e, const float* q, const Dims& d, int i, int j, int k) {
+  const int c[3] = {i, j, k}, n[3] = {d.n0, d.n1, d.n2}, stride[3] = {d.n1 * d.n2, d.n2, 1};
+  const int own = at(d, i, j, k);
+  float sq = 0.0f;
+#pragma unroll
+  for (int axis = 0; axis < 3; ++axis) {
+    const float t0 = c[axis] > 0 ? e.c[2 * axis] * q[own - stride[axis]] : 0.0f;
+    const float t1 = c[axis] < n[axis] - 1 ? e.c[2 * axis + 1] * q[own + stride[axis]] : 0.0f;
+    sq = (sq + t0) + t1;
+  }
+  return sq;
+}
 
 // The coarsest level's sweeps in double (the defect-correction solve's correction cycles; no reference
 // counterpart): q and rhs widened into `dq`/`drhs`, the red-black sweeps of relaxed_f64 over the whole block,
@@ -929,7 +984,48 @@ __device__ __forceinline__ bool stencil_smooth(const PlumeGridInfo& info, float*
   return true;
 }
 
-__device__ __forceinline__ void block_smooth(const PlumeGridInfo& info, float* q, const float* rhs, int sweeps, float relaxation) {
+// block_smooth of a level with overhanging cells from its CellCoef table: relaxed's operations, the couplings
+// read from the table. Out of line, so that the uniform levels' register stencils keep their registers.
+__device__ __noinline__ void table_smooth(Dims d, float* q, const float* rhs, int sweeps, float relaxation,
+                                          const CellCoef* coef) {
+  const int pairs_k = (d.n2 + 1) / 2;
+  const int pairs = d.n0 * d.n1 * pairs_k;
+  const bool one_warp = pairs <= BOTTOM_WARP_PAIRS;
+  if (!one_warp || threadIdx.x < 32) {
+    for (int s = 0; s < sweeps; ++s)
+      for (int color = 0; color < 2; ++color) {
+        const int stride = one_warp ? 32 : BOTTOM_THREADS;
+        Walk w((int)threadIdx.x, stride, d.n1, pairs_k);
+        for (int p = threadIdx.x; p < pairs; p += stride, w.next()) {
+          const int i = w.i, j = w.j;
+          const int k = 2 * w.c + ((i + j + color) & 1);
+          if (k >= d.n2) continue;
+          const int idx = at(d, i, j, k);
+          const CellCoef& e = coef[idx];
+          if (e.sc == 0.0f) continue;
+          const float sq = coef_sum(e, q, d, i, j, k);
+          const float source = e.vc * rhs[idx];
+          const float target = (sq - source) / e.sc;
+          q[idx] = q[idx] + relaxation * (target - q[idx]);
+        }
+        if (one_warp) __syncwarp();
+        else __syncthreads();
+      }
+  }
+  __syncthreads();
+}
+
+// residual_at of a level with overhanging cells from its CellCoef table.
+__device__ __noinline__ float table_residual(const CellCoef* coef, const float* q, const float* rhs, Dims d, int i, int j,
+                                             int k) {
+  const int f = at(d, i, j, k);
+  const CellCoef& e = coef[f];
+  return rhs[f] - divide(coef_sum(e, q, d, i, j, k) - e.sc * q[f], divisor(e.vc));
+}
+
+__device__ __forceinline__ void block_smooth(const PlumeGridInfo& info, float* q, const float* rhs, int sweeps, float relaxation,
+                                             const CellCoef* coef = nullptr) {
+  if (coef) return table_smooth(dims_of(info), q, rhs, sweeps, relaxation, coef);
   if (stencil_smooth(info, q, rhs, sweeps, relaxation)) return;
   const Dims d = dims_of(info);
   const int pairs_k = (d.n2 + 1) / 2;
@@ -958,7 +1054,9 @@ __device__ __forceinline__ void block_smooth(const PlumeGridInfo& info, float* q
   __syncthreads();
 }
 
-template <bool COARSE_F64>
+// TABLES: some level has overhanging cells (CellCoef tables in b.coef_offset); without, the uniform levels'
+// code is compiled alone.
+template <bool COARSE_F64, bool TABLES>
 __global__ void __launch_bounds__(BOTTOM_THREADS) k_block_solve(BlockArgs b) {
   wait_for_previous_grid();
   extern __shared__ float smem[];
@@ -972,6 +1070,18 @@ __global__ void __launch_bounds__(BOTTOM_THREADS) k_block_solve(BlockArgs b) {
       q[n + idx] = b.lv[0].rhs[idx];
     }
   }
+  auto coef_of = [&](int l) -> CellCoef* {
+    if constexpr (TABLES) return b.coef_offset[l] >= 0 ? reinterpret_cast<CellCoef*>(smem + b.coef_offset[l]) : nullptr;
+    else return nullptr;
+  };
+  for (int l = 0; TABLES && l < b.count; ++l) {
+    CellCoef* table = coef_of(l);
+    if (!table) continue;
+    const Dims d = dims_of(b.lv[l].info);
+    Walk w(t, BOTTOM_THREADS, d.n1, d.n2);
+    for (int idx = t; idx < d.n0 * d.n1 * d.n2; idx += BOTTOM_THREADS, w.next())
+      table[idx] = cell_coef(b.lv[l].info, w.i, w.j, w.c);
+  }
   __syncthreads();
   for (int l = 0; l + 1 < b.count; ++l) {
     const PlumeGridInfo& info = b.lv[l].info;
@@ -980,7 +1090,8 @@ __global__ void __launch_bounds__(BOTTOM_THREADS) k_block_solve(BlockArgs b) {
     float* rhs = q + fd.n0 * fd.n1 * fd.n2;
     float* cq = smem + b.offset[l + 1];
     float* crhs = cq + cd.n0 * cd.n1 * cd.n2;
-    block_smooth(info, q, rhs, b.sweeps, 1.0f);
+    const CellCoef* table = coef_of(l);
+    block_smooth(info, q, rhs, b.sweeps, 1.0f, table);
     auto load = [&](int a, int bb, int c) { return q[at(fd, a, bb, c)]; };
     const bool uniform = is_uniform(info);
     const float ghost = ghost_coupling(info);
@@ -995,7 +1106,11 @@ __global__ void __launch_bounds__(BOTTOM_THREADS) k_block_solve(BlockArgs b) {
             const int fi = 2 * i + di, fj = 2 * j + dj, fk = 2 * k + dk;
             if (fi < fd.n0 && fj < fd.n1 && fk < fd.n2) {
               const int f = at(fd, fi, fj, fk);
-              total = total + residual_cell(uniform, info, ghost, fi, fj, fk, q[f], rhs[f], load);
+              if (table) {
+                total = total + table_residual(table, q, rhs, fd, fi, fj, fk);
+              } else {
+                total = total + residual_cell(uniform, info, ghost, fi, fj, fk, q[f], rhs[f], load);
+              }
               count = count + 1.0f;
             }
           }
@@ -1015,7 +1130,7 @@ __global__ void __launch_bounds__(BOTTOM_THREADS) k_block_solve(BlockArgs b) {
       double* staged = reinterpret_cast<double*>(smem + b.f64_offset);
       coarsest_f64(info, q, q + n, sweeps, 1.5, staged, staged + n);
     } else {
-      block_smooth(info, q, q + n, sweeps, 1.5f);
+      block_smooth(info, q, q + n, sweeps, 1.5f, coef_of(b.count - 1));
     }
   }
   for (int l = b.count - 2; l >= 0; --l) {
@@ -1028,7 +1143,7 @@ __global__ void __launch_bounds__(BOTTOM_THREADS) k_block_solve(BlockArgs b) {
     for (int idx = t; idx < n; idx += BOTTOM_THREADS, w.next())
       q[idx] = q[idx] + sample_plain(cq, cd, prolong_point(w.i, w.j, w.c));
     __syncthreads();
-    block_smooth(info, q, q + n, b.sweeps, 1.0f);
+    block_smooth(info, q, q + n, b.sweeps, 1.0f, coef_of(l));
   }
   for (int l = 0; l < b.count; ++l) {
     const Dims d = dims_of(b.lv[l].info);
@@ -1226,6 +1341,23 @@ static int bottom_kind(int coarse_f64) { return coarse_f64 ? 0 : g_bottom_kind; 
 
 static size_t f64_staging_offset(size_t float_bytes) { return (float_bytes + 7) / 8 * 8; }
 
+static bool overhangs(const PlumeGridInfo& info) {
+  return info.fill_hi[0] != 1.0f || info.fill_hi[1] != 1.0f || info.fill_hi[2] != 1.0f;
+}
+
+// The one-block solve's shared memory after its q and rhs arrays (`bytes`): a CellCoef table per level with
+// overhanging cells, each from a 16-byte boundary. With `offsets`, the tables' float offsets (-1: none).
+static size_t coef_bytes(const PlumeLevel* levels, int count, size_t bytes, int* offsets = nullptr) {
+  for (int l = 0; l < count; ++l) {
+    if (offsets) offsets[l] = -1;
+    if (!overhangs(levels[l].info)) continue;
+    bytes = (bytes + 15) / 16 * 16;
+    if (offsets) offsets[l] = (int)(bytes / sizeof(float));
+    bytes += sizeof(CellCoef) * (size_t)cells_of(levels[l].info);
+  }
+  return bytes;
+}
+
 static int bottom_start(const PlumeLevel* levels, int count, size_t* smem_bytes, int coarse_f64) {
   for (int first = 0; first < count; ++first) {
     if (count - first > BOTTOM_MAX_LEVELS || cells_of(levels[first].info) > g_bottom_max_cells) continue;
@@ -1236,6 +1368,7 @@ static int bottom_start(const PlumeLevel* levels, int count, size_t* smem_bytes,
       const long planes = single ? info.dims[0] : (info.dims[0] + CLUSTER - 1) / CLUSTER;
       bytes += 2 * sizeof(float) * (size_t)planes * info.dims[1] * info.dims[2];
     }
+    if (bottom_kind(coarse_f64) == 0) bytes = coef_bytes(levels + first, count - first, bytes);
     if (coarse_f64) bytes = f64_staging_offset(bytes) + 2 * sizeof(double) * (size_t)cells_of(levels[count - 1].info);
     if (bytes > BOTTOM_MAX_SMEM) continue;
     *smem_bytes = bytes;
@@ -1256,14 +1389,12 @@ static int prepare_bottom() {
     status = runtime_status("coarse solve shared memory",
                             cudaFuncSetAttribute(k_cluster_solve, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                                  (int)BOTTOM_MAX_SMEM));
-    if (status == PLUME_OK)
-      status = runtime_status("coarse solve shared memory",
-                              cudaFuncSetAttribute(k_block_solve<false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                                   (int)BOTTOM_MAX_SMEM));
-    if (status == PLUME_OK)
-      status = runtime_status("coarse solve shared memory",
-                              cudaFuncSetAttribute(k_block_solve<true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                                   (int)BOTTOM_MAX_SMEM));
+    for (auto kernel : {k_block_solve<false, false>, k_block_solve<true, false>, k_block_solve<false, true>,
+                        k_block_solve<true, true>})
+      if (status == PLUME_OK)
+        status = runtime_status("coarse solve shared memory",
+                                cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                                     (int)BOTTOM_MAX_SMEM));
     if (status == PLUME_OK)
       status = runtime_status("coarse solve shared memory",
                               cudaFuncSetAttribute(k_coarsest_f64, cudaFuncAttributeMaxDynamicSharedMemorySize,
@@ -1288,8 +1419,13 @@ static int launch_bottom(const PlumeLevel* levels, int count, int sweeps, size_t
       b.offset[l] = offset;
       offset += 2 * (int)cells_of(levels[l].info);
     }
-    b.f64_offset = (int)(f64_staging_offset(sizeof(float) * (size_t)offset) / sizeof(float));
-    return launch_solve_kernel(coarse_f64 ? k_block_solve<true> : k_block_solve<false>, dim3(1), dim3(BOTTOM_THREADS),
+    const size_t table_end = coef_bytes(levels, count, sizeof(float) * (size_t)offset, b.coef_offset);
+    b.f64_offset = (int)(f64_staging_offset(table_end) / sizeof(float));
+    bool tables = false;
+    for (int l = 0; l < count; ++l) tables = tables || b.coef_offset[l] >= 0;
+    auto kernel = coarse_f64 ? (tables ? k_block_solve<true, true> : k_block_solve<true, false>)
+                             : (tables ? k_block_solve<false, true> : k_block_solve<false, false>);
+    return launch_solve_kernel(kernel, dim3(1), dim3(BOTTOM_THREADS),
                                smem, st, "coarse-level block solve", b);
   }
   ClusterArgs b{};
