@@ -1210,7 +1210,11 @@ static void launch_tiled(const PlumeGridInfo& info, Pressure& q, const float* rh
 }
 
 // Levels of at least this many cells (q and rhs over 64 MB) sweep two planes per thread (k_rb_colour_pair).
-constexpr long RB_PAIR_MIN_CELLS = 1L << 23;
+// PLUME_PAIR_MIN_CELLS overrides the threshold (for measurements).
+static const long RB_PAIR_MIN_CELLS = [] {
+  const char* v = getenv("PLUME_PAIR_MIN_CELLS");
+  return v ? atol(v) : 1L << 23;
+}();
 // Smaller levels with rows of a multiple of four cells sweep four cells of a row per thread (k_rb_colour4);
 // PLUME_COLOUR4=0 keeps one cell per thread.
 static const bool g_colour4 = [] {
