@@ -584,9 +584,10 @@ __device__ __forceinline__ void march(const Args<T>& A, int seg, float* sm) {
   }
 }
 
-// MINB: blocks per SM the kernel is compiled for (2: at most 64 registers a thread; 1: up to 128).
+// MINB: resident blocks per SM the kernel is compiled for (4 at 256 threads: at most 64 registers a thread;
+// 3: 80; 2: 128).
 template <class T, int MINB>
-__global__ void __launch_bounds__(NT, MINB * BLOCKS_PER_SM / 2) k_mac_velocity(Args<T> A) {
+__global__ void __launch_bounds__(NT, MINB) k_mac_velocity(Args<T> A) {
   extern __shared__ float sm[];
   int z = blockIdx.z;
   if (z < A.segs[0]) return march<T, 0>(A, z, sm);
@@ -596,7 +597,7 @@ __global__ void __launch_bounds__(NT, MINB * BLOCKS_PER_SM / 2) k_mac_velocity(A
 }
 
 template <class T, int MINB>
-__global__ void __launch_bounds__(NT, MINB * BLOCKS_PER_SM / 2) k_mac_scalars(Args<T> A) {
+__global__ void __launch_bounds__(NT, MINB) k_mac_scalars(Args<T> A) {
   extern __shared__ float sm[];
   march<T, 3>(A, blockIdx.z, sm);
 }
@@ -641,10 +642,15 @@ static int env_int(const char* name) {
 }
 
 // Blocks per SM the march kernels run with (PLUME_MAC_BLOCKS = 1 selects the 128-register form).
+// Blocks per SM the marches are compiled for: PLUME_MAC_BLOCKS = 2, 3 or 4 (the default, BLOCKS_PER_SM).
 static int blocks_per_sm() {
-  static const int b = env_int("PLUME_MAC_BLOCKS") == 1 ? 1 : 2;
+  static const int b = [] {
+    const int v = env_int("PLUME_MAC_BLOCKS");
+    return v == 2 || v == 3 ? v : BLOCKS_PER_SM;
+  }();
   return b;
 }
+
 
 template <class Kernel>
 static int configure(Kernel k, size_t smem, bool& done) {
@@ -674,9 +680,10 @@ long long mac_partial_floats(const PlumeGridInfo& info) {
 template <class T>
 int launch_mac_velocity(const PlumeGridInfo& info, const T* u, const T* v, const T* w, T* u_next, T* v_next,
                         T* w_next, float dt_over_cell, cudaStream_t st) {
-  static bool configured[2] = {false, false};
-  auto kernel = mac::blocks_per_sm() == 1 ? mac::k_mac_velocity<T, 1> : mac::k_mac_velocity<T, 2>;
-  int status = mac::configure(kernel, mac::VELOCITY_SMEM, configured[mac::blocks_per_sm() - 1]);
+  static bool configured[5] = {};
+  const int bps = mac::blocks_per_sm();
+  auto kernel = bps == 2 ? mac::k_mac_velocity<T, 2> : (bps == 3 ? mac::k_mac_velocity<T, 3> : mac::k_mac_velocity<T, 4>);
+  int status = mac::configure(kernel, mac::VELOCITY_SMEM, configured[bps]);
   if (status != PLUME_OK) return status;
   const int nx = info.dims[0], ny = info.dims[1], nz = info.dims[2];
   mac::Args<T> A{};
@@ -704,9 +711,10 @@ int launch_mac_scalars(const PlumeGridInfo& info, const T* u, const T* v, const 
                        const T* temperature, T* smoke_next, T* temperature_next, float smoke_outside,
                        float heat_outside, int uses_outside, float* seg_sums, double* line_partials, int dissipate,
                        float heat_keep, float ambient, float dt_over_cell, cudaStream_t st) {
-  static bool configured[2] = {false, false};
-  auto kernel = mac::blocks_per_sm() == 1 ? mac::k_mac_scalars<T, 1> : mac::k_mac_scalars<T, 2>;
-  int status = mac::configure(kernel, mac::SCALAR_SMEM, configured[mac::blocks_per_sm() - 1]);
+  static bool configured[5] = {};
+  const int bps = mac::blocks_per_sm();
+  auto kernel = bps == 2 ? mac::k_mac_scalars<T, 2> : (bps == 3 ? mac::k_mac_scalars<T, 3> : mac::k_mac_scalars<T, 4>);
+  int status = mac::configure(kernel, mac::SCALAR_SMEM, configured[bps]);
   if (status != PLUME_OK) return status;
   const int nx = info.dims[0], ny = info.dims[1], nz = info.dims[2];
   mac::Args<T> A{};
