@@ -202,7 +202,15 @@ __global__ void k_residual_restrict(PlumeGridInfo fine, const float* __restrict_
         const int fi = 2 * i + di, fj = 2 * j + dj, fk = 2 * k + dk;
         if (fi < fd.n0 && fj < fd.n1 && fk < fd.n2) {
           const int idx = at(fd, fi, fj, fk);
-          total = total + residual_cell(uniform, fine, ghost, fi, fj, fk, __ldg(q + idx), __ldg(rhs + idx), load);
+          if (uniform && fi > 0 && fi < fd.n0 - 1 && fj > 0 && fj < fd.n1 - 1) {
+            const int plane = fd.n1 * fd.n2;
+            const float zm = fk > 0 ? __ldg(q + idx - 1) : 0.0f, zp = fk < fd.n2 - 1 ? __ldg(q + idx + 1) : 0.0f;
+            total = total + residual_xy_interior(fine, ghost, fk, __ldg(q + idx), __ldg(rhs + idx), __ldg(q + idx - plane),
+                                                 __ldg(q + idx + plane), __ldg(q + idx - fd.n2), __ldg(q + idx + fd.n2),
+                                                 zm, zp);
+          } else {
+            total = total + residual_cell(uniform, fine, ghost, fi, fj, fk, __ldg(q + idx), __ldg(rhs + idx), load);
+          }
           count = count + 1.0f;
         }
       }
@@ -247,6 +255,46 @@ __global__ void k_split_layout(Dims d, int H, const float* __restrict__ in, floa
 __device__ __forceinline__ float4 ld4(const float* p) { return *reinterpret_cast<const float4*>(p); }
 __device__ __forceinline__ float4 ldg4(const float* p) { return __ldg(reinterpret_cast<const float4*>(p)); }
 
+// The cells of a row with all four x and y neighbours (the row is neither on a face of the level in x or y):
+// relaxed_uniform's floats with straight-line arithmetic. A z neighbour beyond the level reads 0 (the value
+// beyond the row, and the split rows' padding slots, hold 0), which is what neighbor_sum_uniform adds there; the
+// two cells at the row's ends divide by its couplings, every other cell by six (div6's reciprocal form, with
+// IEEE division where x is outside its range).
+template <int P>
+__device__ __forceinline__ void split_row_interior(const PlumeGridInfo& info, int H, float* __restrict__ qs,
+                                                   const float* __restrict__ rs, long own, long oth, long plane,
+                                                   int m0, float relaxation) {
+  const int nz = info.dims[2];
+  const float4 q4 = ld4(qs + own), r4 = ldg4(rs + own);
+  const float4 x0 = ldg4(qs + oth - plane), x1 = ldg4(qs + oth + plane);
+  const float4 y0 = ldg4(qs + oth - H), y1 = ldg4(qs + oth + H);
+  const float4 zc = ldg4(qs + oth);
+  const int mz = P == 0 ? m0 - 1 : m0 + 4;  // the other colour's value beyond the four that this parity needs
+  const float zx = (P == 0 ? mz >= 0 : mz < H) ? __ldg(qs + oth - m0 + mz) : 0.0f;
+  const float zs[6] = {P == 0 ? zx : 0.0f, zc.x, zc.y, zc.z, zc.w, P == 0 ? 0.0f : zx};  // m0 - 1 .. m0 + 4
+  const float qv[4] = {q4.x, q4.y, q4.z, q4.w}, rv[4] = {r4.x, r4.y, r4.z, r4.w};
+  const float xa[4] = {x0.x, x0.y, x0.z, x0.w}, xb[4] = {x1.x, x1.y, x1.z, x1.w};
+  const float ya[4] = {y0.x, y0.y, y0.z, y0.w}, yb[4] = {y1.x, y1.y, y1.z, y1.w};
+  const float h2 = info.cell_m * info.cell_m;
+  float out[4];
+#pragma unroll
+  for (int n = 0; n < 4; ++n) {
+    const int k = 2 * (m0 + n) + P;
+    out[n] = qv[n];
+    if (k >= nz) continue;
+    const float sq = ((((xa[n] + xb[n]) + ya[n]) + yb[n]) + zs[n + P]) + zs[n + 1 + P];
+    const float x = sq - h2 * rv[n];  // (cell_m * cell_m) * rhs, as relaxed_uniform forms the source
+    float target = div6_core(x);
+    if (k == 0 || k == nz - 1 || !div6_in_range(x)) {
+      const float c0 = k > 0 ? 1.0f : (info.open_lo[2] == 1 ? ghost_coupling(info) : 0.0f);
+      const float c1 = k < nz - 1 ? 1.0f : (info.open_hi[2] == 1 ? ghost_coupling(info) : 0.0f);
+      target = x / ((4.0f + c0) + c1);  // neighbor_sum_uniform's couplings: 4 over x and y, then the z faces
+    }
+    out[n] = qv[n] + relaxation * (target - qv[n]);
+  }
+  *reinterpret_cast<float4*>(qs + own) = make_float4(out[0], out[1], out[2], out[3]);
+}
+
 __global__ void k_rb_split4(PlumeGridInfo info, int H, float* __restrict__ qs, const float* __restrict__ rs, int color,
                             float relaxation) {
   wait_for_previous_grid();
@@ -259,6 +307,11 @@ __global__ void k_rb_split4(PlumeGridInfo info, int H, float* __restrict__ qs, c
   const long own = ((long)(color * nx + i) * ny + j) * H + m0;
   const long oth = ((long)((1 - color) * nx + i) * ny + j) * H + m0;
   // the other colour is not written by this pass
+  if (i > 0 && i < nx - 1 && j > 0 && j < ny - 1) {  // the same for a whole row: one branch per warp
+    if (p == 0) split_row_interior<0>(info, H, qs, rs, own, oth, plane, m0, relaxation);
+    else split_row_interior<1>(info, H, qs, rs, own, oth, plane, m0, relaxation);
+    return;
+  }
   const float4 q4 = ld4(qs + own), r4 = ldg4(rs + own);
   const float4 x0 = ldg4(qs + (i > 0 ? oth - plane : oth)), x1 = ldg4(qs + (i < nx - 1 ? oth + plane : oth));
   const float4 y0 = ldg4(qs + (j > 0 ? oth - H : oth)), y1 = ldg4(qs + (j < ny - 1 ? oth + H : oth));
@@ -275,7 +328,7 @@ __global__ void k_rb_split4(PlumeGridInfo info, int H, float* __restrict__ qs, c
   for (int n = 0; n < 4; ++n) {
     const int k = 2 * (m0 + n) + p;
     if (k >= nz) continue;
-    const float zm = zs[n + p], zp = zs[n + 1 + p];  // at m - 1 + p and m + p
+    const float zm = p ? zs[n + 1] : zs[n], zp = p ? zs[n + 2] : zs[n + 1];  // at m - 1 + p and m + p
     auto load = [&](int a, int b, int c) {
       return a < i ? xa[n] : (a > i ? xb[n] : (b < j ? ya[n] : (b > j ? yb[n] : (c < k ? zm : zp))));
     };
@@ -290,6 +343,40 @@ __global__ void k_rb_split4(PlumeGridInfo info, int H, float* __restrict__ qs, c
 // four that the row's parity needs. The other colour's two values are stored back unchanged: this pass never
 // writes them, so any thread reading them sees the same floats. Every update is relax_cell's. Rows of a
 // multiple of four cells, 16-byte-aligned arrays.
+// k_rb_colour4's two cells of a row with all four x and y neighbours on a uniform level, with split_row_interior's
+// straight-line arithmetic (the value beyond the row's ends reads 0).
+template <int P>
+__device__ __forceinline__ void colour4_row_interior(const PlumeGridInfo& info, float* __restrict__ q,
+                                                     const float* __restrict__ rhs, long row, long plane, int k0,
+                                                     float relaxation) {
+  const int nz = info.dims[2];
+  const float4 c4 = ld4(q + row), r4 = ldg4(rhs + row);
+  const float4 x0 = ld4(q + row - plane), x1 = ld4(q + row + plane);
+  const float4 y0 = ld4(q + row - nz), y1 = ld4(q + row + nz);
+  const int ze = P == 0 ? k0 - 1 : k0 + 4;
+  const float zx = (P == 0 ? ze >= 0 : ze < nz) ? q[row - k0 + ze] : 0.0f;
+  const float cv[4] = {c4.x, c4.y, c4.z, c4.w}, rv[4] = {r4.x, r4.y, r4.z, r4.w};
+  const float xa[4] = {x0.x, x0.y, x0.z, x0.w}, xb[4] = {x1.x, x1.y, x1.z, x1.w};
+  const float ya[4] = {y0.x, y0.y, y0.z, y0.w}, yb[4] = {y1.x, y1.y, y1.z, y1.w};
+  const float h2 = info.cell_m * info.cell_m;
+  float out[4] = {cv[0], cv[1], cv[2], cv[3]};
+#pragma unroll
+  for (int n = 0; n < 2; ++n) {
+    const int a = P + 2 * n, k = k0 + a;
+    const float zm = a == 0 ? zx : cv[a > 0 ? a - 1 : 0], zp = a == 3 ? zx : cv[a < 3 ? a + 1 : 3];
+    const float sq = ((((xa[a] + xb[a]) + ya[a]) + yb[a]) + zm) + zp;
+    const float x = sq - h2 * rv[a];
+    float target = div6_core(x);
+    if (k == 0 || k == nz - 1 || !div6_in_range(x)) {
+      const float c0 = k > 0 ? 1.0f : (info.open_lo[2] == 1 ? ghost_coupling(info) : 0.0f);
+      const float c1 = k < nz - 1 ? 1.0f : (info.open_hi[2] == 1 ? ghost_coupling(info) : 0.0f);
+      target = x / ((4.0f + c0) + c1);
+    }
+    out[a] = cv[a] + relaxation * (target - cv[a]);
+  }
+  *reinterpret_cast<float4*>(q + row) = make_float4(out[0], out[1], out[2], out[3]);
+}
+
 template <bool UNIFORM>
 __global__ void k_rb_colour4(PlumeGridInfo info, float* __restrict__ q, const float* __restrict__ rhs, int color,
                              float relaxation) {
@@ -300,6 +387,11 @@ __global__ void k_rb_colour4(PlumeGridInfo info, float* __restrict__ q, const fl
   if (j >= ny || k0 >= nz) return;
   const int p = (i + j + color) & 1;  // this colour's cells: k0 + p and k0 + p + 2
   const long plane = (long)ny * nz, row = ((long)i * ny + j) * nz + k0;
+  if (UNIFORM && i > 0 && i < nx - 1 && j > 0 && j < ny - 1) {  // the same for a whole row
+    if (p == 0) colour4_row_interior<0>(info, q, rhs, row, plane, k0, relaxation);
+    else colour4_row_interior<1>(info, q, rhs, row, plane, k0, relaxation);
+    return;
+  }
   const float4 c4 = ld4(q + row), r4 = ldg4(rhs + row);
   const float4 x0 = ld4(q + (i > 0 ? row - plane : row)), x1 = ld4(q + (i < nx - 1 ? row + plane : row));
   const float4 y0 = ld4(q + (j > 0 ? row - nz : row)), y1 = ld4(q + (j < ny - 1 ? row + nz : row));
@@ -383,6 +475,7 @@ __global__ void __launch_bounds__(256, PLUME_RESTRICT_MINB)
     for (int dj = 0; dj < 2; ++dj) {
       const int fi = 2 * i + di, fj = 2 * j + dj;
       if (fi >= fd.n0 || fj >= fd.n1) continue;
+      const bool xy_interior = uniform && fi > 0 && fi < fd.n0 - 1 && fj > 0 && fj < fd.n1 - 1;
       const int c0 = (fi + fj) & 1;  // the colour of child dk = 0; child dk = 1 has the other
 #pragma unroll
       for (int dk = 0; dk < 2; ++dk) {
@@ -401,6 +494,12 @@ __global__ void __launch_bounds__(256, PLUME_RESTRICT_MINB)
           if (fk >= fd.n2) continue;
           const float zm = dk == 0 ? (n == 0 ? beyond : other.v[n > 0 ? n - 1 : 0]) : other.v[n];
           const float zp = dk == 0 ? other.v[n] : (n == V - 1 ? beyond : other.v[n < V - 1 ? n + 1 : V - 1]);
+          if (xy_interior) {
+            total[n] = total[n] + residual_xy_interior(fine, ghost, fk, own.v[n], rhs.v[n], xm.v[n], xp.v[n], ym.v[n],
+                                                       yp.v[n], zm, zp);
+            count[n] = count[n] + 1.0f;
+            continue;
+          }
           auto load = [&](int a, int b, int c) {
             return a < fi ? xm.v[n]
                           : (a > fi ? xp.v[n] : (b < fj ? ym.v[n] : (b > fj ? yp.v[n] : (c < fk ? zm : zp))));

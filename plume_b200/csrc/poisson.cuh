@@ -116,11 +116,26 @@ __device__ __forceinline__ void neighbor_sum_uniform(const PlumeGridInfo& info, 
   }
 }
 
+// x / 6, correctly rounded, by the reciprocal with one remainder correction (Brisebarre, Muller and Raina,
+// "Accelerating correctly rounded floating-point division when the divisor is known in advance", IEEE Trans.
+// Computers 53(8), 2004): q0 = x * RN(1/6), r = fma(-q0, 6, x) (exact), q = fma(r, RN(1/6), q0). For d = 6 this
+// returns IEEE x / 6 whenever x and the quotient are normal floats (every float x checked against the division;
+// the failures are all subnormal); below |x| = 2^-120, and for zeros, infinities and NaN, it divides.
+__device__ __forceinline__ bool div6_in_range(float x) { return fabsf(x) >= 0x1p-120f && fabsf(x) <= 0x1p+127f; }
+__device__ __forceinline__ float div6_core(float x) {
+  constexpr float z = 0x1.555556p-3f;  // RN(1/6)
+  const float q0 = x * z;
+  return __fmaf_rn(__fmaf_rn(-q0, 6.0f, x), z, q0);
+}
+__device__ __forceinline__ float div6(float x) { return div6_in_range(x) ? div6_core(x) : x / 6.0f; }
+
 template <class Load>
 __device__ __forceinline__ bool relaxed_uniform(const PlumeGridInfo& info, float ghost, int i, int j, int k, float q,
                                                 float rhs, float relaxation, Load load, float& out) {
   float sq, sc;
-  if (i > 0 && j > 0 && k > 0 && i < info.dims[0] - 1 && j < info.dims[1] - 1 && k < info.dims[2] - 1) {
+  const bool interior =
+      i > 0 && j > 0 && k > 0 && i < info.dims[0] - 1 && j < info.dims[1] - 1 && k < info.dims[2] - 1;
+  if (interior) {
     // an interior cell: six unit couplings; the same sums as neighbor_sum_uniform (0 + x == x in value)
     sq = ((((load(i - 1, j, k) + load(i + 1, j, k)) + load(i, j - 1, k)) + load(i, j + 1, k)) + load(i, j, k - 1)) +
          load(i, j, k + 1);
@@ -130,7 +145,7 @@ __device__ __forceinline__ bool relaxed_uniform(const PlumeGridInfo& info, float
   }
   if (sc == 0.0f) return false;
   float source = info.cell_m * info.cell_m * rhs;  // cell volume 1: (1 * cell_m) * cell_m == cell_m * cell_m
-  float target = (sq - source) / sc;
+  float target = interior ? div6(sq - source) : (sq - source) / sc;
   out = q + relaxation * (target - q);
   return true;
 }
@@ -140,6 +155,19 @@ __device__ __forceinline__ float residual_uniform(const PlumeGridInfo& info, flo
                                                   float rhs, Load load) {
   float sq, sc;
   neighbor_sum_uniform(info, ghost, i, j, k, load, sq, sc);
+  return rhs - divide(sq - sc * q, divisor(info.cell_m * info.cell_m));
+}
+
+// residual_uniform for a cell whose four x and y neighbours all exist, at any k, from the neighbours passed in:
+// neighbor_sum_uniform's sums in its order (a missing z neighbour adds 0 and its face's coupling), so every value
+// is residual_uniform's.
+__device__ __forceinline__ float residual_xy_interior(const PlumeGridInfo& info, float ghost, int k, float q, float rhs,
+                                                      float x0, float x1, float y0, float y1, float zm, float zp) {
+  const bool lo = k > 0, hi = k < info.dims[2] - 1;
+  const float sq = (((((0.0f + x0) + x1) + y0) + y1) + (lo ? zm : 0.0f)) + (hi ? zp : 0.0f);
+  const float c0 = lo ? 1.0f : (info.open_lo[2] == 1 ? ghost : 0.0f);
+  const float c1 = hi ? 1.0f : (info.open_hi[2] == 1 ? ghost : 0.0f);
+  const float sc = (4.0f + c0) + c1;  // (((0 + 1) + 1) + 1) + 1 == 4 over x and y, then the two z faces
   return rhs - divide(sq - sc * q, divisor(info.cell_m * info.cell_m));
 }
 

@@ -121,9 +121,11 @@ def smoke_puff_recipe(cells=(64, 96, 64), frames: int = 48):
     return resolve_table(table, "smoke_puff_c1")
 
 
-def run_plain_steps(cells=(128, 192, 128), substeps: int = 1, device: str = "cuda:0", render: bool = False):
+def run_plain_steps(cells=(128, 192, 128), substeps: int = 1, device: str = "cuda:0", render: bool = False,
+                    storage: str = "f32"):
     """Steps the seeded operator-level state `substeps` times through Stepper.step (and renders one frame when
-    `render`), for profiling single kernels on a small case."""
+    `render`), for profiling single kernels on a small case; `storage` ("f32", "bf16" or "f16") is the element
+    type of the stored fields."""
     import torch
 
     from plume_b200.recipe.derived import derive
@@ -135,9 +137,10 @@ def run_plain_steps(cells=(128, 192, 128), substeps: int = 1, device: str = "cud
     recipe = plain_step_recipe(tuple(cells))
     derived = derive(recipe)
     d = recipe.domain
-    grid = make_grid(derived, d.cell_m, d.faces, d.ambient_k, device)
+    dtype = {"f32": torch.float32, "bf16": torch.bfloat16, "f16": torch.float16}[storage]
+    grid = make_grid(derived, d.cell_m, d.faces, d.ambient_k, device, storage=dtype)
     for name, values in operator_fields(derived.cells, DEFAULT_SEED, d.ambient_k).items():
-        getattr(grid, name).data.copy_(torch.from_numpy(values))
+        getattr(grid, name).data.copy_(torch.from_numpy(values).to(dtype))
     stepper = Stepper(grid, recipe)
     for n in range(substeps):
         stepper.step(n * derived.dt_s, derived.dt_s)
@@ -155,8 +158,10 @@ if __name__ == "__main__":
     ap.add_argument("--cells", default="128,192,128")
     ap.add_argument("--substeps", type=int, default=1)
     ap.add_argument("--render", action="store_true")
+    ap.add_argument("--storage", choices=("f32", "bf16", "f16"), default="f32")
     args = ap.parse_args()
-    run_plain_steps(tuple(int(x) for x in args.cells.split(",")), args.substeps, render=args.render)
+    run_plain_steps(tuple(int(x) for x in args.cells.split(",")), args.substeps, render=args.render,
+                    storage=args.storage)
     print("ok")
 
 
