@@ -285,9 +285,10 @@ __global__ void __launch_bounds__(256, 4) k_raymarch(MarchArgs a, const T* __res
     const float margin = (8.0f * fmaxf(fabsf(s0), fabsf(s1)) + 6.0f * box_far) * 5.9604645e-8f / info.cell_m +
                          cells_far * 9.5367432e-7f + 1.0e-3f;
     const F3 delta = mul3(direction, step_m / info.cell_m);
+    const Divisor cell = divisor(info.cell_m);  // (position - origin) / cell_m: a product when cell_m is 2^-e
     for (int s = 0; s < steps; ++s) {
       F3 position = add3(origin, mul3(direction, s0 + ((float)s + 0.5f) * step_m));
-      F3 g = sub3(div3(sub3(position, box_origin), info.cell_m), f3(0.5f, 0.5f, 0.5f));
+      F3 g = sub3(divide3(sub3(position, box_origin), cell), f3(0.5f, 0.5f, 0.5f));
       bool empty = false;
       if (bricks) {
         const int i0 = (int)fminf(fmaxf(g[0], 0.0f), (float)(a.d.n0 - 1));
