@@ -82,37 +82,55 @@ __global__ void k_brick_max(Dims d, const T* __restrict__ f, float* __restrict__
   bricks[at(b, bi, bj, bk)] = best;
 }
 
-// light_volume_kernel (light_volume.py:18-33): one thread per cell marches toward the light in at most
-// half-cell steps to the box edge and writes exp(-opacity * column * cell_m). With `bricks`, samples whose
-// corners are all <= 0 add exactly 0: the march steps over the whole run of them that lies in one brick.
+// light_volume_kernel (light_volume.py:18-33): each lit cell marches toward the light in at most half-cell
+// steps to the box edge and gets exp(-opacity * column * cell_m). With `bricks`, samples whose corners are all
+// <= 0 add exactly 0: the march steps over the whole run of them that lies in one brick.
 //
 // With `march_cells`, only the cells a camera march of the same smoke can read get their value: a march sample
 // reads the light at its eight corners only when its alpha is > 0, so when one of those corners holds smoke
 // > 0; the corners of every sample that reads cell c lie in {c-1, c, c+1}^3. So c is read only if one of those
 // 27 cells holds smoke > 0 (tested first through the bricks of the lower corners {c-1, c}^3, which hold the
 // largest smoke of every such corner). Every other cell gets 1.
+//
+// Arithmetic: the trilinear blends are fma(t, b - a, a) and the column adds each sample with one fma, one
+// rounding fewer than light_volume_kernel's lerp and multiply-add, so the light agrees with the reference's to
+// about an ulp of the column (held to 1e-5 relative); the empty-space skipping and the march_cells form change
+// no bit of it.
+__device__ __forceinline__ float lerp_fma(float a, float b, float t) { return __fmaf_rn(t, b - a, a); }
+
 template <class T>
-__global__ void k_light_volume(Dims d, const T* __restrict__ smoke, F3 toward, float cell_m, float opacity,
-                               float* __restrict__ light, const float* __restrict__ bricks, int march_cells) {
-  const int i = blockIdx.z, j = blockIdx.y * blockDim.y + threadIdx.y, k = blockIdx.x * blockDim.x + threadIdx.x;
-  if (j >= d.n1 || k >= d.n2) return;
+__device__ __forceinline__ float sample_fma(const T* __restrict__ f, const Dims& d, F3 g) {
+  const Axis1 x = axis_of(g[0], d.n0, d.n1 * d.n2), y = axis_of(g[1], d.n1, d.n2), z = axis_of(g[2], d.n2, 1);
+  const T* p = f + (x.i0 * d.n1 + y.i0) * d.n2 + z.i0;
+  const float c00 = lerp_fma(ldg_f(p), ldg_f(p + x.step), x.t);
+  const float c10 = lerp_fma(ldg_f(p + y.step), ldg_f(p + x.step + y.step), x.t);
+  const float c01 = lerp_fma(ldg_f(p + z.step), ldg_f(p + x.step + z.step), x.t);
+  const float c11 = lerp_fma(ldg_f(p + y.step + z.step), ldg_f(p + x.step + y.step + z.step), x.t);
+  return lerp_fma(lerp_fma(c00, c10, y.t), lerp_fma(c01, c11, y.t), z.t);
+}
+
+// Whether a camera march of this smoke reads the light at cell (i, j, k) (the march_cells test above).
+template <class T>
+__device__ __forceinline__ bool read_by_march(const Dims& d, const T* __restrict__ smoke, const float* __restrict__ bricks,
+                                              int i, int j, int k) {
   const Dims bd = brick_dims(d);
-  if (march_cells) {
-    bool read = false;
-    for (int a = imax_(i - 1, 0); a <= i; ++a)
-      for (int b = imax_(j - 1, 0); b <= j; ++b)
-        for (int c = imax_(k - 1, 0); c <= k; ++c) read |= __ldg(bricks + at(bd, a / BRICK, b / BRICK, c / BRICK)) > 0.0f;
-    if (read) {
-      read = false;
-      for (int a = imax_(i - 1, 0); a <= imin_(i + 1, d.n0 - 1); ++a)
-        for (int b = imax_(j - 1, 0); b <= imin_(j + 1, d.n1 - 1); ++b)
-          for (int c = imax_(k - 1, 0); c <= imin_(k + 1, d.n2 - 1); ++c) read |= ldg_f(smoke + at(d, a, b, c)) > 0.0f;
-    }
-    if (!read) {
-      light[at(d, i, j, k)] = 1.0f;
-      return;
-    }
-  }
+  bool read = false;
+  for (int a = imax_(i - 1, 0); a <= i; ++a)
+    for (int b = imax_(j - 1, 0); b <= j; ++b)
+      for (int c = imax_(k - 1, 0); c <= k; ++c) read |= __ldg(bricks + at(bd, a / BRICK, b / BRICK, c / BRICK)) > 0.0f;
+  if (!read) return false;
+  read = false;
+  for (int a = imax_(i - 1, 0); a <= imin_(i + 1, d.n0 - 1); ++a)
+    for (int b = imax_(j - 1, 0); b <= imin_(j + 1, d.n1 - 1); ++b)
+      for (int c = imax_(k - 1, 0); c <= imin_(k + 1, d.n2 - 1); ++c) read |= ldg_f(smoke + at(d, a, b, c)) > 0.0f;
+  return read;
+}
+
+// The light of one cell: its march toward the light.
+template <class T>
+__device__ __forceinline__ float light_at(const Dims& d, const T* __restrict__ smoke, F3 toward, float cell_m,
+                                          float opacity, const float* __restrict__ bricks, int i, int j, int k) {
+  const Dims bd = brick_dims(d);
   const F3 half = f3(0.5f, 0.5f, 0.5f);
   F3 start = add3(f3((float)i, (float)j, (float)k), half);
   F3 box_max = f3((float)d.n0, (float)d.n1, (float)d.n2);
@@ -122,14 +140,16 @@ __global__ void k_light_volume(Dims d, const T* __restrict__ smoke, F3 toward, f
   float column = 0.0f;
   if (steps > 0) {
     float step = length / (float)steps;
-    // the computed points are start + toward * ((s + 0.5) * step) - 0.5: within (2 * length + 2 * extent) * 2^-24
-    // cells of the exact line
+    // the computed points (i, j, k) + toward * ((s + 0.5) * step), from the cell's lower corner, are within
+    // (2 * length + 2 * extent) * 2^-24 cells of the exact line
     const float extent = (float)(imax_(imax_(d.n0, d.n1), d.n2) + 1);
     const float margin = (4.0f * length + 4.0f * extent) * 5.9604645e-8f + 1.0e-3f;
     const F3 delta = mul3(toward, step);
+    const F3 corner = f3((float)i, (float)j, (float)k);
     for (int s = 0; s < steps; ++s) {
-      F3 position = add3(start, mul3(toward, ((float)s + 0.5f) * step));
-      const F3 g = sub3(position, half);
+      const float t = ((float)s + 0.5f) * step;
+      const F3 g = f3(__fmaf_rn(toward[0], t, corner[0]), __fmaf_rn(toward[1], t, corner[1]),
+                      __fmaf_rn(toward[2], t, corner[2]));
       if (bricks) {
         const int i0 = (int)fminf(fmaxf(g[0], 0.0f), (float)(d.n0 - 1));
         const int j0 = (int)fminf(fmaxf(g[1], 0.0f), (float)(d.n1 - 1));
@@ -139,10 +159,46 @@ __global__ void k_light_volume(Dims d, const T* __restrict__ smoke, F3 toward, f
           continue;
         }
       }
-      column = column + fmax_(sample_index_space(smoke, d, g), 0.0f) * step;
+      column = __fmaf_rn(fmax_(sample_fma(smoke, d, g), 0.0f), step, column);
     }
   }
-  light[at(d, i, j, k)] = exp_f(-opacity * column * cell_m);
+  return exp_f(-opacity * column * cell_m);
+}
+
+// A block of 32 x 8 threads covers 32 cells along z of LIGHT_ROWS * 8 rows of one x-plane; each warp takes
+// LIGHT_ROWS rows. The warp first gives every cell that no march reads its 1 and queues the others in shared
+// memory in row order, then marches the queue 32 cells at a time, so its lanes stay busy where only part of a
+// row is lit.
+constexpr int LIGHT_ROWS = 8;
+
+template <class T>
+__global__ void __launch_bounds__(256, 5) k_light_volume(Dims d, const T* __restrict__ smoke, F3 toward, float cell_m,
+                                                      float opacity, float* __restrict__ light,
+                                                      const float* __restrict__ bricks, int march_cells) {
+  __shared__ unsigned short queue[8][LIGHT_ROWS * 32];
+  const int lane = threadIdx.x, warp = threadIdx.y;
+  const int i = blockIdx.z, k = blockIdx.x * 32 + lane, j0 = (blockIdx.y * 8 + warp) * LIGHT_ROWS;
+  int count = 0;
+#pragma unroll 1
+  for (int r = 0; r < LIGHT_ROWS; ++r) {
+    const int j = j0 + r;
+    bool lit = j < d.n1 && k < d.n2;
+    if (lit && march_cells && !read_by_march(d, smoke, bricks, i, j, k)) {
+      light[at(d, i, j, k)] = 1.0f;
+      lit = false;
+    }
+    const unsigned vote = __ballot_sync(0xffffffffu, lit);
+    if (lit) queue[warp][count + __popc(vote & ((1u << lane) - 1u))] = (unsigned short)(r * 32 + lane);
+    count += __popc(vote);
+  }
+  __syncwarp();
+#pragma unroll 1
+  for (int b = 0; b < count; b += 32) {
+    if (b + lane < count) {
+      const int e = queue[warp][b + lane], j = j0 + e / 32, kk = blockIdx.x * 32 + e % 32;
+      light[at(d, i, j, kk)] = light_at(d, smoke, toward, cell_m, opacity, bricks, i, j, kk);
+    }
+  }
 }
 
 // blur_axis_kernel (normal_field.py:12-22); weights in constant memory.
@@ -366,8 +422,8 @@ static int light_volume(const Dims& d, const T* smoke, F3 toward, float cell_m, 
     int status = launch_status("smoke brick map");
     if (status != PLUME_OK) return status;
   }
-  k_light_volume<T><<<cell_grid(d.n0, d.n1, d.n2), cell_block(), 0, st>>>(d, smoke, toward, cell_m, opacity, light,
-                                                                          bricks, march_cells);
+  const dim3 grid((d.n2 + 31) / 32, (d.n1 + 8 * LIGHT_ROWS - 1) / (8 * LIGHT_ROWS), d.n0);
+  k_light_volume<T><<<grid, dim3(32, 8), 0, st>>>(d, smoke, toward, cell_m, opacity, light, bricks, march_cells);
   return launch_status("light volume");
 }
 
