@@ -64,6 +64,29 @@ __device__ __forceinline__ float samples_in_brick(const Dims& d, F3 g, F3 delta,
   return count;
 }
 
+// samples_in_brick with the divisions by |delta| replaced by products with their reciprocals `per_cell`
+// (computed once per march). The count may move by a few ulps, far inside the margin, so every sample it
+// counts still lies in the brick.
+__device__ __forceinline__ float samples_in_brick_by(const Dims& d, F3 g, F3 delta, F3 per_cell, float margin) {
+  const int n[3] = {d.n0, d.n1, d.n2};
+  float count = 3.0e38f;
+#pragma unroll
+  for (int a = 0; a < 3; ++a) {
+    if (delta[a] == 0.0f) continue;
+    const int b = (int)fminf(fmaxf(g[a], 0.0f), (float)(n[a] - 1)) / BRICK;
+    float room;
+    if (delta[a] > 0.0f) {
+      if (b == (n[a] - 1) / BRICK) continue;
+      room = (float)((b + 1) * BRICK) - g[a];
+    } else {
+      if (b == 0) continue;
+      room = g[a] - (float)(b * BRICK);
+    }
+    count = fminf(count, (room - margin) * per_cell[a]);
+  }
+  return count;
+}
+
 // Index of the sample a march continues from after the sample `s` in an empty brick: past every later sample
 // that `samples_in_brick` places in the same brick, and at most `end`.
 __device__ __forceinline__ int past_brick(int s, int end, float count) {
@@ -99,8 +122,8 @@ __global__ void k_brick_max(Dims d, const T* __restrict__ f, float* __restrict__
 __device__ __forceinline__ float lerp_fma(float a, float b, float t) { return __fmaf_rn(t, b - a, a); }
 
 template <class T>
-__device__ __forceinline__ float sample_fma(const T* __restrict__ f, const Dims& d, F3 g) {
-  const Axis1 x = axis_of(g[0], d.n0, d.n1 * d.n2), y = axis_of(g[1], d.n1, d.n2), z = axis_of(g[2], d.n2, 1);
+__device__ __forceinline__ float sample_fma(const T* __restrict__ f, const Dims& d, const Axis1& x, const Axis1& y,
+                                            const Axis1& z) {
   const T* p = f + (x.i0 * d.n1 + y.i0) * d.n2 + z.i0;
   const float c00 = lerp_fma(ldg_f(p), ldg_f(p + x.step), x.t);
   const float c10 = lerp_fma(ldg_f(p + y.step), ldg_f(p + x.step + y.step), x.t);
@@ -145,21 +168,26 @@ __device__ __forceinline__ float light_at(const Dims& d, const T* __restrict__ s
     const float extent = (float)(imax_(imax_(d.n0, d.n1), d.n2) + 1);
     const float margin = (4.0f * length + 4.0f * extent) * 5.9604645e-8f + 1.0e-3f;
     const F3 delta = mul3(toward, step);
+    const F3 per_cell = f3(1.0f / fabsf(delta[0]), 1.0f / fabsf(delta[1]), 1.0f / fabsf(delta[2]));
     const F3 corner = f3((float)i, (float)j, (float)k);
+    int occupied = -1;  // the last brick of the map found holding smoke: its samples need no look-up
     for (int s = 0; s < steps; ++s) {
       const float t = ((float)s + 0.5f) * step;
       const F3 g = f3(__fmaf_rn(toward[0], t, corner[0]), __fmaf_rn(toward[1], t, corner[1]),
                       __fmaf_rn(toward[2], t, corner[2]));
+      // the sample's axes; a sample's brick is that of its clamped lower corner (x.i0, y.i0, z.i0)
+      const Axis1 x = axis_of(g[0], d.n0, d.n1 * d.n2), y = axis_of(g[1], d.n1, d.n2), z = axis_of(g[2], d.n2, 1);
       if (bricks) {
-        const int i0 = (int)fminf(fmaxf(g[0], 0.0f), (float)(d.n0 - 1));
-        const int j0 = (int)fminf(fmaxf(g[1], 0.0f), (float)(d.n1 - 1));
-        const int k0 = (int)fminf(fmaxf(g[2], 0.0f), (float)(d.n2 - 1));
-        if (__ldg(bricks + at(bd, i0 / BRICK, j0 / BRICK, k0 / BRICK)) <= 0.0f) {
-          s = past_brick(s, steps - 1, samples_in_brick(d, g, delta, margin));
-          continue;
+        const int brick = at(bd, x.i0 / BRICK, y.i0 / BRICK, z.i0 / BRICK);
+        if (brick != occupied) {
+          if (__ldg(bricks + brick) <= 0.0f) {
+            s = past_brick(s, steps - 1, samples_in_brick_by(d, g, delta, per_cell, margin));
+            continue;
+          }
+          occupied = brick;
         }
       }
-      column = __fmaf_rn(fmax_(sample_fma(smoke, d, g), 0.0f), step, column);
+      column = __fmaf_rn(fmax_(sample_fma(smoke, d, x, y, z), 0.0f), step, column);
     }
   }
   return exp_f(-opacity * column * cell_m);
