@@ -575,6 +575,35 @@ __device__ __forceinline__ float pick7(const float* e, int o) {
   return o == 0 ? e[0] : o == 1 ? e[1] : o == 2 ? e[2] : o == 3 ? e[3] : o == 4 ? e[4] : o == 5 ? e[5] : e[6];
 }
 
+// The z blend of k_prolong_add_split8 for the four cells k = 2 (m0 + n) + P of a row. Cell m of parity P sits at
+// coarse z = m - 0.25 (P = 0: columns m - 1 and m, weight 0.75 on m) or m + 0.25 (P = 1: columns m and m + 1,
+// weight 0.25 on m + 1); axis_of forms exactly those indices and weights (t = 0.75 or 0.25, 1 - t = 0.25 or
+// 0.75, all exact) except where a clamp holds: cell m = 0 of parity 0 and cell m = n2 - 1 of parity 1, which
+// take the general blend.
+template <int P>
+__device__ __forceinline__ void prolong_row(const float* e, float* out, int i, int j, int m0, const Dims& coarse,
+                                            const Dims& fine, const float* __restrict__ cq) {
+  constexpr float t = P == 0 ? 0.75f : 0.25f, u = P == 0 ? 0.25f : 0.75f;
+#pragma unroll
+  for (int n = 0; n < 4; ++n) {
+    const int m = m0 + n, k = 2 * m + P;
+    if (k >= fine.n2) continue;
+    float value = e[n + P] * u + e[n + P + 1] * t;  // lerp_w(column m - 1 + P, column m + P, z)
+    if ((P == 0 && m == 0) || (P == 1 && m == coarse.n2 - 1)) {
+      const F3 gk = prolong_point(i, j, k);
+      const Axis1 z = axis_of(gk[2], coarse.n2, 1);
+      const int off = z.i0 - (m0 - 1);  // the clamped cell's column in e
+      if (off >= 0 && off <= 5) {
+        const float lo = pick7(e, off);
+        value = lerp_w(lo, z.step == 0 ? lo : pick7(e, off + 1), z);
+      } else {
+        value = sample_index_space(cq, coarse, gk);
+      }
+    }
+    out[n] = out[n] + value;
+  }
+}
+
 __global__ void k_prolong_add_split8(Dims coarse, Dims fine, int H, const float* __restrict__ cq,
                                      float* __restrict__ qs) {
   wait_for_previous_grid();
@@ -603,22 +632,8 @@ __global__ void k_prolong_add_split8(Dims coarse, Dims fine, int H, const float*
     const long own = ((long)(col * fine.n0 + i) * fine.n1 + j) * H + m0;
     const float4 q4 = ld4(qs + own);
     float out[4] = {q4.x, q4.y, q4.z, q4.w};
-#pragma unroll
-    for (int n = 0; n < 4; ++n) {
-      const int k = 2 * (m0 + n) + p;
-      if (k >= fine.n2) continue;
-      const F3 gk = prolong_point(i, j, k);
-      const Axis1 z = axis_of(gk[2], coarse.n2, 1);
-      const int off = z.i0 - (m0 - 1);  // n + p, or n + p + 1 where the lower clamp holds cell 0 at column 0
-      float value;
-      if (off >= 0 && off <= 5) {
-        const float lo = pick7(e, off);
-        value = lerp_w(lo, z.step == 0 ? lo : pick7(e, off + 1), z);
-      } else {
-        value = sample_index_space(cq, coarse, gk);
-      }
-      out[n] = out[n] + value;
-    }
+    if (p == 0) prolong_row<0>(e, out, i, j, m0, coarse, fine, cq);
+    else prolong_row<1>(e, out, i, j, m0, coarse, fine, cq);
     *reinterpret_cast<float4*>(qs + own) = make_float4(out[0], out[1], out[2], out[3]);
   }
 }

@@ -447,18 +447,25 @@ struct FaceForces {
 
 // One pass over the three face arrays applying, per face and in the reference's order, the confinement push,
 // the turbulence push and drag. blockIdx.z segments: nx+1 u slices, nx v slices, nx w slices.
+// The push of the two cells beside face (i, j, k) along AXIS (add_face_push_kernel's neighbours, clamped).
+template <int AXIS>
+__device__ __forceinline__ void face_push_pair(const PlumeGridInfo& info, int i, int j, int k, const FaceForces& ff,
+                                               float& below, float& above) {
+  const int index = AXIS == 0 ? i : (AXIS == 1 ? j : k);
+  const int lo = imax_(index - 1, 0), hi = imin_(index, info.dims[AXIS] - 1);
+  const Dims d{info.dims[0], info.dims[1], info.dims[2]};
+  const int at_lo = AXIS == 0 ? at(d, lo, j, k) : (AXIS == 1 ? at(d, i, lo, k) : at(d, i, j, lo));
+  const int at_hi = AXIS == 0 ? at(d, hi, j, k) : (AXIS == 1 ? at(d, i, hi, k) : at(d, i, j, hi));
+  below = __ldg(ff.push[AXIS] + at_lo);
+  above = __ldg(ff.push[AXIS] + at_hi);
+}
+
+// `below` and `above`: the face's face_push_pair (read only with the confinement push).
 template <int AXIS>
 __device__ __forceinline__ float face_forces_value(const PlumeGridInfo& info, float value, int i, int j, int k,
-                                                   const FaceForces& ff) {
-  const int nx = info.dims[0], ny = info.dims[1], nz = info.dims[2];
+                                                   const FaceForces& ff, float below, float above) {
   if (ff.confinement) {
-    const int index = AXIS == 0 ? i : (AXIS == 1 ? j : k);
-    const int lo = imax_(index - 1, 0), hi = imin_(index, info.dims[AXIS] - 1);
-    const Dims d{nx, ny, nz};
-    const int at_lo = AXIS == 0 ? at(d, lo, j, k) : (AXIS == 1 ? at(d, i, lo, k) : at(d, i, j, lo));
-    const int at_hi = AXIS == 0 ? at(d, hi, j, k) : (AXIS == 1 ? at(d, i, hi, k) : at(d, i, j, hi));
-    const float* p = ff.push[AXIS];
-    float average = 0.5f * (__ldg(p + at_lo) + __ldg(p + at_hi));
+    float average = 0.5f * (below + above);
     value = value + average * ff.dt;
   }
   if (ff.turbulence) {
@@ -510,13 +517,17 @@ __device__ __forceinline__ void face_forces_planes(const PlumeGridInfo& info, T*
   const Dims d = {info.dims[0] + (AXIS == 0), info.dims[1] + (AXIS == 1), info.dims[2] + (AXIS == 2)};
   if (j >= d.n1 || k >= d.n2) return;
   const long plane = (long)d.n1 * d.n2, at_jk = (long)j * d.n2 + k;
-  float value[PLANES];
+  float value[PLANES], below[PLANES] = {}, above[PLANES] = {};
+#pragma unroll
+  for (int p = 0; p < PLANES; ++p)  // every face and push value loaded before any face is stored
+    if (i0 + p < d.n0) {
+      value[p] = ld_f(f + (i0 + p) * plane + at_jk);
+      if (ff.confinement) face_push_pair<AXIS>(info, i0 + p, j, k, ff, below[p], above[p]);
+    }
 #pragma unroll
   for (int p = 0; p < PLANES; ++p)
-    if (i0 + p < d.n0) value[p] = ld_f(f + (i0 + p) * plane + at_jk);
-#pragma unroll
-  for (int p = 0; p < PLANES; ++p)
-    if (i0 + p < d.n0) st_f(f + (i0 + p) * plane + at_jk, face_forces_value<AXIS>(info, value[p], i0 + p, j, k, ff));
+    if (i0 + p < d.n0)
+      st_f(f + (i0 + p) * plane + at_jk, face_forces_value<AXIS>(info, value[p], i0 + p, j, k, ff, below[p], above[p]));
 }
 
 template <class T, int PLANES>
