@@ -196,8 +196,9 @@ __device__ __forceinline__ float light_at(const Dims& d, const T* __restrict__ s
 // A block of 32 x 8 threads covers 32 cells along z of LIGHT_ROWS * 8 rows of one x-plane; each warp takes
 // LIGHT_ROWS rows. The warp first gives every cell that no march reads its 1 and queues the others in shared
 // memory in row order, then marches the queue 32 cells at a time, so its lanes stay busy where only part of a
-// row is lit.
-constexpr int LIGHT_ROWS = 8;
+// row is lit. Measured on B200 at 256x384x256 (14% of the cells lit): 5.83 ms at 4 rows, 5.85 at 2, 6.15 at 8,
+// where more rows per warp leave fewer, longer blocks to balance over the SMs.
+constexpr int LIGHT_ROWS = 4;
 
 template <class T>
 __global__ void __launch_bounds__(256, 5) k_light_volume(Dims d, const T* __restrict__ smoke, F3 toward, float cell_m,
