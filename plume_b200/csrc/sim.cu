@@ -411,6 +411,23 @@ __device__ __forceinline__ void push_at(const PlumeGridInfo& info, const float* 
   pz[c] = push[2];
 }
 
+// push_at from values loaded beforehand: the spin of the two neighbours on each axis (clamped) and the curl.
+__device__ __forceinline__ F3 push_from(const PlumeGridInfo& info, int i, int j, int k, const float* spin_lo,
+                                        const float* spin_hi, F3 curl, float strength) {
+  const int cell[3] = {i, j, k};
+  const int n[3] = {info.dims[0], info.dims[1], info.dims[2]};
+  F3 toward = f3(0.0f, 0.0f, 0.0f);
+#pragma unroll
+  for (int axis = 0; axis < 3; ++axis) {
+    const int lo = imax_(cell[axis] - 1, 0), hi = imin_(cell[axis] + 1, n[axis] - 1);
+    float span = (float)(hi - lo);
+    if (span > 0.0f) toward[axis] = divide(spin_hi[axis] - spin_lo[axis], divisor(span * info.cell_m));
+  }
+  float length = len3(toward);
+  if (length < 1.0e-12f) return f3(0.0f, 0.0f, 0.0f);
+  return mul3(cross3(div3(toward, length), curl), strength * info.cell_m);
+}
+
 template <int PLANES, bool SPIN>
 __global__ void k_push(PlumeGridInfo info, const float* __restrict__ cx, const float* __restrict__ cy,
                        const float* __restrict__ cz, const float* __restrict__ spin, float* __restrict__ px,
@@ -418,9 +435,36 @@ __global__ void k_push(PlumeGridInfo info, const float* __restrict__ cx, const f
   const int nx = info.dims[0], ny = info.dims[1], nz = info.dims[2];
   const int i0 = blockIdx.z * PLANES, j = blockIdx.y * blockDim.y + threadIdx.y, k = blockIdx.x * blockDim.x + threadIdx.x;
   if (j >= ny || k >= nz) return;
+  if constexpr (SPIN) {
+    // every plane's spins and curl loaded before any push is stored (the loads do not wait on the stores)
+    const Dims d{nx, ny, nz};
+    float lo[PLANES][3], hi[PLANES][3];
+    F3 curl[PLANES];
 #pragma unroll
-  for (int p = 0; p < PLANES; ++p)
-    if (i0 + p < nx) push_at<SPIN>(info, cx, cy, cz, spin, px, py, pz, strength, i0 + p, j, k);
+    for (int p = 0; p < PLANES; ++p) {
+      const int i = imin_(i0 + p, nx - 1);
+      lo[p][0] = __ldg(spin + at(d, imax_(i - 1, 0), j, k));
+      hi[p][0] = __ldg(spin + at(d, imin_(i + 1, nx - 1), j, k));
+      lo[p][1] = __ldg(spin + at(d, i, imax_(j - 1, 0), k));
+      hi[p][1] = __ldg(spin + at(d, i, imin_(j + 1, ny - 1), k));
+      lo[p][2] = __ldg(spin + at(d, i, j, imax_(k - 1, 0)));
+      hi[p][2] = __ldg(spin + at(d, i, j, imin_(k + 1, nz - 1)));
+      curl[p] = load3(cx, cy, cz, at(d, i, j, k));
+    }
+#pragma unroll
+    for (int p = 0; p < PLANES; ++p) {
+      if (i0 + p >= nx) break;
+      const F3 push = push_from(info, i0 + p, j, k, lo[p], hi[p], curl[p], strength);
+      const int c = at(d, i0 + p, j, k);
+      px[c] = push[0];
+      py[c] = push[1];
+      pz[c] = push[2];
+    }
+  } else {
+#pragma unroll
+    for (int p = 0; p < PLANES; ++p)
+      if (i0 + p < nx) push_at<SPIN>(info, cx, cy, cz, spin, px, py, pz, strength, i0 + p, j, k);
+  }
 }
 
 // ---- turbulence: turbulence.py:26-53 -----------------------------------------------------------------------
