@@ -733,11 +733,21 @@ __device__ __forceinline__ void advect_forward_at(const PlumeGridInfo& info, con
   const F3 src = trace_from(vel, p, node_velocity<LAYOUT, G>(vel, i, j, k, p), dt_over_cell);
   const bool outside = fd.uses_outside == 1 && is_outside_open_face(src, info);
   const F3 g = sub3(src, fd.offset);
-  for (int n = 0; n < (FIELDS ? FIELDS : fd.fields); ++n) {
-    float value = fd.outside[n], lo = fd.outside[n], hi = fd.outside[n];
-    if (!outside) value = sample_with_range(fd.data[n], fd.d, g, lo, hi);
-    st_f((write_next ? fd.next[n] : fd.hat[n]) + c, value);
-    if (fd.range[n]) fd.range[n][c] = make_pair_t<T>(lo, hi);
+  // every field sampled before any result is stored: the second field's loads do not wait on the first's stores
+  constexpr int MAXF = FIELDS ? FIELDS : 2;
+  const int count = FIELDS ? FIELDS : fd.fields;
+  float value[MAXF], lo[MAXF], hi[MAXF];
+#pragma unroll
+  for (int n = 0; n < MAXF; ++n) {
+    if (n >= count) break;
+    value[n] = lo[n] = hi[n] = fd.outside[n];
+    if (!outside) value[n] = sample_with_range(fd.data[n], fd.d, g, lo[n], hi[n]);
+  }
+#pragma unroll
+  for (int n = 0; n < MAXF; ++n) {
+    if (n >= count) break;
+    st_f((write_next ? fd.next[n] : fd.hat[n]) + c, value[n]);
+    if (fd.range[n]) fd.range[n][c] = make_pair_t<T>(lo[n], hi[n]);
   }
 }
 
@@ -775,7 +785,13 @@ __device__ __forceinline__ void advect_correct_at(const PlumeGridInfo& info, con
     source_outside = fd.uses_outside == 1 && is_outside_open_face(source, info);
     gs = sub3(source, fd.offset);
   }
-  for (int n = 0; n < (FIELDS ? FIELDS : fd.fields); ++n) {
+  // every field corrected before any is stored: the second field's loads do not wait on the first's store
+  constexpr int MAXF = FIELDS ? FIELDS : 2;
+  const int count = FIELDS ? FIELDS : fd.fields;
+  float result[MAXF];
+#pragma unroll
+  for (int n = 0; n < MAXF; ++n) {
+    if (n >= count) break;
     const float back = back_outside ? fd.outside[n] : sample_index_space(fd.hat[n], fd.d, gb);
     const float corrected = ldg_f(fd.hat[n] + c) + 0.5f * (ldg_f(fd.data[n] + c) - back);
     float lo = fd.outside[n], hi = fd.outside[n];
@@ -786,7 +802,12 @@ __device__ __forceinline__ void advect_correct_at(const PlumeGridInfo& info, con
     } else if (!source_outside) {
       sample_with_range(fd.data[n], fd.d, gs, lo, hi);
     }
-    st_f(fd.next[n] + c, clampf_(corrected, lo, hi));
+    result[n] = clampf_(corrected, lo, hi);
+  }
+#pragma unroll
+  for (int n = 0; n < MAXF; ++n) {
+    if (n >= count) break;
+    st_f(fd.next[n] + c, result[n]);
   }
 }
 
