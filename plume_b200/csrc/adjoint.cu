@@ -223,8 +223,8 @@ __global__ void k_budget_adjoint_apply(const float* __restrict__ a_out, long n, 
 }
 
 // The ortho thickness march (raymarch.py:86-140, thickness channel only) and its adjoint for
-// loss = sum over pixels (thickness - target)^2: writes thickness, adds the pixel's squared error to *loss and
-// scatters d loss / d smoke into a_smoke.
+// loss = sum over pixels (thickness - target)^2: writes thickness and scatters d loss / d smoke into a_smoke
+// (k_loss_sum adds the squared errors to *loss).
 __global__ void k_thickness_adjoint(PlumeGridInfo info, PlumeViewParams view, float opacity,
                                     const float* __restrict__ smoke, const float* __restrict__ target, int height,
                                     int width, float* __restrict__ thickness_out, double* __restrict__ loss,
@@ -270,7 +270,6 @@ __global__ void k_thickness_adjoint(PlumeGridInfo info, PlumeViewParams view, fl
   const long pixel = (long)py * width + px;
   thickness_out[pixel] = thickness;
   const float error = thickness - target[pixel];
-  atomicAdd(loss, (double)error * (double)error);
   const float a_rho = 2.0f * error * opacity * step_m * tr;
   if (a_rho == 0.0f) return;
   for (int s = 0; s < steps; ++s) {
@@ -723,6 +722,25 @@ extern "C" int plume_smoke_adjoint(const PlumeGridInfo* info, const float* u, co
   return launch_status("MacCormack adjoint (forward sample)");
 }
 
+// *loss += sum over pixels (thickness - target)^2 in double, in one fixed order: one block, each thread a fixed
+// stride of pixels, then a halving tree, so the same images give the same loss bit for bit on every run.
+__global__ void __launch_bounds__(1024) k_loss_sum(const float* __restrict__ thickness, const float* __restrict__ target,
+                                                   long n, double* __restrict__ loss) {
+  __shared__ double slot[1024];
+  double value = 0.0;
+  for (long i = threadIdx.x; i < n; i += 1024) {
+    const float error = thickness[i] - target[i];
+    value = value + (double)error * (double)error;
+  }
+  slot[threadIdx.x] = value;
+  __syncthreads();
+  for (int h = 512; h >= 1; h >>= 1) {
+    if ((int)threadIdx.x < h) slot[threadIdx.x] = slot[threadIdx.x] + slot[threadIdx.x + h];
+    __syncthreads();
+  }
+  if (threadIdx.x == 0) *loss = *loss + slot[0];
+}
+
 extern "C" int plume_thickness_adjoint(const PlumeGridInfo* info, const PlumeViewParams* view, float opacity,
                                        const float* smoke, const float* target, int32_t height, int32_t width,
                                        float* thickness, double* loss, float* a_smoke, void* stream) {
@@ -732,7 +750,10 @@ extern "C" int plume_thickness_adjoint(const PlumeGridInfo* info, const PlumeVie
   dim3 block(16, 16), grid((width + 15) / 16, (height + 15) / 16);
   k_thickness_adjoint<<<grid, block, 0, as_stream(stream)>>>(*info, *view, opacity, smoke, target, height, width,
                                                              thickness, loss, a_smoke);
-  return launch_status("thickness adjoint");
+  int status = launch_status("thickness adjoint");
+  if (status != PLUME_OK) return status;
+  k_loss_sum<<<1, 1024, 0, as_stream(stream)>>>(thickness, target, (long)height * width, loss);
+  return launch_status("thickness loss");
 }
 
 extern "C" int plume_maccormack_adjoint(const PlumeGridInfo* info, const int32_t shape[3], const float offset[3],
